@@ -1,0 +1,258 @@
+/*
+ * rodgpu.h - C ABI of the B200 rigid-rod contact hot path (librodgpu.so).
+ *
+ * One rg_system holds the device state of one periodic (or open) system of
+ * capsules and advances it with the contact model of rod-dynamics-3d's
+ * App::physicsStep (src/app/main.cpp:4333-4858):
+ *   - "nsc":            free flight, detection, PSOR friction-cone sweeps,
+ *                       semi-implicit position update, normal-only position
+ *                       projection        (main.cpp:4383-4528)
+ *   - "harmonic":       soft penalty contact with smooth / Cundall-Strack /
+ *                       Karnopp friction, velocity Verlet (main.cpp:4610-4810)
+ *   - "hertz-mindlin":  Hertz normal + Mindlin tangential spring with history
+ *                       and rolling friction, applied to capsule contacts,
+ *                       velocity Verlet    (main.cpp:4529-4609)
+ *
+ * Plain pointers and sizes only; no exceptions cross this boundary.  Every
+ * entry point returns an rg_status (0 = ok).  Arrays are structure-of-arrays
+ * FP64 in HOST memory unless the name says _dev.  A handle is not thread
+ * safe; use one handle per host thread.
+ *
+ * The reference has no C ABI for this path.  The entry points below replace
+ * the solver-class seam that App::physicsStep calls:
+ *   ContactDetector::detectContacts   (include/physics/contact_detector.hpp:70)
+ *   SoftContactSolver::computeForces  (include/physics/soft_contact.hpp:47)
+ *   HertzMindlinSolver::computeForces (include/physics/hertz_mindlin.hpp:90)
+ *   NscContactSolver::detectAndBuildManifolds / solveVelocities /
+ *     projectPositions                (include/physics/nsc_contact.hpp:88-103)
+ *   integrateHalfPos / integrateSecondHalf (include/physics/integrator.hpp:33-34)
+ * and the free-function CUDA precedent cudaDetectCapsulePairsTwoPass
+ *   (include/physics/cuda_broadphase.hpp:95-101).
+ */
+#ifndef RODGPU_H
+#define RODGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RG_ABI_VERSION 1
+
+typedef enum rg_status {
+  RG_OK = 0,
+  RG_ERR_ARG = 1,          /* bad argument (null pointer, n <= 0, ...)        */
+  RG_ERR_CUDA = 2,         /* a CUDA runtime call failed                      */
+  RG_ERR_CAPACITY = 3,     /* a device buffer overflowed and could not grow   */
+  RG_ERR_NONFINITE = 4,    /* non-finite body state after a step              */
+  RG_ERR_NOT_CONVERGED = 5,/* PSOR hit max sweeps above tolerance (strict)    */
+  RG_ERR_NO_DEVICE = 6,    /* no CUDA device visible                          */
+  RG_ERR_TIMEOUT = 7,      /* a bounded device-side wait gave up              */
+  RG_ERR_STATE = 8         /* call out of order (e.g. step before bodies set) */
+} rg_status;
+
+typedef enum rg_model {
+  RG_MODEL_NONE = 0,          /* physicsStep with no model enabled: no-op   */
+  RG_MODEL_NSC = 1,           /* contact_model "nsc"                        */
+  RG_MODEL_HARMONIC = 2,      /* contact_model "harmonic" (soft penalty)    */
+  RG_MODEL_HERTZ_MINDLIN = 3  /* contact_model "hertz-mindlin" (capsules)   */
+} rg_model;
+
+typedef enum rg_friction_mode {  /* SoftContactSolver::computeFriction      */
+  RG_FRICTION_SMOOTH = 0,        /* default (soft_contact.cpp:458-485)      */
+  RG_FRICTION_CUNDALL = 1,       /* friction_cundall (soft_contact.cpp:317) */
+  RG_FRICTION_KARNOPP = 2        /* friction_karnopp (soft_contact.cpp:369) */
+} rg_friction_mode;
+
+typedef enum rg_psor_order {
+  RG_ORDER_COLORED = 0,  /* graph-coloured Gauss-Seidel (the device order)   */
+  RG_ORDER_SORTED = 1    /* sequential sorted (a,b) order of the reference
+                            (nsc_contact.cpp:91-102); oracle only           */
+} rg_psor_order;
+
+typedef enum rg_warm_start {
+  RG_WARM_CACHE = 0,     /* previous-step impulses by pair (nsc_contact.cpp:305-317) */
+  RG_WARM_NONE = 1,      /* cold start                                       */
+  RG_WARM_MLP = 2        /* learned warm start from rg_mlp weights           */
+} rg_warm_start;
+
+/* Configuration.  Field meanings and defaults follow AppCfg
+ * (include/config/config.hpp:6-110); rg_config_default() fills them. */
+typedef struct rg_config {
+  int32_t n_bodies;
+  int32_t model;                 /* rg_model */
+  double dt;
+  double gravity[3];
+  double lin_damp, ang_damp, w_max;
+  int32_t pbc_enabled;
+  double pbc_min[3], pbc_max[3];
+
+  /* SoftContactCfg (config.hpp:6-27) */
+  double soft_delta, soft_k_scaler, soft_damping, soft_mu, soft_mu_static;
+  double soft_nu, soft_kt, soft_vel_deadband;
+  int32_t soft_enable_friction;
+  int32_t soft_friction_mode;    /* rg_friction_mode */
+
+  /* HertzMindlinCfg (config.hpp:29-64) */
+  double hm_youngs_modulus, hm_poisson_ratio, hm_restitution;
+  double hm_friction, hm_friction_static, hm_friction_transition_vel;
+  double hm_rolling_friction;
+  int32_t hm_enable_tangential, hm_enable_rolling;
+
+  /* NscContactCfg (config.hpp:66-88) */
+  double nsc_mu, nsc_beta, nsc_cfm, nsc_omega, nsc_slop, nsc_tol;
+  int32_t nsc_velocity_iters, nsc_position_stabilization;
+  int32_t nsc_position_iters, nsc_position_psor_iters;
+  int32_t nsc_warm_start;        /* rg_warm_start */
+  int32_t psor_order;            /* rg_psor_order; device supports COLORED */
+
+  /* Neighbour-list broad phase (project-specific, no reference field). */
+  double skin;                   /* Verlet skin; <= 0 selects automatic      */
+  int32_t max_neighbors;         /* initial per-rod list capacity; <= 0 auto */
+  int32_t reserved[7];
+} rg_config;
+
+/* Per-call statistics (the profile-CSV columns of main.cpp:3276-3355). */
+typedef struct rg_step_stats {
+  int64_t steps;            /* steps taken in this call                       */
+  int64_t contacts;         /* contacts at the last detection                 */
+  int64_t collisions;       /* NSC: manifolds with v_n_pre < -1e-6 (last step)*/
+  int64_t psor_sweeps;      /* NSC: velocity sweeps summed over the call      */
+  int64_t psor_sweeps_last; /* NSC: velocity sweeps of the last step          */
+  int64_t list_rebuilds;    /* neighbour-list rebuilds in this call           */
+  int64_t colors;           /* NSC: colours of the last velocity solve        */
+  int64_t history_size;     /* HM / Cundall: live history entries             */
+  double residual;          /* NSC: last PSOR residual (max |dλ| sum)         */
+  double jn_sum, jt_sum;    /* NSC: Σλn, Σ|λt| of the last step               */
+  double potential_energy;  /* soft / HM: last contact potential energy       */
+  double kinetic_energy;    /* ½Σ m|v|² + ½Σ ω·Iω after the call              */
+  double max_residual;      /* NSC: worst final residual over the call        */
+  int64_t not_converged;    /* NSC: steps that stopped at max sweeps          */
+  double device_ms;         /* device time of the call (CUDA events, stream)  */
+  int64_t psor_row_sweeps;  /* NSC: Σ over steps of contacts x sweeps         */
+  int64_t kernel_launches;  /* kernels this library launched during the call  */
+  int64_t reserved[3];
+} rg_step_stats;
+
+/* Stage timers (CUDA events on the system's stream), enabled per system.
+ * Stages: 0 integrate, 1 detect (incl. list rebuild), 2 colour, 3 manifolds,
+ * 4 PSOR sweeps, 5 position projection, 6 contact forces + history, 7 other. */
+#define RG_NSTAGES 8
+
+typedef struct rg_system rg_system;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+int rg_abi_version(void);
+void rg_config_default(rg_config* cfg);
+const char* rg_status_string(int status);
+/* Last error text of this handle (empty when none). */
+const char* rg_last_error(const rg_system* sys);
+
+/* Creates a system on the current CUDA device.  Replaces the solver objects
+ * softContactSolver / hertzMindlinSolver / nscSolver owned by App
+ * (src/app/main.cpp:439-442) as configured in App::resetScene (:1541-1590). */
+int rg_create(const rg_config* cfg, rg_system** out);
+int rg_destroy(rg_system* sys);
+int rg_get_config(const rg_system* sys, rg_config* cfg);
+
+/* Body properties, one value per body (RigidBody fields,
+ * include/physics/rigid_body.hpp:30-41; makeCapsule rigid_body.cpp:11-47).
+ * inertia = body-frame principal moments (Ixx, Iyy, Izz) per body, 3 per body.
+ * mass <= 0 marks a static body (invMass = 0, App::createRod main.cpp:1523). */
+int rg_set_bodies(rg_system* sys, const double* radius, const double* half_height,
+                  const double* mass, const double* inertia,
+                  const double* restitution);
+
+/* State, structure of arrays: x[3N], q[4N] (w,x,y,z), v[3N], w[3N].
+ * Forces f[3N], tau[3N] may be NULL on set (zeroed) or on get (skipped). */
+int rg_set_state(rg_system* sys, const double* x, const double* q,
+                 const double* v, const double* w,
+                 const double* f, const double* tau);
+int rg_get_state(const rg_system* sys, double* x, double* q, double* v,
+                 double* w, double* f, double* tau);
+
+/* Advances nsteps of App::physicsStep for the configured model.
+ * stats may be NULL. */
+int rg_step(rg_system* sys, int nsteps, rg_step_stats* stats);
+
+/* Runs one detection at the current state (ContactDetector::detectContacts,
+ * contact_detector.cpp:71-211, activation margin = the model's delta) and
+ * copies the contacts, sorted by (a,b), to host buffers of capacity cap.
+ * pairs[2*i] = a, pairs[2*i+1] = b (a < b);
+ * geom[12*i..] = point_a(3), point_b(3), normal(3), distance, surface_limit,
+ *                type (0 P2P, 1 E2P, 2 E2E as double);
+ * shift[3*i..] = minimum-image shift applied to body b.
+ * Any of geom / shift may be NULL.  *n receives the contact count even when
+ * it exceeds cap (then only cap are written and RG_ERR_CAPACITY returned). */
+int rg_detect(rg_system* sys, double delta, int32_t* pairs, double* geom,
+              double* shift, size_t cap, size_t* n);
+
+/* Contacts / impulses of the last NSC velocity solve, sorted by (a,b):
+ * lambda[3*i..] = (λn, λt1, λt2); color[i] = PSOR colour (may be NULL). */
+int rg_get_impulses(const rg_system* sys, int32_t* pairs, double* lambda,
+                    int32_t* color, size_t cap, size_t* n);
+
+/* Per-body force and torque of one force evaluation at the current state
+ * (soft or HM model), without integrating: f[3N], tau[3N].  Advances the
+ * tangential history exactly like one computeForces call of the reference. */
+int rg_compute_forces(rg_system* sys, double* f, double* tau, double* pe);
+
+/* Tangential-history table (HM: ξ per pair; Cundall: F_t per pair), sorted
+ * by pair: pairs[2*i..], value[3*i..], last_frame[i] (may be NULL). */
+int rg_get_history(const rg_system* sys, int32_t* pairs, double* value,
+                   int64_t* last_frame, size_t cap, size_t* n);
+
+/* Enables (1) or disables (0) the stage timers; resets the accumulators. */
+int rg_set_profiling(rg_system* sys, int enable);
+/* Accumulated milliseconds and launch counts per stage since enabling. */
+int rg_get_profile(const rg_system* sys, double* ms, int64_t* launches);
+
+/* ---- learned PSOR warm start ------------------------------------------- */
+/* MLP 8 -> 128 -> 128 -> 128 -> 3 (SiLU), BF16 weights and activations,
+ * FP32 accumulation.  Features per contact (in this order): gap φ, v_n,
+ * v_t1, v_t2, previous λn, λt1, λt2 (0 when new), contact-graph degree.
+ * Targets: converged (λn, λt1, λt2).  Weights are held by the system. */
+#define RG_MLP_IN 8
+#define RG_MLP_HIDDEN 128
+#define RG_MLP_OUT 3
+/* Number of float parameters: W1 128x8, b1, W2 128x128, b2, W3 128x128, b3,
+ * W4 3x128, b4, then input mean/scale (8+8) and output scale (3). */
+size_t rg_mlp_param_count(void);
+int rg_mlp_set_params(rg_system* sys, const float* params, size_t n);
+int rg_mlp_get_params(const rg_system* sys, float* params, size_t n);
+/* Records (features, converged impulses) of every NSC step taken while
+ * recording is on are appended to a device buffer of capacity cap records. */
+int rg_mlp_record(rg_system* sys, int enable, size_t cap);
+int rg_mlp_records(const rg_system* sys, float* features, float* targets,
+                   size_t cap, size_t* n);
+/* Trains on host records with the device forward/backward kernels (Adam). */
+int rg_mlp_train(rg_system* sys, const float* features, const float* targets,
+                 size_t n, int epochs, int batch, float lr, uint64_t seed,
+                 float* final_loss);
+/* Inference: out[3*n] = MLP(features[8*n]). */
+int rg_mlp_infer(rg_system* sys, const float* features, float* out, size_t n);
+
+/* ---- batched independent systems ---------------------------------------- */
+/* A batch runs many independent periodic systems of uneven size in one
+ * device step (one launch sequence, CUDA-graph captured).  Each member has
+ * its own rg_config (box, model, dt, μ, ...).  Bodies of member k occupy
+ * global indices [offset_k, offset_k + n_k). */
+typedef struct rg_batch rg_batch;
+int rg_batch_create(const rg_config* cfgs, int n_systems, rg_batch** out);
+int rg_batch_destroy(rg_batch* b);
+int rg_batch_set_bodies(rg_batch* b, int k, const double* radius,
+                        const double* half_height, const double* mass,
+                        const double* inertia, const double* restitution);
+int rg_batch_set_state(rg_batch* b, int k, const double* x, const double* q,
+                       const double* v, const double* w);
+int rg_batch_get_state(const rg_batch* b, int k, double* x, double* q,
+                       double* v, double* w);
+int rg_batch_step(rg_batch* b, int nsteps, rg_step_stats* per_system);
+int rg_batch_set_mlp(rg_batch* b, const float* params, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RODGPU_H */

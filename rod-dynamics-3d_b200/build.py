@@ -1,0 +1,72 @@
+"""Builds librodgpu.so (the CUDA hot path + C ABI) in-tree for sm_100a.
+
+Usage: python rod-dynamics-3d_b200/build.py [--force]
+The library is written next to this file so it travels with the repository.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "librodgpu.so")
+HOSTLIB = os.path.join(HERE, "librodhost.so")
+HOST_SRCS = [os.path.join(HERE, "host", "scene_gen.cpp")]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+# -fmad=false: no contraction of a*b+c into FMA, so every FP64 expression
+# rounds as written (bit-exact contact predicate against the FP64 oracle).
+FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+         "-fmad=false", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-shared",
+         "-Xcompiler", "-fvisibility=default"]
+
+
+def sources():
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+
+
+def headers():
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    hs.append(os.path.join(HERE, "..", "include", "rodgpu.h"))
+    return hs
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(p) <= t for p in sources() + headers() + [__file__])
+
+
+def build_host(force=False, verbose=False):
+    """Host C++ helpers (scene generator, mass properties)."""
+    if (not force and os.path.exists(HOSTLIB)
+            and all(os.path.getmtime(p) <= os.path.getmtime(HOSTLIB) for p in HOST_SRCS)):
+        return HOSTLIB
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", HOSTLIB] + HOST_SRCS
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("g++ failed building librodhost.so")
+    return HOSTLIB
+
+
+def build(force=False, verbose=False):
+    build_host(force, verbose)
+    if not force and up_to_date():
+        return LIB
+    cmd = [NVCC] + FLAGS + ["-o", LIB] + sources() + ["-lcudart"]
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed building librodgpu.so")
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(LIB)

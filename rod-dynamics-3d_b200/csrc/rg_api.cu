@@ -1,0 +1,731 @@
+// rg_api.cu - the C ABI of librodgpu.so (declared in include/rodgpu.h).
+//
+// Owns the device buffers of one system, sequences the per-step kernels of
+// App::physicsStep (src/app/main.cpp:4333-4858) for the configured model, and
+// turns device-side error bits into rg_status codes.  Capacity overflows
+// (contacts, neighbour lists, history, colours) are recovered transparently:
+// the state at the start of the call is kept in a device snapshot, the
+// buffers grow, and the call re-runs from the snapshot.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "rg_internal.cuh"
+
+using namespace rg;
+
+namespace {
+
+const char* kStatus[] = {"ok", "bad argument", "CUDA error", "capacity exceeded",
+                         "non-finite state", "PSOR not converged", "no CUDA device",
+                         "device wait timed out", "call out of order"};
+
+int fail(rg_system* s, int code, const std::string& msg) {
+  if (s) s->err_text = msg;
+  return code;
+}
+
+int cuda_fail(rg_system* s, cudaError_t e, const char* where) {
+  cudaGetLastError();
+  return fail(s, RG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define RG_TRY(call, where)                         \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return cuda_fail(s, e_, where); \
+  } while (0)
+
+void bind_state(rg_system* s) {
+  const int n = s->n;
+  double* b = s->d_state;
+  State& st = s->st;
+  st.n = n;
+  st.x = {b, b + n, b + 2 * n};
+  st.q = {b + 3 * n, b + 4 * n, b + 5 * n, b + 6 * n};
+  st.v = {b + 7 * n, b + 8 * n, b + 9 * n};
+  st.w = {b + 10 * n, b + 11 * n, b + 12 * n};
+  st.f = {b + 13 * n, b + 14 * n, b + 15 * n};
+  st.tau = {b + 16 * n, b + 17 * n, b + 18 * n};
+  double* p = s->d_props;
+  st.r = p; st.h = p + n; st.mass = p + 2 * n; st.inv_mass = p + 3 * n; st.rest = p + 4 * n;
+  st.I = {p + 5 * n, p + 6 * n, p + 7 * n};
+  st.Iinv = {p + 8 * n, p + 9 * n, p + 10 * n};
+}
+
+size_t ctl_size(const rg_config& c) {
+  int slots = c.nsc_velocity_iters;
+  if (c.nsc_position_psor_iters + 2 > slots) slots = c.nsc_position_psor_iters + 2;
+  if (slots < 4) slots = 4;
+  return sizeof(Ctl) + sizeof(double) * (size_t)slots;
+}
+
+void free_contact_buffers(rg_system* s) {
+  s->con.free_();
+  cudaFree(s->csr.cnt); cudaFree(s->csr.off); cudaFree(s->csr.fill); cudaFree(s->csr.ent);
+  s->csr = BodyCSR();
+  History& H = s->hist;
+  for (int k = 0; k < 2; ++k) { cudaFree(H.key[k]); cudaFree(H.val[k]); cudaFree(H.frame[k]); }
+  cudaFree(H.found); cudaFree(H.touched); cudaFree(H.touched_off); cudaFree(H.kept);
+  cudaFree(H.kept_off); cudaFree(H.newval);
+  H = History();
+  Nsc& N = s->nsc;
+  cudaFree(N.row); cudaFree(N.lam); cudaFree(N.color); cudaFree(N.color_tmp); cudaFree(N.order);
+  cudaFree(N.color_cnt); cudaFree(N.color_off); cudaFree(N.wkey); cudaFree(N.wlam); cudaFree(N.wn);
+  cudaFree(N.dx); cudaFree(N.prow); cudaFree(N.pactive);
+  N = Nsc();
+  cudaFree(s->d_cf);
+  s->d_cf = nullptr;
+  s->scan.free_();
+  cudaFree(s->d_feat); cudaFree(s->d_pred);
+  s->d_feat = nullptr; s->d_pred = nullptr;
+}
+
+// Allocates every contact-sized buffer for capacity ccap and history hcap.
+cudaError_t alloc_contact_buffers(rg_system* s, int ccap, int hcap) {
+  const int n = s->n;
+  s->ccap = ccap;
+  cudaError_t e;
+  if ((e = s->con.alloc(ccap))) return e;
+  if ((e = cudaMalloc(&s->csr.cnt, sizeof(int) * (n + 1)))) return e;
+  if ((e = cudaMalloc(&s->csr.off, sizeof(int) * (n + 1)))) return e;
+  if ((e = cudaMalloc(&s->csr.fill, sizeof(int) * n))) return e;
+  if ((e = cudaMalloc(&s->csr.ent, sizeof(int) * 2 * (size_t)ccap))) return e;
+  History& H = s->hist;
+  H.cap = hcap;
+  for (int k = 0; k < 2; ++k) {
+    if ((e = cudaMalloc(&H.key[k], sizeof(unsigned long long) * hcap))) return e;
+    if ((e = cudaMalloc(&H.val[k], sizeof(double) * 3 * (size_t)hcap))) return e;
+    if ((e = cudaMalloc(&H.frame[k], sizeof(long long) * hcap))) return e;
+  }
+  if ((e = cudaMalloc(&H.found, sizeof(int) * ccap))) return e;
+  if ((e = cudaMalloc(&H.touched, sizeof(int) * (ccap + 1)))) return e;
+  if ((e = cudaMalloc(&H.touched_off, sizeof(int) * (ccap + 1)))) return e;
+  if ((e = cudaMalloc(&H.kept, sizeof(int) * (hcap + 1)))) return e;
+  if ((e = cudaMalloc(&H.kept_off, sizeof(int) * (hcap + 1)))) return e;
+  if ((e = cudaMalloc(&H.newval, sizeof(double) * 3 * (size_t)ccap))) return e;
+  Nsc& N = s->nsc;
+  if ((e = cudaMalloc(&N.row, sizeof(double) * kRowComps * (size_t)ccap))) return e;
+  if ((e = cudaMalloc(&N.lam, sizeof(double) * 3 * (size_t)ccap))) return e;
+  if ((e = cudaMalloc(&N.color, sizeof(int) * (ccap + 1)))) return e;
+  if ((e = cudaMalloc(&N.color_tmp, sizeof(int) * ((size_t)ccap + 1024)))) return e;
+  if ((e = cudaMalloc(&N.order, sizeof(int) * (ccap + 1)))) return e;
+  if ((e = cudaMalloc(&N.color_cnt, sizeof(int) * (kMaxColors + 2)))) return e;
+  if ((e = cudaMalloc(&N.color_off, sizeof(int) * (kMaxColors + 2)))) return e;
+  N.wcap = ccap;
+  if ((e = cudaMalloc(&N.wkey, sizeof(unsigned long long) * ccap))) return e;
+  if ((e = cudaMalloc(&N.wlam, sizeof(double) * 3 * (size_t)ccap + sizeof(int) * (size_t)ccap))) return e;
+  if ((e = cudaMalloc(&N.wn, sizeof(int)))) return e;
+  if ((e = cudaMemset(N.wn, 0, sizeof(int)))) return e;
+  if ((e = cudaMalloc(&N.dx, sizeof(double) * 6 * (size_t)n))) return e;
+  if ((e = cudaMemset(N.dx, 0, sizeof(double) * 6 * (size_t)n))) return e;
+  if ((e = cudaMalloc(&N.prow, sizeof(double) * kPosComps * (size_t)ccap))) return e;
+  if ((e = cudaMalloc(&N.pactive, sizeof(int) * ccap))) return e;
+  if ((e = cudaMalloc(&s->d_cf, sizeof(double) * (13 * (size_t)ccap + 64)))) return e;
+  if ((e = cudaMalloc(&s->d_feat, sizeof(float) * 8 * (size_t)ccap))) return e;
+  if ((e = cudaMalloc(&s->d_pred, sizeof(float) * 3 * (size_t)ccap))) return e;
+  int scap = ccap + 1;
+  if (hcap + 1 > scap) scap = hcap + 1;
+  if (n + 1 > scap) scap = n + 1;
+  if (s->det.ncells + 1 > scap) scap = s->det.ncells + 1;
+  return s->scan.alloc(scap);
+}
+
+__global__ void k_ke(State st, Ctl* ctl, double* out) {
+  __shared__ double sm[32];
+  double ke = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
+    d3 v = st.v.ld(i), w = st.w.ld(i);
+    ke += 0.5 * st.mass[i] * dot(v, v);
+    ke += 0.5 * dot(w, rot_diag_apply(st.q.ld(i), st.I.ld(i), w));
+  }
+  ke = warp_sum(ke);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = ke;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double u = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+    u = warp_sum(u);
+    if (threadIdx.x == 0) out[blockIdx.x] = u;
+  }
+  (void)ctl;
+}
+
+struct Snapshot {
+  std::vector<char> ctl;
+  int hist_cur = 0;
+  int wn = 0;
+};
+
+// Device snapshot of everything a step mutates: state, control words,
+// current history table and the NSC warm cache.
+cudaError_t take_snapshot(rg_system* s, Snapshot& sn) {
+  const int n = s->n;
+  cudaError_t e;
+  size_t need = sizeof(double) * 19 * (size_t)n;
+  if (!s->d_snap && (e = cudaMalloc(&s->d_snap, need))) return e;
+  const History& H = s->hist;
+  if (s->snap_hcap != H.cap) {
+    cudaFree(s->snap_hkey); cudaFree(s->snap_hval); cudaFree(s->snap_hframe);
+    if ((e = cudaMalloc(&s->snap_hkey, sizeof(unsigned long long) * H.cap))) return e;
+    if ((e = cudaMalloc(&s->snap_hval, sizeof(double) * 3 * (size_t)H.cap))) return e;
+    if ((e = cudaMalloc(&s->snap_hframe, sizeof(long long) * H.cap))) return e;
+    s->snap_hcap = H.cap;
+  }
+  const Nsc& N = s->nsc;
+  const size_t wl_bytes = sizeof(double) * 3 * (size_t)N.wcap + sizeof(int) * (size_t)N.wcap;
+  if (s->snap_wcap != N.wcap) {
+    cudaFree(s->snap_wkey); cudaFree(s->snap_wlam);
+    if ((e = cudaMalloc(&s->snap_wkey, sizeof(unsigned long long) * N.wcap))) return e;
+    if ((e = cudaMalloc(&s->snap_wlam, wl_bytes))) return e;
+    s->snap_wcap = N.wcap;
+  }
+  cudaStream_t st = s->stream;
+  cudaMemcpyAsync(s->d_snap, s->d_state, need, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(s->snap_hkey, H.key[H.cur], sizeof(unsigned long long) * H.cap, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(s->snap_hval, H.val[H.cur], sizeof(double) * 3 * (size_t)H.cap, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(s->snap_hframe, H.frame[H.cur], sizeof(long long) * H.cap, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(s->snap_wkey, N.wkey, sizeof(unsigned long long) * N.wcap, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(s->snap_wlam, N.wlam, wl_bytes, cudaMemcpyDeviceToDevice, st);
+  sn.ctl.resize(s->ctl_bytes);
+  cudaMemcpyAsync(sn.ctl.data(), s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&sn.wn, N.wn, sizeof(int), cudaMemcpyDeviceToHost, st);
+  sn.hist_cur = H.cur;
+  return cudaStreamSynchronize(st);
+}
+
+// Puts the snapshot back into the live buffers (same capacities).
+cudaError_t restore_snapshot(rg_system* s, const Snapshot& sn) {
+  History& H = s->hist;
+  const Nsc& N = s->nsc;
+  H.cur = sn.hist_cur;
+  const size_t wl_bytes = sizeof(double) * 3 * (size_t)N.wcap + sizeof(int) * (size_t)N.wcap;
+  cudaMemcpy(s->d_state, s->d_snap, sizeof(double) * 19 * (size_t)s->n, cudaMemcpyDeviceToDevice);
+  cudaMemcpy(H.key[H.cur], s->snap_hkey, sizeof(unsigned long long) * H.cap, cudaMemcpyDeviceToDevice);
+  cudaMemcpy(H.val[H.cur], s->snap_hval, sizeof(double) * 3 * (size_t)H.cap, cudaMemcpyDeviceToDevice);
+  cudaMemcpy(H.frame[H.cur], s->snap_hframe, sizeof(long long) * H.cap, cudaMemcpyDeviceToDevice);
+  cudaMemcpy(N.wkey, s->snap_wkey, sizeof(unsigned long long) * N.wcap, cudaMemcpyDeviceToDevice);
+  cudaMemcpy(N.wlam, s->snap_wlam, wl_bytes, cudaMemcpyDeviceToDevice);
+  cudaMemcpy(N.wn, &sn.wn, sizeof(int), cudaMemcpyHostToDevice);
+  std::memcpy(s->h_ctl, sn.ctl.data(), s->ctl_bytes);
+  return cudaMemcpy(s->d_ctl, sn.ctl.data(), s->ctl_bytes, cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rg_abi_version(void) { return RG_ABI_VERSION; }
+
+const char* rg_status_string(int status) {
+  if (status < 0 || status > RG_ERR_STATE) return "unknown status";
+  return kStatus[status];
+}
+
+const char* rg_last_error(const rg_system* s) { return s ? s->err_text.c_str() : ""; }
+
+void rg_config_default(rg_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->n_bodies = 0;
+  c->model = RG_MODEL_NONE;
+  c->dt = 1.0 / 600.0;                  // PhysicsCfg (config.hpp:91)
+  c->gravity[1] = -10.0;
+  c->lin_damp = 0.08; c->ang_damp = 0.12; c->w_max = 80.0;
+  c->pbc_enabled = 0;
+  c->pbc_min[0] = -3; c->pbc_min[1] = -1; c->pbc_min[2] = -3;
+  c->pbc_max[0] = 3; c->pbc_max[1] = 3; c->pbc_max[2] = 3;
+  c->soft_delta = 0.005; c->soft_k_scaler = 1000.0; c->soft_damping = 0.0; c->soft_mu = 0.5;
+  c->soft_mu_static = 0.0; c->soft_nu = 1e-5; c->soft_kt = 1000.0; c->soft_vel_deadband = 1e-3;
+  c->soft_enable_friction = 1; c->soft_friction_mode = RG_FRICTION_SMOOTH;
+  c->hm_youngs_modulus = 7e10; c->hm_poisson_ratio = 0.25; c->hm_restitution = 0.9;
+  c->hm_friction = 0.3; c->hm_friction_static = 0.5; c->hm_friction_transition_vel = 1e-3;
+  c->hm_rolling_friction = 0.01; c->hm_enable_tangential = 1; c->hm_enable_rolling = 1;
+  c->nsc_mu = 0.3; c->nsc_beta = 0.2; c->nsc_cfm = 0.0; c->nsc_omega = 1.0; c->nsc_slop = 1e-4;
+  c->nsc_tol = 1e-6; c->nsc_velocity_iters = 40; c->nsc_position_stabilization = 1;
+  c->nsc_position_iters = 5; c->nsc_position_psor_iters = 50; c->nsc_warm_start = RG_WARM_CACHE;
+  c->psor_order = RG_ORDER_COLORED;
+  c->skin = 0.0; c->max_neighbors = 0;
+}
+
+int rg_create(const rg_config* cfg, rg_system** out) {
+  if (!cfg || !out) return RG_ERR_ARG;
+  *out = nullptr;
+  if (cfg->n_bodies <= 0 || cfg->model < RG_MODEL_NONE || cfg->model > RG_MODEL_HERTZ_MINDLIN ||
+      !(cfg->dt > 0.0))
+    return RG_ERR_ARG;
+  if (cfg->psor_order != RG_ORDER_COLORED) return RG_ERR_ARG;  // device order is coloured
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return RG_ERR_NO_DEVICE;
+  }
+  rg_system* s = new rg_system();
+  s->cfg = *cfg;
+  s->n = cfg->n_bodies;
+  cudaGetDevice(&s->device);
+  cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device);
+  s->box.pbc = cfg->pbc_enabled ? 1 : 0;
+  for (int k = 0; k < 3; ++k) {
+    s->box.lo[k] = cfg->pbc_min[k];
+    s->box.hi[k] = cfg->pbc_max[k];
+    s->box.L[k] = cfg->pbc_max[k] - cfg->pbc_min[k];
+  }
+  if (s->box.pbc && !(s->box.L[0] > 0 && s->box.L[1] > 0 && s->box.L[2] > 0)) {
+    delete s;
+    return RG_ERR_ARG;
+  }
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) ||
+      (e = cudaMalloc(&s->d_state, sizeof(double) * 19 * (size_t)s->n)) ||
+      (e = cudaMalloc(&s->d_props, sizeof(double) * 11 * (size_t)s->n)) ||
+      (e = cudaMemset(s->d_state, 0, sizeof(double) * 19 * (size_t)s->n)) ||
+      (e = cudaMemset(s->d_props, 0, sizeof(double) * 11 * (size_t)s->n)) ||
+      (e = cudaMallocHost(&s->h_stage, sizeof(double) * 19 * (size_t)s->n))) {
+    rg_destroy(s);
+    return RG_ERR_CUDA;
+  }
+  s->ctl_bytes = ctl_size(*cfg);
+  if ((e = cudaMalloc(&s->d_ctl, s->ctl_bytes)) || (e = cudaMemset(s->d_ctl, 0, s->ctl_bytes)) ||
+      (e = cudaMallocHost(&s->h_ctl, s->ctl_bytes))) {
+    rg_destroy(s);
+    return RG_ERR_CUDA;
+  }
+  bind_state(s);
+  // identity orientations
+  std::vector<double> one(s->n, 1.0);
+  cudaMemcpy(s->st.q.w, one.data(), sizeof(double) * s->n, cudaMemcpyHostToDevice);
+  // persistent kernels run one 256-thread block per SM (co-residency is
+  // guaranteed by the cooperative launch attribute)
+  s->coop_blocks = s->sm_count;
+  *out = s;
+  return RG_OK;
+}
+
+int rg_destroy(rg_system* s) {
+  if (!s) return RG_ERR_ARG;
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  free_contact_buffers(s);
+  detector_free(s);
+  cudaFree(s->d_state); cudaFree(s->d_props); cudaFree(s->d_ctl); cudaFree(s->d_snap);
+  cudaFree(s->snap_hkey); cudaFree(s->snap_hval); cudaFree(s->snap_hframe);
+  cudaFree(s->snap_wkey); cudaFree(s->snap_wlam);
+  cudaFree(s->d_mlp); cudaFree(s->d_rec_x); cudaFree(s->d_rec_y);
+  if (s->h_ctl) cudaFreeHost(s->h_ctl);
+  if (s->h_stage) cudaFreeHost(s->h_stage);
+  for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return RG_OK;
+}
+
+int rg_get_config(const rg_system* s, rg_config* cfg) {
+  if (!s || !cfg) return RG_ERR_ARG;
+  *cfg = s->cfg;
+  return RG_OK;
+}
+
+int rg_set_bodies(rg_system* s, const double* radius, const double* half_height,
+                  const double* mass, const double* inertia, const double* restitution) {
+  if (!s || !radius || !half_height || !mass || !inertia) return RG_ERR_ARG;
+  const int n = s->n;
+  std::vector<double> p(11 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    if (!(radius[i] > 0) || !(half_height[i] >= 0)) return fail(s, RG_ERR_ARG, "radius must be > 0 and half height >= 0");
+    bool dyn = mass[i] > 0;
+    p[i] = radius[i];
+    p[n + i] = half_height[i];
+    p[2 * n + i] = dyn ? mass[i] : 0.0;
+    p[3 * n + i] = dyn ? 1.0 / mass[i] : 0.0;
+    p[4 * n + i] = restitution ? restitution[i] : 0.2;
+    for (int k = 0; k < 3; ++k) {
+      double I = dyn ? inertia[3 * i + k] : 0.0;
+      p[(5 + k) * (size_t)n + i] = I;
+      p[(8 + k) * (size_t)n + i] = (dyn && I > 0) ? 1.0 / I : 0.0;
+    }
+  }
+  RG_TRY(cudaMemcpy(s->d_props, p.data(), sizeof(double) * p.size(), cudaMemcpyHostToDevice), "upload bodies");
+  free_contact_buffers(s);
+  detector_free(s);
+  cudaError_t e = detector_alloc(s);
+  if (e == cudaErrorInvalidValue)
+    return fail(s, RG_ERR_ARG, "periodic box smaller than twice the contact range with more than 4096 bodies");
+  if (e) return cuda_fail(s, e, "detector_alloc");
+  int ccap = 4 * n > 4096 ? 4 * n : 4096;
+  RG_TRY(alloc_contact_buffers(s, ccap, 2 * ccap), "alloc contact buffers");
+  force_rebuild(s);
+  RG_TRY(cudaStreamSynchronize(s->stream), "set_bodies sync");
+  s->bodies_set = true;
+  s->contacts_fresh = false;
+  return RG_OK;
+}
+
+int rg_set_state(rg_system* s, const double* x, const double* q, const double* v, const double* w,
+                 const double* f, const double* tau) {
+  if (!s || !x || !q || !v || !w) return RG_ERR_ARG;
+  const int n = s->n;
+  double* b = s->h_stage;
+  std::memset(b, 0, sizeof(double) * 19 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) {
+      b[(size_t)k * n + i] = x[3 * i + k];
+      b[(size_t)(7 + k) * n + i] = v[3 * i + k];
+      b[(size_t)(10 + k) * n + i] = w[3 * i + k];
+      if (f) b[(size_t)(13 + k) * n + i] = f[3 * i + k];
+      if (tau) b[(size_t)(16 + k) * n + i] = tau[3 * i + k];
+    }
+    for (int k = 0; k < 4; ++k) b[(size_t)(3 + k) * n + i] = q[4 * i + k];
+  }
+  // The neighbour lists need no forced rebuild: the displacement check
+  // against the positions of the last build catches any jump of the state.
+  RG_TRY(cudaMemcpyAsync(s->d_state, b, sizeof(double) * 19 * (size_t)n, cudaMemcpyHostToDevice,
+                         s->stream), "upload state");
+  RG_TRY(cudaStreamSynchronize(s->stream), "set_state sync");
+  s->state_set = true;
+  s->contacts_fresh = false;
+  return RG_OK;
+}
+
+int rg_get_state(const rg_system* s, double* x, double* q, double* v, double* w, double* f, double* tau) {
+  if (!s) return RG_ERR_ARG;
+  const int n = s->n;
+  const double* b = s->h_stage;
+  cudaError_t e = cudaMemcpyAsync(s->h_stage, s->d_state, sizeof(double) * 19 * (size_t)n,
+                                  cudaMemcpyDeviceToHost, s->stream);
+  if (!e) e = cudaStreamSynchronize(s->stream);
+  if (e) return cuda_fail(const_cast<rg_system*>(s), e, "download state");
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) {
+      if (x) x[3 * i + k] = b[(size_t)k * n + i];
+      if (v) v[3 * i + k] = b[(size_t)(7 + k) * n + i];
+      if (w) w[3 * i + k] = b[(size_t)(10 + k) * n + i];
+      if (f) f[3 * i + k] = b[(size_t)(13 + k) * n + i];
+      if (tau) tau[3 * i + k] = b[(size_t)(16 + k) * n + i];
+    }
+    if (q)
+      for (int k = 0; k < 4; ++k) q[4 * i + k] = b[(size_t)(3 + k) * n + i];
+  }
+  return RG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+void launch_steps(rg_system* s, int nsteps) {
+  const int model = s->cfg.model;
+  for (int k = 0; k < nsteps; ++k) {
+    if (model == RG_MODEL_NSC) {
+      nsc_step_launch(s);
+    } else if (model == RG_MODEL_HARMONIC || model == RG_MODEL_HERTZ_MINDLIN) {
+      force_eval_launch(s);      // forces at t (reuses fresh contacts)
+      half_pos_launch(s);
+      clear_forces_launch(s);
+      s->contacts_fresh = false;
+      force_eval_launch(s);      // forces at t + dt
+      second_half_launch(s);
+      s->contacts_fresh = true;  // positions unchanged until the next drift
+    }
+  }
+}
+
+// Grows the buffer named by the error bits.  Returns false if nothing grew.
+bool grow(rg_system* s, int err) {
+  bool grew = false;
+  if (err & (ERR_CONTACT_CAP | ERR_HIST_CAP)) {
+    // keep the history table contents: copy the current table to host
+    History& H = s->hist;
+    int hn = s->h_ctl->hist_n;
+    std::vector<unsigned long long> hk(hn);
+    std::vector<double> hv(3 * (size_t)hn);
+    std::vector<long long> hf(hn);
+    int cur = H.cur;
+    cudaMemcpy(hk.data(), H.key[cur], sizeof(unsigned long long) * hn, cudaMemcpyDeviceToHost);
+    for (int k = 0; k < 3; ++k)
+      cudaMemcpy(hv.data() + (size_t)k * hn, H.val[cur] + (size_t)k * H.cap, sizeof(double) * hn,
+                 cudaMemcpyDeviceToHost);
+    cudaMemcpy(hf.data(), H.frame[cur], sizeof(long long) * hn, cudaMemcpyDeviceToHost);
+    // warm cache
+    int wn = 0;
+    cudaMemcpy(&wn, s->nsc.wn, sizeof(int), cudaMemcpyDeviceToHost);
+    std::vector<unsigned long long> wk(wn);
+    std::vector<double> wl(3 * (size_t)wn);
+    cudaMemcpy(wk.data(), s->nsc.wkey, sizeof(unsigned long long) * wn, cudaMemcpyDeviceToHost);
+    for (int k = 0; k < 3; ++k)
+      cudaMemcpy(wl.data() + (size_t)k * wn, s->nsc.wlam + (size_t)k * s->nsc.wcap, sizeof(double) * wn,
+                 cudaMemcpyDeviceToHost);
+    int ccap = s->ccap, hcap = H.cap;
+    if (err & ERR_CONTACT_CAP) ccap *= 2;
+    if (err & ERR_HIST_CAP) hcap *= 2;
+    if (hcap < 2 * ccap) hcap = 2 * ccap;
+    free_contact_buffers(s);
+    if (alloc_contact_buffers(s, ccap, hcap)) return false;
+    History& G = s->hist;
+    G.cur = 0;
+    cudaMemcpy(G.key[0], hk.data(), sizeof(unsigned long long) * hn, cudaMemcpyHostToDevice);
+    for (int k = 0; k < 3; ++k)
+      cudaMemcpy(G.val[0] + (size_t)k * G.cap, hv.data() + (size_t)k * hn, sizeof(double) * hn,
+                 cudaMemcpyHostToDevice);
+    cudaMemcpy(G.frame[0], hf.data(), sizeof(long long) * hn, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->nsc.wkey, wk.data(), sizeof(unsigned long long) * wn, cudaMemcpyHostToDevice);
+    for (int k = 0; k < 3; ++k)
+      cudaMemcpy(s->nsc.wlam + (size_t)k * s->nsc.wcap, wl.data() + (size_t)k * wn, sizeof(double) * wn,
+                 cudaMemcpyHostToDevice);
+    cudaMemcpy(s->nsc.wn, &wn, sizeof(int), cudaMemcpyHostToDevice);
+    grew = true;
+  }
+  if (err & ERR_NBR_CAP) {
+    int nb = s->det.maxnb * 2;
+    int ncells = s->det.ncells;
+    detector_free(s);
+    s->det.maxnb = nb;
+    if (detector_alloc(s)) return false;
+    if (s->det.ncells + 1 > s->scan.cap) {
+      s->scan.free_();
+      s->scan.alloc(s->det.ncells + 1);
+    }
+    (void)ncells;
+    grew = true;
+  }
+  return grew;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rg_step(rg_system* s, int nsteps, rg_step_stats* stats) {
+  if (!s || nsteps < 0) return RG_ERR_ARG;
+  if (!s->bodies_set || !s->state_set) return fail(s, RG_ERR_STATE, "set bodies and state before stepping");
+  Snapshot sn;
+  RG_TRY(take_snapshot(s, sn), "snapshot");
+  const bool fresh0 = s->contacts_fresh;
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    // reset per-call counters
+    Ctl* h = s->h_ctl;
+    std::memcpy(h, sn.ctl.data(), s->ctl_bytes);
+    h->err = 0;
+    h->rebuilds = 0;
+    h->sweeps_sum = 0;
+    h->not_conv = 0;
+    h->max_residual = 0;
+    h->row_sweeps = 0;
+    h->bar_count = 0;
+    RG_TRY(cudaMemcpyAsync(s->d_ctl, h, s->ctl_bytes, cudaMemcpyHostToDevice, s->stream), "ctl upload");
+    s->rec_stage.clear(); s->rec_a.clear(); s->rec_b.clear(); s->ev_used = 0;
+    int ev0 = prof_event(s), ev1 = prof_event(s);
+    const long long l0 = g_launches;
+    cudaEventRecord(s->ev_pool[ev0], s->stream);
+    launch_steps(s, nsteps);
+    cudaEventRecord(s->ev_pool[ev1], s->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e) return cuda_fail(s, e, "kernel launch");
+    RG_TRY(cudaMemcpyAsync(h, s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost, s->stream), "ctl download");
+    RG_TRY(cudaStreamSynchronize(s->stream), "step");
+    int err = h->err;
+    float call_ms = 0;
+    cudaEventElapsedTime(&call_ms, s->ev_pool[ev0], s->ev_pool[ev1]);
+    s->last_call_ms = call_ms;
+    s->last_call_launches = g_launches - l0;
+    if (!err) {
+      prof_resolve(s);
+      break;
+    }
+    s->rec_stage.clear(); s->rec_a.clear(); s->rec_b.clear(); s->ev_used = 0;
+    if (err & ERR_TIMEOUT) return fail(s, RG_ERR_TIMEOUT, "a device-side barrier timed out");
+    if (err & ERR_NONFINITE) return fail(s, RG_ERR_NONFINITE, "non-finite body state");
+    if (err & ERR_COLOR) return fail(s, RG_ERR_CAPACITY, "contact graph needs more than 64 colours");
+    // capacity: restore the snapshot, grow, retry
+    RG_TRY(restore_snapshot(s, sn), "restore");
+    if (!grow(s, err)) return fail(s, RG_ERR_CAPACITY, "could not grow device buffers");
+    RG_TRY(take_snapshot(s, sn), "snapshot");
+    reinterpret_cast<Ctl*>(sn.ctl.data())->rebuild = 1;
+    s->contacts_fresh = false;
+    (void)fresh0;
+    if (attempt == 7) return fail(s, RG_ERR_CAPACITY, "capacity retries exhausted");
+  }
+  if (stats) {
+    Ctl* h = s->h_ctl;
+    std::memset(stats, 0, sizeof(*stats));
+    stats->steps = nsteps;
+    stats->contacts = h->contacts;
+    stats->collisions = h->collisions;
+    stats->psor_sweeps = h->sweeps_sum;
+    stats->psor_sweeps_last = h->sweeps_last;
+    stats->list_rebuilds = h->rebuilds;
+    stats->colors = h->colors;
+    stats->history_size = h->hist_n;
+    stats->residual = h->residual;
+    stats->jn_sum = h->jn_sum;
+    stats->jt_sum = h->jt_sum;
+    stats->potential_energy = h->pe;
+    stats->max_residual = h->max_residual;
+    stats->not_converged = h->not_conv;
+    stats->device_ms = s->last_call_ms;
+    stats->psor_row_sweeps = h->row_sweeps;
+    stats->kernel_launches = s->last_call_launches;
+    // kinetic energy (deterministic two-level sum)
+    double* part = nullptr;
+    const int g = 64;
+    if (cudaMalloc(&part, sizeof(double) * g) == cudaSuccess) {
+      RGL k_ke<<<g, 256, 0, s->stream>>>(s->st, s->d_ctl, part);
+      std::vector<double> hp(g);
+      cudaMemcpyAsync(hp.data(), part, sizeof(double) * g, cudaMemcpyDeviceToHost, s->stream);
+      cudaStreamSynchronize(s->stream);
+      double ke = 0;
+      for (int i = 0; i < g; ++i) ke += hp[i];
+      stats->kinetic_energy = ke;
+      cudaFree(part);
+    }
+  }
+  return RG_OK;
+}
+
+int rg_detect(rg_system* s, double delta, int32_t* pairs, double* geom, double* shift, size_t cap,
+              size_t* n) {
+  if (!s || !n) return RG_ERR_ARG;
+  if (!s->bodies_set || !s->state_set) return fail(s, RG_ERR_STATE, "set bodies and state first");
+  if (delta > s->det.margin) return fail(s, RG_ERR_ARG, "delta exceeds the neighbour-list margin of this model");
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    Ctl* h = s->h_ctl;
+    RG_TRY(cudaMemcpy(h, s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost), "ctl");
+    h->err = 0;
+    RG_TRY(cudaMemcpy(s->d_ctl, h, s->ctl_bytes, cudaMemcpyHostToDevice), "ctl");
+    detect_launch(s, delta, true);
+    RG_TRY(cudaGetLastError(), "detect launch");
+    RG_TRY(cudaMemcpyAsync(h, s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost, s->stream), "ctl");
+    RG_TRY(cudaStreamSynchronize(s->stream), "detect");
+    if (!h->err) break;
+    if (!grow(s, h->err)) return fail(s, RG_ERR_CAPACITY, "could not grow device buffers");
+    force_rebuild(s);
+  }
+  s->contacts_fresh = false;  // the force path must rebuild its CSR
+  const int C = s->h_ctl->contacts;
+  *n = (size_t)C;
+  size_t m = cap < (size_t)C ? cap : (size_t)C;
+  if (m) {
+    std::vector<int> a(m), b(m), t(m);
+    cudaMemcpy(a.data(), s->con.a, sizeof(int) * m, cudaMemcpyDeviceToHost);
+    cudaMemcpy(b.data(), s->con.b, sizeof(int) * m, cudaMemcpyDeviceToHost);
+    cudaMemcpy(t.data(), s->con.type, sizeof(int) * m, cudaMemcpyDeviceToHost);
+    std::vector<double> g(14 * m);
+    for (int k = 0; k < 14; ++k)
+      cudaMemcpy(g.data() + (size_t)k * m, s->con.comp(k), sizeof(double) * m, cudaMemcpyDeviceToHost);
+    for (size_t i = 0; i < m; ++i) {
+      if (pairs) { pairs[2 * i] = a[i]; pairs[2 * i + 1] = b[i]; }
+      if (geom) {
+        double* o = geom + 12 * i;
+        for (int k = 0; k < 9; ++k) o[k] = g[(size_t)k * m + i];
+        o[9] = g[12 * m + i];
+        o[10] = g[13 * m + i];
+        o[11] = (double)t[i];
+      }
+      if (shift)
+        for (int k = 0; k < 3; ++k) shift[3 * i + k] = g[(size_t)(9 + k) * m + i];
+    }
+  }
+  return (size_t)C > cap ? RG_ERR_CAPACITY : RG_OK;
+}
+
+int rg_get_impulses(const rg_system* s, int32_t* pairs, double* lambda, int32_t* color, size_t cap,
+                    size_t* n) {
+  if (!s || !n) return RG_ERR_ARG;
+  int wn = 0;
+  cudaMemcpy(&wn, s->nsc.wn, sizeof(int), cudaMemcpyDeviceToHost);
+  *n = (size_t)wn;
+  size_t m = cap < (size_t)wn ? cap : (size_t)wn;
+  if (m) {
+    std::vector<unsigned long long> k(m);
+    std::vector<double> l(3 * m);
+    std::vector<int> c(m);
+    cudaMemcpy(k.data(), s->nsc.wkey, sizeof(unsigned long long) * m, cudaMemcpyDeviceToHost);
+    for (int j = 0; j < 3; ++j)
+      cudaMemcpy(l.data() + (size_t)j * m, s->nsc.wlam + (size_t)j * s->nsc.wcap, sizeof(double) * m,
+                 cudaMemcpyDeviceToHost);
+    const int* wcol = reinterpret_cast<const int*>(s->nsc.wlam + 3 * (size_t)s->nsc.wcap);
+    cudaMemcpy(c.data(), wcol, sizeof(int) * m, cudaMemcpyDeviceToHost);
+    for (size_t i = 0; i < m; ++i) {
+      if (pairs) { pairs[2 * i] = (int32_t)(k[i] >> 32); pairs[2 * i + 1] = (int32_t)(k[i] & 0xffffffffu); }
+      if (lambda) for (int j = 0; j < 3; ++j) lambda[3 * i + j] = l[(size_t)j * m + i];
+      if (color) color[i] = c[i];
+    }
+  }
+  return (size_t)wn > cap ? RG_ERR_CAPACITY : RG_OK;
+}
+
+int rg_compute_forces(rg_system* s, double* f, double* tau, double* pe) {
+  if (!s) return RG_ERR_ARG;
+  if (!s->bodies_set || !s->state_set) return fail(s, RG_ERR_STATE, "set bodies and state first");
+  if (s->cfg.model != RG_MODEL_HARMONIC && s->cfg.model != RG_MODEL_HERTZ_MINDLIN)
+    return fail(s, RG_ERR_ARG, "force evaluation needs the harmonic or hertz-mindlin model");
+  Snapshot sn;
+  RG_TRY(take_snapshot(s, sn), "snapshot");
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    Ctl* h = s->h_ctl;
+    std::memcpy(h, sn.ctl.data(), s->ctl_bytes);
+    h->err = 0;
+    RG_TRY(cudaMemcpyAsync(s->d_ctl, h, s->ctl_bytes, cudaMemcpyHostToDevice, s->stream), "ctl");
+    clear_forces_launch(s);
+    s->contacts_fresh = false;
+    force_eval_launch(s);
+    RG_TRY(cudaGetLastError(), "force launch");
+    RG_TRY(cudaMemcpyAsync(h, s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost, s->stream), "ctl");
+    RG_TRY(cudaStreamSynchronize(s->stream), "forces");
+    if (!h->err) break;
+    if (h->err & (ERR_TIMEOUT | ERR_NONFINITE | ERR_COLOR)) return fail(s, RG_ERR_CUDA, "force evaluation failed");
+    int err = h->err;
+    RG_TRY(restore_snapshot(s, sn), "restore");
+    if (!grow(s, err)) return fail(s, RG_ERR_CAPACITY, "could not grow device buffers");
+    RG_TRY(take_snapshot(s, sn), "snapshot");
+    reinterpret_cast<Ctl*>(sn.ctl.data())->rebuild = 1;
+  }
+  s->contacts_fresh = true;
+  if (pe) *pe = s->h_ctl->pe;
+  return rg_get_state(s, nullptr, nullptr, nullptr, nullptr, f, tau);
+}
+
+int rg_set_profiling(rg_system* s, int enable) {
+  if (!s) return RG_ERR_ARG;
+  s->prof_on = enable != 0;
+  for (int k = 0; k < 8; ++k) { s->prof_ms[k] = 0; s->prof_cnt[k] = 0; }
+  return RG_OK;
+}
+
+int rg_get_profile(const rg_system* s, double* ms, int64_t* launches) {
+  if (!s) return RG_ERR_ARG;
+  for (int k = 0; k < 8; ++k) {
+    if (ms) ms[k] = s->prof_ms[k];
+    if (launches) launches[k] = s->prof_cnt[k];
+  }
+  return RG_OK;
+}
+
+int rg_get_history(const rg_system* s, int32_t* pairs, double* value, int64_t* last_frame, size_t cap,
+                   size_t* n) {
+  if (!s || !n) return RG_ERR_ARG;
+  Ctl h;
+  cudaMemcpy(&h, s->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost);
+  const History& H = s->hist;
+  int hn = h.hist_n;
+  *n = (size_t)hn;
+  size_t m = cap < (size_t)hn ? cap : (size_t)hn;
+  if (m) {
+    std::vector<unsigned long long> k(m);
+    std::vector<double> v(3 * m);
+    std::vector<long long> fr(m);
+    cudaMemcpy(k.data(), H.key[H.cur], sizeof(unsigned long long) * m, cudaMemcpyDeviceToHost);
+    for (int j = 0; j < 3; ++j)
+      cudaMemcpy(v.data() + (size_t)j * m, H.val[H.cur] + (size_t)j * H.cap, sizeof(double) * m,
+                 cudaMemcpyDeviceToHost);
+    cudaMemcpy(fr.data(), H.frame[H.cur], sizeof(long long) * m, cudaMemcpyDeviceToHost);
+    for (size_t i = 0; i < m; ++i) {
+      if (pairs) { pairs[2 * i] = (int32_t)(k[i] >> 32); pairs[2 * i + 1] = (int32_t)(k[i] & 0xffffffffu); }
+      if (value) for (int j = 0; j < 3; ++j) value[3 * i + j] = v[(size_t)j * m + i];
+      if (last_frame) last_frame[i] = fr[i];
+    }
+  }
+  return (size_t)hn > cap ? RG_ERR_CAPACITY : RG_OK;
+}
+
+}  // extern "C"

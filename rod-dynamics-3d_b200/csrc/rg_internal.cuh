@@ -1,0 +1,266 @@
+// rg_internal.cuh - host-side layout of an rg_system and the launch helpers
+// each .cu file provides.  Not part of the public ABI (include/rodgpu.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rg_common.cuh"
+
+namespace rg {
+
+// Exclusive scan of int32 counts: out[0..n] with out[n] = total, n read
+// from the device (n_dev) so launches do not depend on host-known sizes.
+struct Scan {
+  int cap = 0;
+  int* d_blocks = nullptr;  // per-block totals
+  cudaError_t alloc(int cap_);
+  void free_();
+  void run(const int* in, int* out, const int* n_dev, cudaStream_t s) const;
+};
+
+// Device-resident control words of one system (one cudaMalloc).
+struct Ctl {
+  int err;              // error bits
+  int rebuild;          // 1: neighbour list must be rebuilt before next use
+  int contacts;         // contacts of the last detection
+  int hist_n;           // live history entries (current table)
+  int hist_touched;     // scratch
+  int colors;           // colours of the last colouring
+  int proj_active;      // projection rows active in the current pass
+  int sweeps_last;      // PSOR sweeps of the last solve
+  double maxdisp;       // max displacement since the last list build
+  double residual;      // last PSOR residual
+  long long frame;      // force-evaluation counter (HM / Cundall frames)
+  long long rebuilds;   // list rebuilds (cumulative)
+  long long sweeps_sum; // PSOR sweeps (cumulative)
+  long long not_conv;   // steps whose PSOR stopped at max sweeps
+  double max_residual;  // worst final residual (cumulative)
+  long long collisions; // NSC impacts of the last step
+  double jn_sum, jt_sum, pe;
+  long long row_sweeps; // Σ contacts x sweeps (cumulative)
+  int rec_n;            // MLP records stored
+  int pad;
+  unsigned int bar_count, bar_gen;  // grid barrier
+  double res_sweep[1];  // per-sweep residual slots follow (velocity_iters)
+};
+
+struct Contacts {  // sorted by (a,b)
+  int cap = 0;
+  int *a = nullptr, *b = nullptr, *type = nullptr;
+  double* g = nullptr;  // 14 component arrays of cap: pa(3) pb(3) n(3) sh(3) dist surf
+  cudaError_t alloc(int cap_);
+  void free_();
+  __host__ __device__ double* comp(int k) const { return g + (size_t)k * cap; }
+};
+
+struct Detector {
+  int maxnb = 0;
+  int* nbr_cnt = nullptr;   // n
+  int* nbr = nullptr;       // n * maxnb (j > i, ascending)
+  double* ref = nullptr;    // 6n: x_ref(3n), u_ref(3n)
+  Seg* seg = nullptr;       // n
+  int ncell[3] = {1, 1, 1};
+  int ncells = 1;
+  double cell[3] = {1, 1, 1};
+  int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr,
+      *cell_rods = nullptr;
+  int* hit_cnt = nullptr;         // n+1
+  int* hit_off = nullptr;         // n+1
+  unsigned long long* hit_mask = nullptr;  // n * words
+  int mask_words = 1;
+  double skin = 0, margin = 0;    // skin and the largest activation margin
+  double cut_center = 0;          // centre-distance cutoff for list building
+  bool all_pairs = false;         // tiny periodic box: scan every cell
+};
+
+struct BodyCSR {  // contacts incident to each body, in contact order
+  int* cnt = nullptr;   // n+1
+  int* off = nullptr;   // n+1
+  int* fill = nullptr;  // n
+  int* ent = nullptr;   // 2*ccap: 2c (side a) or 2c+1 (side b)
+};
+
+struct History {  // sorted by key (a<<32|b)
+  int cap = 0;
+  unsigned long long* key[2] = {nullptr, nullptr};
+  double* val[2] = {nullptr, nullptr};       // 3 * cap each (SoA)
+  long long* frame[2] = {nullptr, nullptr};
+  int cur = 0;
+  int* found = nullptr;        // ccap: index into current table or -1
+  int* touched = nullptr;      // ccap+1 flags -> scan
+  int* touched_off = nullptr;  // ccap+1
+  int* kept = nullptr;         // cap+1
+  int* kept_off = nullptr;     // cap+1
+  double* newval = nullptr;    // 3*ccap
+};
+
+struct Nsc {
+  // manifold rows, SoA, ccap each
+  double* row = nullptr;  // kRowComps * ccap
+  double* lam = nullptr;  // 3*ccap (λn, λt1, λt2)
+  int* color = nullptr;   // ccap
+  int* color_tmp = nullptr;
+  int* order = nullptr;   // colour-major contact order
+  int* color_cnt = nullptr;   // kMaxColors+1
+  int* color_off = nullptr;   // kMaxColors+1
+  // warm cache: previous step's sorted keys and impulses
+  unsigned long long* wkey = nullptr;
+  double* wlam = nullptr;
+  int* wn = nullptr;  // device count of the warm cache
+  int wcap = 0;
+  // projection scratch
+  double* dx = nullptr;   // 6n: dx(3n), dθ(3n)
+  double* prow = nullptr; // kPosComps * ccap
+  int* pactive = nullptr; // ccap
+};
+constexpr int kRowComps = 42;
+constexpr int kPosComps = 12;
+
+}  // namespace rg
+
+struct rg_system {
+  rg_config cfg;
+  int n = 0;
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  std::string err_text;
+  bool bodies_set = false, state_set = false;
+  bool contacts_fresh = false;  // contacts match the current positions
+
+  double* d_state = nullptr;  // 19 n
+  double* d_props = nullptr;  // 11 n
+  rg::State st;
+  rg::Box box;
+  rg::Ctl* d_ctl = nullptr;
+  rg::Ctl* h_ctl = nullptr;   // pinned mirror
+  size_t ctl_bytes = 0;
+
+  int ccap = 0;
+  rg::Contacts con;
+  rg::Detector det;
+  rg::BodyCSR csr;
+  rg::History hist;
+  rg::Nsc nsc;
+  rg::Scan scan;
+  double* d_cf = nullptr;     // per-contact force/torque addends, 12 * ccap
+
+  // snapshot for capacity retry: state, current history table, warm cache
+  double* d_snap = nullptr;
+  unsigned long long* snap_hkey = nullptr;
+  double* snap_hval = nullptr;
+  long long* snap_hframe = nullptr;
+  int snap_hcap = 0;
+  unsigned long long* snap_wkey = nullptr;
+  double* snap_wlam = nullptr;  // 3*wcap doubles + wcap ints (colours)
+  int snap_wcap = 0;
+
+  // MLP (learned warm start)
+  float* d_mlp = nullptr;
+  size_t mlp_n = 0;
+  bool mlp_ready = false;
+  bool recording = false;
+  int rec_cap = 0;
+  float* d_rec_x = nullptr;
+  float* d_rec_y = nullptr;
+  float* d_feat = nullptr;    // 8 * ccap scratch
+  float* d_pred = nullptr;    // 3 * ccap scratch
+
+  int coop_blocks = 0;        // co-resident blocks for the persistent kernels
+  cudaGraphExec_t graph = nullptr;
+  int graph_kind = -1;
+
+  // pinned staging for host <-> device state copies (19 n doubles)
+  double* h_stage = nullptr;
+  double last_call_ms = 0;
+  long long last_call_launches = 0;
+
+  // stage timers
+  bool prof_on = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<int> rec_stage, rec_a, rec_b;
+  double prof_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long long prof_cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+namespace rg {
+// Kernel launches issued by this library (all systems), for run statistics.
+extern long long g_launches;
+#define RGL ++::rg::g_launches;
+
+enum Stage { ST_INTEGRATE = 0, ST_DETECT, ST_COLOR, ST_MANIFOLDS, ST_PSOR, ST_PROJECT, ST_FORCES, ST_OTHER };
+
+inline int prof_event(rg_system* s) {
+  if (s->ev_used == s->ev_pool.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    s->ev_pool.push_back(e);
+  }
+  return (int)s->ev_used++;
+}
+// Records CUDA events around a group of launches of one stage.
+struct ProfScope {
+  rg_system* s;
+  int stage, a;
+  ProfScope(rg_system* s_, int st) : s(s_), stage(st), a(-1) {
+    if (!s->prof_on) return;
+    a = prof_event(s);
+    cudaEventRecord(s->ev_pool[a], s->stream);
+  }
+  ~ProfScope() { end(); }
+  void end() {
+    if (a < 0) return;
+    int b = prof_event(s);
+    cudaEventRecord(s->ev_pool[b], s->stream);
+    s->rec_stage.push_back(stage);
+    s->rec_a.push_back(a);
+    s->rec_b.push_back(b);
+    a = -1;
+  }
+};
+// Folds recorded event pairs into the accumulators (after a stream sync).
+inline void prof_resolve(rg_system* s) {
+  for (size_t i = 0; i < s->rec_stage.size(); ++i) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, s->ev_pool[s->rec_a[i]], s->ev_pool[s->rec_b[i]]);
+    s->prof_ms[s->rec_stage[i]] += ms;
+    s->prof_cnt[s->rec_stage[i]] += 1;
+  }
+  s->rec_stage.clear();
+  s->rec_a.clear();
+  s->rec_b.clear();
+  s->ev_used = 0;
+}
+
+// rg_detect.cu
+cudaError_t detector_alloc(rg_system* s);
+void detector_free(rg_system* s);
+void detect_launch(rg_system* s, double delta, bool check_rebuild);
+void force_rebuild(rg_system* s);
+// rg_forces.cu
+void force_eval_launch(rg_system* s);  // detect (unless fresh) + forces into f, tau
+void csr_launch(rg_system* s);         // body CSR of the current contacts
+// rg_integrate.cu
+void half_pos_launch(rg_system* s);
+void second_half_launch(rg_system* s);
+void clear_forces_launch(rg_system* s);
+void nsc_free_flight_launch(rg_system* s);
+void nsc_position_update_launch(rg_system* s);
+void wrap_launch(rg_system* s);
+// rg_nsc.cu
+void nsc_step_launch(rg_system* s);
+void color_launch(rg_system* s);
+// rg_mlp.cu
+void mlp_warm_launch(rg_system* s);
+void mlp_record_launch(rg_system* s);
+// launch geometry helper
+inline int grid_for(long long n, int bs, int maxb = 148 * 16) {
+  long long g = (n + bs - 1) / bs;
+  if (g < 1) g = 1;
+  if (g > maxb) g = maxb;
+  return (int)g;
+}
+}  // namespace rg

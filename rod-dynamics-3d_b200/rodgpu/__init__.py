@@ -1,0 +1,278 @@
+"""ctypes binding of librodgpu.so, the B200 contact hot path.
+
+This is the thin Python edge over the C ABI declared in include/rodgpu.h.
+It holds no physics: every step, detection and force evaluation runs in the
+CUDA library, which must be loadable (there is no CPU fallback; a missing or
+unloadable library raises at import of the first System).
+
+Arrays are numpy float64 in the ABI's layouts: x (N,3), q (N,4) as
+(w,x,y,z), v (N,3), w (N,3).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "librodgpu.so")
+HOST_PATH = os.path.join(PKG, "librodhost.so")
+
+MODEL = {"none": 0, "nsc": 1, "harmonic": 2, "hertz-mindlin": 3}
+FRICTION = {"smooth": 0, "cundall": 1, "karnopp": 2}
+WARM = {"cache": 0, "none": 1, "mlp": 2}
+STATUS = ["ok", "bad argument", "CUDA error", "capacity exceeded", "non-finite state",
+          "PSOR not converged", "no CUDA device", "device wait timed out", "call out of order"]
+
+_d = ctypes.c_double
+_i = ctypes.c_int32
+
+
+class RgConfig(ctypes.Structure):
+    """Mirror of struct rg_config (include/rodgpu.h)."""
+    _fields_ = [
+        ("n_bodies", _i), ("model", _i), ("dt", _d), ("gravity", _d * 3),
+        ("lin_damp", _d), ("ang_damp", _d), ("w_max", _d),
+        ("pbc_enabled", _i), ("pbc_min", _d * 3), ("pbc_max", _d * 3),
+        ("soft_delta", _d), ("soft_k_scaler", _d), ("soft_damping", _d), ("soft_mu", _d),
+        ("soft_mu_static", _d), ("soft_nu", _d), ("soft_kt", _d), ("soft_vel_deadband", _d),
+        ("soft_enable_friction", _i), ("soft_friction_mode", _i),
+        ("hm_youngs_modulus", _d), ("hm_poisson_ratio", _d), ("hm_restitution", _d),
+        ("hm_friction", _d), ("hm_friction_static", _d), ("hm_friction_transition_vel", _d),
+        ("hm_rolling_friction", _d), ("hm_enable_tangential", _i), ("hm_enable_rolling", _i),
+        ("nsc_mu", _d), ("nsc_beta", _d), ("nsc_cfm", _d), ("nsc_omega", _d), ("nsc_slop", _d),
+        ("nsc_tol", _d), ("nsc_velocity_iters", _i), ("nsc_position_stabilization", _i),
+        ("nsc_position_iters", _i), ("nsc_position_psor_iters", _i), ("nsc_warm_start", _i),
+        ("psor_order", _i), ("skin", _d), ("max_neighbors", _i), ("reserved", _i * 7),
+    ]
+
+
+class RgStepStats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int64), ("contacts", ctypes.c_int64), ("collisions", ctypes.c_int64),
+        ("psor_sweeps", ctypes.c_int64), ("psor_sweeps_last", ctypes.c_int64),
+        ("list_rebuilds", ctypes.c_int64), ("colors", ctypes.c_int64),
+        ("history_size", ctypes.c_int64), ("residual", _d), ("jn_sum", _d), ("jt_sum", _d),
+        ("potential_energy", _d), ("kinetic_energy", _d), ("max_residual", _d),
+        ("not_converged", ctypes.c_int64), ("device_ms", _d), ("psor_row_sweeps", ctypes.c_int64),
+        ("kernel_launches", ctypes.c_int64), ("reserved", ctypes.c_int64 * 3),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_lib = None
+_host = None
+
+# Every entry point of include/rodgpu.h, in declaration order.
+ABI_SYMBOLS = [
+    "rg_abi_version", "rg_config_default", "rg_status_string", "rg_last_error", "rg_create",
+    "rg_destroy", "rg_get_config", "rg_set_bodies", "rg_set_state", "rg_get_state", "rg_step",
+    "rg_detect", "rg_get_impulses", "rg_compute_forces", "rg_get_history", "rg_set_profiling",
+    "rg_get_profile",
+    "rg_mlp_param_count", "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_record",
+    "rg_mlp_records", "rg_mlp_train", "rg_mlp_infer", "rg_batch_create", "rg_batch_destroy",
+    "rg_batch_set_bodies", "rg_batch_set_state", "rg_batch_get_state", "rg_batch_step",
+    "rg_batch_set_mlp",
+]
+
+
+def lib():
+    """Loads librodgpu.so (raises if it is missing: no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"librodgpu.so not built ({LIB_PATH}); run rod-dynamics-3d_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        dp = ctypes.POINTER(_d)
+        L.rg_config_default.argtypes = [ctypes.POINTER(RgConfig)]
+        L.rg_config_default.restype = None
+        L.rg_status_string.restype = ctypes.c_char_p
+        L.rg_last_error.argtypes = [P]
+        L.rg_last_error.restype = ctypes.c_char_p
+        L.rg_create.argtypes = [ctypes.POINTER(RgConfig), ctypes.POINTER(P)]
+        L.rg_destroy.argtypes = [P]
+        L.rg_set_bodies.argtypes = [P, dp, dp, dp, dp, dp]
+        L.rg_set_state.argtypes = [P, dp, dp, dp, dp, dp, dp]
+        L.rg_get_state.argtypes = [P, dp, dp, dp, dp, dp, dp]
+        L.rg_step.argtypes = [P, ctypes.c_int, ctypes.POINTER(RgStepStats)]
+        L.rg_detect.argtypes = [P, _d, ctypes.POINTER(_i), dp, dp, ctypes.c_size_t,
+                                ctypes.POINTER(ctypes.c_size_t)]
+        L.rg_get_impulses.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.POINTER(_i),
+                                      ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+        L.rg_compute_forces.argtypes = [P, dp, dp, dp]
+        L.rg_get_history.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.POINTER(ctypes.c_int64),
+                                     ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+        L.rg_set_profiling.argtypes = [P, ctypes.c_int]
+        L.rg_get_profile.argtypes = [P, dp, ctypes.POINTER(ctypes.c_int64)]
+        L.rg_mlp_param_count.restype = ctypes.c_size_t
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.rg_mlp_set_params.argtypes = [P, fp, ctypes.c_size_t]
+        L.rg_mlp_get_params.argtypes = [P, fp, ctypes.c_size_t]
+        L.rg_mlp_record.argtypes = [P, ctypes.c_int, ctypes.c_size_t]
+        L.rg_mlp_records.argtypes = [P, fp, fp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+        L.rg_mlp_train.argtypes = [P, fp, fp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_float, ctypes.c_uint64, fp]
+        L.rg_mlp_infer.argtypes = [P, fp, fp, ctypes.c_size_t]
+        _lib = L
+    return _lib
+
+
+def host():
+    """Loads librodhost.so (scene generator, mass properties)."""
+    global _host
+    if _host is None:
+        H = ctypes.CDLL(HOST_PATH)
+        dp = ctypes.POINTER(_d)
+        H.rg_capsule_mass.argtypes = [ctypes.c_int, dp, dp, dp, dp, dp]
+        H.rg_capsule_mass.restype = None
+        H.rg_scene_rsa.argtypes = [ctypes.c_int, _d, _d, _d, _d, ctypes.c_uint64, ctypes.c_int, dp, dp]
+        H.rg_scene_rsa.restype = ctypes.c_int
+        H.rg_scene_velocities.argtypes = [ctypes.c_int, _d, _d, ctypes.c_uint64, dp, dp]
+        H.rg_scene_velocities.restype = None
+        _host = H
+    return _host
+
+
+def ptr(a, ctype=_d):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def default_config(**kw):
+    """rg_config_default() with keyword overrides (model accepts a name)."""
+    c = RgConfig()
+    lib().rg_config_default(ctypes.byref(c))
+    return apply_config(c, **kw)
+
+
+def apply_config(c, **kw):
+    for k, v in kw.items():
+        if k == "model" and isinstance(v, str):
+            v = MODEL[v]
+        if k == "soft_friction_mode" and isinstance(v, str):
+            v = FRICTION[v]
+        if k == "nsc_warm_start" and isinstance(v, str):
+            v = WARM[v]
+        if k in ("gravity", "pbc_min", "pbc_max"):
+            arr = getattr(c, k)
+            for j in range(3):
+                arr[j] = float(v[j])
+            continue
+        setattr(c, k, v)
+    return c
+
+
+class RgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS[code] if 0 <= code < len(STATUS) else code}: {msg}")
+        self.code = code
+
+
+class System:
+    """One rg_system: device state of N capsules advanced by librodgpu."""
+
+    def __init__(self, cfg):
+        self._lib = lib()
+        self.cfg = cfg
+        self.n = cfg.n_bodies
+        h = ctypes.c_void_p()
+        rc = self._lib.rg_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != 0:
+            raise RgError(rc, "rg_create failed")
+        self._h = h
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = self._lib.rg_last_error(self._h)
+            raise RgError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_bodies(self, radius, half_height, mass, inertia, restitution=None):
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (radius, half_height, mass, inertia)]
+        rest = None if restitution is None else np.ascontiguousarray(restitution, dtype=np.float64)
+        self._keep = args + [rest]
+        self._check(self._lib.rg_set_bodies(self._h, *[ptr(a) for a in args], ptr(rest)), "set_bodies")
+
+    def set_state(self, x, q, v, w, f=None, tau=None):
+        arr = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (x, q, v, w, f, tau)]
+        self._check(self._lib.rg_set_state(self._h, *[ptr(a) for a in arr]), "set_state")
+
+    def get_state(self):
+        n = self.n
+        x, v, w, f, t = (np.zeros((n, 3)) for _ in range(5))
+        q = np.zeros((n, 4))
+        self._check(self._lib.rg_get_state(self._h, ptr(x), ptr(q), ptr(v), ptr(w), ptr(f), ptr(t)), "get_state")
+        return {"x": x, "q": q, "v": v, "w": w, "f": f, "tau": t}
+
+    def step(self, nsteps=1):
+        st = RgStepStats()
+        self._check(self._lib.rg_step(self._h, int(nsteps), ctypes.byref(st)), "step")
+        return st.as_dict()
+
+    def detect(self, delta=0.0):
+        n = ctypes.c_size_t()
+        self._lib.rg_detect(self._h, delta, None, None, None, 0, ctypes.byref(n))
+        cap = max(1, n.value)
+        pairs = np.zeros((cap, 2), np.int32)
+        geom = np.zeros((cap, 12))
+        shift = np.zeros((cap, 3))
+        self._check(self._lib.rg_detect(self._h, delta, ptr(pairs, _i), ptr(geom), ptr(shift), cap,
+                                        ctypes.byref(n)), "detect")
+        m = n.value
+        return pairs[:m], geom[:m], shift[:m]
+
+    def impulses(self):
+        n = ctypes.c_size_t()
+        self._lib.rg_get_impulses(self._h, None, None, None, 0, ctypes.byref(n))
+        cap = max(1, n.value)
+        pairs = np.zeros((cap, 2), np.int32)
+        lam = np.zeros((cap, 3))
+        col = np.zeros(cap, np.int32)
+        self._check(self._lib.rg_get_impulses(self._h, ptr(pairs, _i), ptr(lam), ptr(col, _i), cap,
+                                              ctypes.byref(n)), "impulses")
+        m = n.value
+        return pairs[:m], lam[:m], col[:m]
+
+    def compute_forces(self):
+        f = np.zeros((self.n, 3))
+        t = np.zeros((self.n, 3))
+        pe = ctypes.c_double()
+        self._check(self._lib.rg_compute_forces(self._h, ptr(f), ptr(t), ctypes.byref(pe)), "compute_forces")
+        return f, t, pe.value
+
+    STAGES = ["integrate", "detect", "color", "manifolds", "psor", "project", "forces", "other"]
+
+    def set_profiling(self, on=True):
+        self._check(self._lib.rg_set_profiling(self._h, int(on)), "set_profiling")
+
+    def profile(self):
+        ms = np.zeros(8)
+        cnt = np.zeros(8, np.int64)
+        self._check(self._lib.rg_get_profile(self._h, ptr(ms), ptr(cnt, ctypes.c_int64)), "profile")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.STAGES)}
+
+    def history(self):
+        n = ctypes.c_size_t()
+        self._lib.rg_get_history(self._h, None, None, None, 0, ctypes.byref(n))
+        cap = max(1, n.value)
+        pairs = np.zeros((cap, 2), np.int32)
+        val = np.zeros((cap, 3))
+        fr = np.zeros(cap, np.int64)
+        self._check(self._lib.rg_get_history(self._h, ptr(pairs, _i), ptr(val), ptr(fr, ctypes.c_int64),
+                                             cap, ctypes.byref(n)), "history")
+        m = n.value
+        return pairs[:m], val[:m], fr[:m]

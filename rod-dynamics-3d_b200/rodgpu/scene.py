@@ -1,0 +1,109 @@
+"""Seeded synthetic rod packings and the five benchmark workloads.
+
+The packings come from the host C++ generator (host/scene_gen.cpp): random
+sequential addition in a periodic cube with overlap rejection, isotropic
+axes, Gaussian velocities.  Box sides follow the capsule volume
+V = pi r^2 L + 4/3 pi r^3 used by the reference's broad-phase benchmark
+(src/tools/benchmark_broadphase.cpp:104-106).
+
+Workloads (rod counts and physics as stated; values the description leaves
+open are fixed here and documented in DESIGN.md):
+  hm_small    N=1000,  L=1, d=0.1,  phi=0.10, Hertz-Mindlin E=1e5 nu=0.3 e=0.5
+              mu=0.5, dt=1e-4, 1000 steps
+  nsc_dense   N=20000, L=1, d=0.05, phi=0.20, PSOR mu=0.3, omega=1, tol 1e-6,
+              500 sweeps max, dt=5e-4, 500 steps, no gravity
+  nsc_large   N=50000, same rods, mu ~ U[0.1, 0.8] per run
+  hm_large    N=1e6,   L=1, d=0.02, phi=0.15, Hertz-Mindlin E=1e6 nu=0.3 e=0.3
+              mu=0.5, dt=2e-5, 100 steps
+Damping is zero and gravity is off in every workload.
+"""
+import math
+
+import numpy as np
+
+from . import host, ptr, default_config
+
+
+def capsule_volume(L, d):
+    r = 0.5 * d
+    return math.pi * r * r * L + 4.0 / 3.0 * math.pi * r ** 3
+
+
+def box_side(n, L, d, phi):
+    return (n * capsule_volume(L, d) / phi) ** (1.0 / 3.0)
+
+
+def make_rods(n, L, d, phi=None, side=None, seed=1, sigma_v=0.1, sigma_w=0.1, density=1.0,
+              restitution=0.2, max_attempts=2000):
+    """RSA packing of n rods; returns a dict of body and state arrays.
+
+    'placed' may be below n when the packing jams; arrays are trimmed to it.
+    """
+    if side is None:
+        side = box_side(n, L, d, phi)
+    lo = -0.5 * side
+    H = host()
+    x = np.zeros((n, 3))
+    q = np.zeros((n, 4))
+    placed = H.rg_scene_rsa(int(n), float(L), float(d), float(lo), float(side), int(seed),
+                            int(max_attempts), ptr(x), ptr(q))
+    m = placed
+    x, q = x[:m].copy(), q[:m].copy()
+    v = np.zeros((m, 3))
+    w = np.zeros((m, 3))
+    H.rg_scene_velocities(int(m), float(sigma_v), float(sigma_w), int(seed), ptr(v), ptr(w))
+    radius = np.full(m, 0.5 * d)
+    half = np.full(m, 0.5 * L)
+    dens = np.full(m, float(density))
+    mass = np.zeros(m)
+    inertia = np.zeros((m, 3))
+    H.rg_capsule_mass(int(m), ptr(radius), ptr(half), ptr(dens), ptr(mass), ptr(inertia))
+    phi_ach = m * capsule_volume(L, d) / side ** 3
+    return {"n": m, "requested": n, "L": L, "d": d, "side": side, "lo": lo, "phi": phi_ach,
+            "radius": radius, "half_height": half, "mass": mass, "inertia": inertia,
+            "restitution": np.full(m, float(restitution)), "x": x, "q": q, "v": v, "w": w}
+
+
+def pbc_kwargs(scene):
+    lo, side = scene["lo"], scene["side"]
+    return {"pbc_enabled": 1, "pbc_min": (lo, lo, lo), "pbc_max": (lo + side, lo + side, lo + side)}
+
+
+WORKLOADS = {
+    "hm_small": dict(n=1000, L=1.0, d=0.1, phi=0.10, steps=1000,
+                     cfg=dict(model="hertz-mindlin", dt=1e-4, hm_youngs_modulus=1e5,
+                              hm_poisson_ratio=0.3, hm_restitution=0.5, hm_friction=0.5)),
+    "nsc_dense": dict(n=20000, L=1.0, d=0.05, phi=0.20, steps=500,
+                      cfg=dict(model="nsc", dt=5e-4, nsc_mu=0.3, nsc_omega=1.0, nsc_tol=1e-6,
+                               nsc_velocity_iters=500)),
+    "nsc_large": dict(n=50000, L=1.0, d=0.05, phi=0.20, steps=200,
+                      cfg=dict(model="nsc", dt=5e-4, nsc_mu=0.3, nsc_omega=1.0, nsc_tol=1e-6,
+                               nsc_velocity_iters=500)),
+    "hm_large": dict(n=1000000, L=1.0, d=0.02, phi=0.15, steps=100,
+                     cfg=dict(model="hertz-mindlin", dt=2e-5, hm_youngs_modulus=1e6,
+                              hm_poisson_ratio=0.3, hm_restitution=0.3, hm_friction=0.5)),
+}
+
+
+def workload(name, n=None, seed=1, **overrides):
+    """(config, scene) for a named workload; n overrides the rod count."""
+    w = WORKLOADS[name]
+    nn = w["n"] if n is None else n
+    sc = make_rods(nn, w["L"], w["d"], phi=w["phi"], seed=seed)
+    kw = dict(w["cfg"])
+    kw.update(gravity=(0.0, 0.0, 0.0), lin_damp=0.0, ang_damp=0.0)
+    kw.update(pbc_kwargs(sc))
+    kw.update(overrides)
+    cfg = default_config(n_bodies=sc["n"], **kw)
+    return cfg, sc
+
+
+def config_dict(cfg):
+    """rg_config as a plain dict (for the oracle and for fixtures)."""
+    out = {}
+    for k, _ in type(cfg)._fields_:
+        v = getattr(cfg, k)
+        if hasattr(v, "__len__"):
+            v = list(v)
+        out[k] = v
+    return out

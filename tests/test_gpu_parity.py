@@ -1,0 +1,168 @@
+"""GPU parity: librodgpu (through the C ABI) against the FP64 oracle.
+
+Bars:
+  * contact pair lists, minimum-image shifts and contact types: bit-exact;
+  * contact geometry (closest points, normal, distance): bit-exact (both
+    sides evaluate the same FP64 expressions without FMA contraction);
+  * forces, torques, impulses and states: relative error <= 1e-10 of the
+    array's largest magnitude (FP64; transcendental functions differ by a
+    few ulp between CUDA and glibc, nothing else does).
+"""
+import numpy as np
+import pytest
+
+from helpers import make_pair, packed_scene, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def assert_contacts_equal(g, o, delta):
+    pg, gg, sg = g.detect(delta)
+    po, go, so = o.detect(delta)
+    assert len(po) > 0
+    np.testing.assert_array_equal(pg, po)
+    np.testing.assert_array_equal(sg, so)
+    np.testing.assert_array_equal(gg, go)  # points, normal, distance, surface, type
+    return len(po)
+
+
+@pytest.mark.parametrize("n,d,phi,seed", [(1000, 0.1, 0.10, 1), (3000, 0.05, 0.2, 2), (500, 0.2, 0.15, 3)])
+def test_detect_bit_exact_nsc(n, d, phi, seed):
+    sc = packed_scene(n, d=d, phi=phi, seed=seed)
+    g, o = make_pair(sc, model="nsc")
+    assert_contacts_equal(g, o, 0.0)
+
+
+def test_detect_bit_exact_soft_margin():
+    sc = packed_scene(1500, d=0.1, phi=0.1, seed=4, squeeze=0.95)
+    g, o = make_pair(sc, model="harmonic")
+    assert_contacts_equal(g, o, 0.005)
+
+
+def test_detect_open_box():
+    sc = packed_scene(800, d=0.1, phi=0.1, seed=5)
+    g, o = make_pair(sc, model="nsc", pbc_enabled=0)
+    assert_contacts_equal(g, o, 0.0)
+
+
+def test_detect_tiny_periodic_box():
+    # box smaller than twice the rod length: every pair is listed
+    sc = packed_scene(40, L=1.0, d=0.1, phi=0.02, seed=6, squeeze=0.7)
+    g, o = make_pair(sc, model="nsc")
+    pg, gg, _ = g.detect(0.0)
+    po, go, _ = o.detect(0.0)
+    np.testing.assert_array_equal(pg, po)
+    np.testing.assert_array_equal(gg, go)
+
+
+def test_neighbor_list_overflow_grows():
+    sc = packed_scene(1000, d=0.1, phi=0.1, seed=7)
+    g, o = make_pair(sc, model="nsc", max_neighbors=2)
+    assert_contacts_equal(g, o, 0.0)
+
+
+@pytest.mark.parametrize("mode", ["smooth", "cundall", "karnopp"])
+def test_soft_forces(mode):
+    sc = packed_scene(1200, d=0.1, phi=0.1, seed=8, squeeze=0.9)
+    g, o = make_pair(sc, model="harmonic", dt=1e-4, soft_friction_mode=mode, soft_damping=0.5,
+                     soft_mu_static=0.8 if mode != "cundall" else 0.0)
+    for _ in range(3):
+        fg, tg, peg = g.compute_forces()
+        fo, to, peo = o.compute_forces()
+        assert rel_err(fg, fo) < TOL
+        assert rel_err(tg, to) < TOL
+        assert abs(peg - peo) <= TOL * abs(peo)
+    if mode == "cundall":
+        pg, vg, frg = g.history()
+        po, vo, fro = o.history()
+        np.testing.assert_array_equal(pg, po)
+        np.testing.assert_array_equal(frg, fro)
+        assert rel_err(vg, vo) < TOL
+
+
+def test_hertz_mindlin_forces_and_history():
+    sc = packed_scene(1200, d=0.1, phi=0.1, seed=9, squeeze=0.97)
+    g, o = make_pair(sc, model="hertz-mindlin", dt=1e-4, hm_youngs_modulus=1e5, hm_poisson_ratio=0.3,
+                     hm_restitution=0.5, hm_friction=0.5)
+    for _ in range(3):
+        fg, tg, peg = g.compute_forces()
+        fo, to, peo = o.compute_forces()
+        assert rel_err(fg, fo) < TOL
+        assert rel_err(tg, to) < TOL
+        assert abs(peg - peo) <= TOL * abs(peo)
+    pg, vg, frg = g.history()
+    po, vo, fro = o.history()
+    assert len(po) > 0
+    np.testing.assert_array_equal(pg, po)
+    np.testing.assert_array_equal(frg, fro)
+    assert rel_err(vg, vo) < TOL
+
+
+@pytest.mark.parametrize("model", ["hertz-mindlin", "harmonic"])
+def test_verlet_steps(model):
+    sc = packed_scene(1000, d=0.1, phi=0.1, seed=10, squeeze=0.97)
+    kw = dict(dt=1e-4)
+    if model == "hertz-mindlin":
+        kw.update(hm_youngs_modulus=1e5, hm_poisson_ratio=0.3, hm_restitution=0.5, hm_friction=0.5)
+    else:
+        kw.update(soft_friction_mode="cundall")
+    g, o = make_pair(sc, model=model, **kw)
+    for chunk in (1, 4, 10):
+        sg = g.step(chunk)
+        so = o.step(chunk)
+        a, b = g.get_state(), o.get_state()
+        for k in ("x", "q", "v", "w"):
+            assert rel_err(a[k], b[k]) < TOL, k
+        assert sg["contacts"] == so["contacts"]
+        assert sg["history_size"] == so["history_size"]
+        assert abs(sg["potential_energy"] - so["potential_energy"]) <= 1e-9 * max(1.0, abs(so["potential_energy"]))
+    assert_contacts_equal(g, o, 0.0 if model == "hertz-mindlin" else 0.005)
+
+
+def test_nsc_one_step_impulses_and_colors():
+    sc = packed_scene(1500, d=0.1, phi=0.1, seed=11, squeeze=0.97)
+    g, o = make_pair(sc, model="nsc", dt=5e-4, nsc_velocity_iters=200)
+    sg = g.step(1)
+    so = o.step(1)
+    pg, lg, cg = g.impulses()
+    po, lo, co = o.impulses()
+    assert len(po) > 0
+    np.testing.assert_array_equal(pg, po)
+    np.testing.assert_array_equal(cg, co)
+    assert rel_err(lg, lo) < TOL
+    assert sg["psor_sweeps"] == so["psor_sweeps"]
+    assert sg["colors"] == so["colors"]
+    a, b = g.get_state(), o.get_state()
+    for k in ("x", "q", "v", "w"):
+        assert rel_err(a[k], b[k]) < TOL, k
+
+
+def test_nsc_multi_step_with_warm_start():
+    sc = packed_scene(2000, d=0.05, phi=0.2, seed=12, squeeze=0.97)
+    g, o = make_pair(sc, model="nsc", dt=5e-4, nsc_velocity_iters=500)
+    for chunk in (1, 2, 3):
+        sg = g.step(chunk)
+        so = o.step(chunk)
+        a, b = g.get_state(), o.get_state()
+        for k in ("x", "q", "v", "w"):
+            assert rel_err(a[k], b[k]) < TOL, k
+        assert sg["psor_sweeps"] == so["psor_sweeps"]
+        assert sg["contacts"] == so["contacts"]
+    pg, lg, _ = g.impulses()
+    po, lo, _ = o.impulses()
+    np.testing.assert_array_equal(pg, po)
+    assert rel_err(lg, lo) < TOL
+
+
+def test_list_rebuild_keeps_exact_contacts():
+    # large velocities force neighbour-list rebuilds within a few steps
+    sc = packed_scene(800, d=0.1, phi=0.1, seed=13, squeeze=0.97, sigma_v=20.0, sigma_w=5.0)
+    g, o = make_pair(sc, model="hertz-mindlin", dt=1e-4, hm_youngs_modulus=1e5, hm_poisson_ratio=0.3,
+                     hm_restitution=0.5, hm_friction=0.5, skin=0.01)
+    st = g.step(20)
+    o.step(20)
+    assert st["list_rebuilds"] >= 1
+    a, b = g.get_state(), o.get_state()
+    assert rel_err(a["x"], b["x"]) < 1e-9
+    assert_contacts_equal(g, o, 0.0)
