@@ -549,7 +549,7 @@ int rg_step(rg_system* s, int nsteps, rg_step_stats* stats) {
     Ctl* h = s->h_ctl;
     std::memset(stats, 0, sizeof(*stats));
     stats->steps = nsteps;
-    stats->contacts = h->contacts;
+    stats->contacts = s->cfg.model == RG_MODEL_NSC ? h->vel_contacts : h->contacts;
     stats->collisions = h->collisions;
     stats->psor_sweeps = h->sweeps_sum;
     stats->psor_sweeps_last = h->sweeps_last;

@@ -8,6 +8,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <cuda/atomic>
 
 #include "../../include/rodgpu.h"
 
@@ -237,18 +238,20 @@ __device__ inline bool grid_sync(const GridBar& g, unsigned int nb) {
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
     s_ok = 1;
-    volatile unsigned int* vgen = g.gen;
-    unsigned int my = *vgen;
-    __threadfence();
-    unsigned int arrived = atomicAdd(g.count, 1u);
-    if (arrived == nb - 1) {
-      *g.count = 0;
-      __threadfence();
-      atomicAdd(g.gen, 1u);
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(*g.gen);
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(*g.count);
+    const unsigned int my = gen.load(cuda::memory_order_acquire);
+    if (*(volatile int*)g.err & ERR_TIMEOUT) {
+      s_ok = 0;
+    } else if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == nb - 1) {
+      cnt.store(0u, cuda::memory_order_relaxed);
+      gen.fetch_add(1u, cuda::memory_order_release);
     } else {
       long long it = 0;
-      while (*vgen == my) {
-        if (++it > kSpinLimit) {
+      while (gen.load(cuda::memory_order_acquire) == my) {
+        ++it;
+        if ((it & 63) == 0 && (*(volatile int*)g.err & ERR_TIMEOUT)) { s_ok = 0; break; }
+        if (it > kSpinLimit) {
           atomicOr(g.err, ERR_TIMEOUT);
           s_ok = 0;
           break;
@@ -256,8 +259,6 @@ __device__ inline bool grid_sync(const GridBar& g, unsigned int nb) {
         if (it > 64) __nanosleep(64);
       }
     }
-    __threadfence();
-    if (*(volatile int*)g.err & ERR_TIMEOUT) s_ok = 0;
   }
   __syncthreads();
   return s_ok != 0;

@@ -40,6 +40,8 @@ struct Ctl {
   long long collisions; // NSC impacts of the last step
   double jn_sum, jt_sum, pe;
   long long row_sweeps; // Σ contacts x sweeps (cumulative)
+  int vel_contacts;     // NSC: contacts of the last velocity solve (lastHitCount)
+  int pad2;
   int rec_n;            // MLP records stored
   int pad;
   unsigned int bar_count, bar_gen;  // grid barrier

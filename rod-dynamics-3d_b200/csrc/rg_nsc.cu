@@ -454,7 +454,10 @@ __global__ void k_warm_save(Contacts con, const int* order, const int* color, Ro
     jn += l0;
     jt += sqrt(l1 * l1 + l2 * l2);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *wn = C;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *wn = C;
+    ctl->vel_contacts = C;
+  }
   jn = warp_sum(jn);
   jt = warp_sum(jt);
   if ((threadIdx.x & 31) == 0) {
