@@ -111,7 +111,8 @@ typedef struct rg_config {
   /* Neighbour-list broad phase (project-specific, no reference field). */
   double skin;                   /* Verlet skin; <= 0 selects automatic      */
   int32_t max_neighbors;         /* initial per-rod list capacity; <= 0 auto */
-  int32_t reserved[7];
+  int32_t team_blocks;           /* blocks of the persistent NSC team; 0 auto */
+  int32_t reserved[6];
 } rg_config;
 
 /* Per-call statistics (the profile-CSV columns of main.cpp:3276-3355). */
@@ -208,6 +209,11 @@ int rg_get_history(const rg_system* sys, int32_t* pairs, double* value,
 int rg_set_profiling(rg_system* sys, int enable);
 /* Accumulated milliseconds and launch counts per stage since enabling. */
 int rg_get_profile(const rg_system* sys, double* ms, int64_t* launches);
+/* Phase times of the persistent NSC step since enabling (ms, n <= 12):
+ * 0 free flight, 1 detection, 2 colouring, 3 manifold rows, 4 PSOR,
+ * 5 position update, 6 projection detection, 7 projection colouring,
+ * 8 projection sweeps. */
+int rg_get_phase_times(const rg_system* sys, double* ms, int n);
 
 /* ---- learned PSOR warm start ------------------------------------------- */
 /* MLP 8 -> 128 -> 128 -> 128 -> 3 (SiLU), BF16 weights and activations,

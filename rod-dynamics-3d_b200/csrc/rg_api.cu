@@ -75,6 +75,8 @@ void free_contact_buffers(rg_system* s) {
   cudaFree(N.row); cudaFree(N.lam); cudaFree(N.color); cudaFree(N.color_tmp); cudaFree(N.order);
   cudaFree(N.color_cnt); cudaFree(N.color_off); cudaFree(N.wkey); cudaFree(N.wlam); cudaFree(N.wn);
   cudaFree(N.dx); cudaFree(N.prow); cudaFree(N.pactive);
+  cudaFree(N.pmax); cudaFree(N.cmask); cudaFree(N.owner); cudaFree(N.cursor); cudaFree(N.remaining);
+  cudaFree(N.blk); cudaFree(N.slot_of); cudaFree(N.bar); cudaFree(N.view_dev); cudaFree(N.team_dev);
   N = Nsc();
   cudaFree(s->d_cf);
   s->d_cf = nullptr;
@@ -123,6 +125,18 @@ cudaError_t alloc_contact_buffers(rg_system* s, int ccap, int hcap) {
   if ((e = cudaMemset(N.dx, 0, sizeof(double) * 6 * (size_t)n))) return e;
   if ((e = cudaMalloc(&N.prow, sizeof(double) * kPosComps * (size_t)ccap))) return e;
   if ((e = cudaMalloc(&N.pactive, sizeof(int) * ccap))) return e;
+  if ((e = cudaMalloc(&N.pmax, sizeof(unsigned long long) * 2 * (size_t)n))) return e;
+  if ((e = cudaMalloc(&N.cmask, sizeof(unsigned long long) * (size_t)n))) return e;
+  if ((e = cudaMalloc(&N.owner, sizeof(int) * (size_t)n))) return e;
+  if ((e = cudaMalloc(&N.cursor, sizeof(int) * (kMaxColors + 2)))) return e;
+  if ((e = cudaMalloc(&N.remaining, sizeof(int) * 1024))) return e;
+  if ((e = cudaMalloc(&N.blk, sizeof(int) * (s->coop_blocks + 32)))) return e;
+  if ((e = cudaMalloc(&N.slot_of, sizeof(int) * (size_t)n))) return e;
+  if ((e = cudaMemset(N.slot_of, 0xff, sizeof(int) * (size_t)n))) return e;
+  if ((e = cudaMalloc(&N.bar, sizeof(unsigned int) * 8))) return e;
+  if ((e = cudaMemset(N.bar, 0, sizeof(unsigned int) * 8))) return e;
+  if ((e = cudaMalloc(&N.view_dev, nsc_view_bytes()))) return e;
+  if ((e = cudaMalloc(&N.team_dev, nsc_team_bytes()))) return e;
   if ((e = cudaMalloc(&s->d_cf, sizeof(double) * (13 * (size_t)ccap + 64)))) return e;
   if ((e = cudaMalloc(&s->d_feat, sizeof(float) * 8 * (size_t)ccap))) return e;
   if ((e = cudaMalloc(&s->d_pred, sizeof(float) * 3 * (size_t)ccap))) return e;
@@ -299,6 +313,7 @@ int rg_create(const rg_config* cfg, rg_system** out) {
   // persistent kernels run one 256-thread block per SM (co-residency is
   // guaranteed by the cooperative launch attribute)
   s->coop_blocks = s->sm_count;
+  s->team_blocks = cfg->team_blocks;  // NSC team size; 0 = automatic
   *out = s;
   return RG_OK;
 }
@@ -415,10 +430,12 @@ namespace {
 
 void launch_steps(rg_system* s, int nsteps) {
   const int model = s->cfg.model;
+  if (model == RG_MODEL_NSC) {
+    if (nsteps > 0) nsc_run_launch(s, nsteps);  // one persistent launch for all steps
+    return;
+  }
   for (int k = 0; k < nsteps; ++k) {
-    if (model == RG_MODEL_NSC) {
-      nsc_step_launch(s);
-    } else if (model == RG_MODEL_HARMONIC || model == RG_MODEL_HERTZ_MINDLIN) {
+    if (model == RG_MODEL_HARMONIC || model == RG_MODEL_HERTZ_MINDLIN) {
       force_eval_launch(s);      // forces at t (reuses fresh contacts)
       half_pos_launch(s);
       clear_forces_launch(s);
@@ -689,6 +706,20 @@ int rg_set_profiling(rg_system* s, int enable) {
   if (!s) return RG_ERR_ARG;
   s->prof_on = enable != 0;
   for (int k = 0; k < 8; ++k) { s->prof_ms[k] = 0; s->prof_cnt[k] = 0; }
+  // persistent-step phase timers live in the control block
+  Ctl h;
+  cudaMemcpy(&h, s->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost);
+  h.prof_phases = s->prof_on ? 1 : 0;
+  for (int k = 0; k < 12; ++k) h.phase_ns[k] = 0;
+  cudaMemcpy(s->d_ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice);
+  return RG_OK;
+}
+
+int rg_get_phase_times(const rg_system* s, double* ms, int n) {
+  if (!s || !ms) return RG_ERR_ARG;
+  Ctl h;
+  cudaMemcpy(&h, s->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost);
+  for (int k = 0; k < n && k < 12; ++k) ms[k] = h.phase_ns[k] * 1e-6;
   return RG_OK;
 }
 

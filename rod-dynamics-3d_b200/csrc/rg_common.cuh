@@ -219,6 +219,34 @@ __device__ inline void atomic_max_nonneg(double* addr, double v) {
   atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
 }
 
+// Exclusive block-wide scan of one int per thread (blockDim multiple of 32).
+__device__ inline int block_excl_scan(int v, int* sh_warp, int& total) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh_warp[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    int s = lane < nw ? sh_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < nw) sh_warp[lane] = s;
+  }
+  __syncthreads();
+  int warp_prefix = wid > 0 ? sh_warp[wid - 1] : 0;
+  total = sh_warp[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return warp_prefix + x - v;
+}
+
 // ---- bounded grid barrier ----------------------------------------------------
 // Sense-free generation barrier for co-resident (cooperatively launched)
 // blocks.  Every wait is bounded: after kSpinLimit polls the block records

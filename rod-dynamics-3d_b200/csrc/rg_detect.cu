@@ -16,7 +16,7 @@
 // Neighbour cells are staged through shared memory tile by tile.
 #include <cstdio>
 
-#include "rg_internal.cuh"
+#include "rg_detect_dev.cuh"
 
 namespace rg {
 
@@ -28,33 +28,6 @@ long long g_launches = 0;
 constexpr int kScanBS = 1024;
 constexpr int kScanItems = 2;
 constexpr int kScanTile = kScanBS * kScanItems;
-
-__device__ inline int block_excl_scan(int v, int* sh_warp, int& total) {
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int x = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) sh_warp[wid] = x;
-  __syncthreads();
-  if (wid == 0) {
-    int nw = blockDim.x >> 5;
-    int s = lane < nw ? sh_warp[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= o) s += y;
-    }
-    if (lane < nw) sh_warp[lane] = s;
-  }
-  __syncthreads();
-  int warp_prefix = wid > 0 ? sh_warp[wid - 1] : 0;
-  total = sh_warp[(blockDim.x >> 5) - 1];
-  __syncthreads();
-  return warp_prefix + x - v;
-}
 
 __global__ void k_scan_tiles(const int* in, int* out, const int* n_dev, int* blocks) {
   __shared__ int shw[32];
@@ -165,22 +138,6 @@ __global__ void k_disp_check(State st, const Seg* seg, const double* ref, Box bo
   }
 }
 
-__device__ inline int cell_coord(double x, double lo, double cell, int nc, int pbc) {
-  int c = (int)floor((x - lo) / cell);
-  if (pbc) {
-    c %= nc;
-    if (c < 0) c += nc;
-  } else {
-    c = c < 0 ? 0 : (c >= nc ? nc - 1 : c);
-  }
-  return c;
-}
-
-struct GridDev {
-  double lo[3], cell[3];
-  int n[3], ncells;
-};
-
 __global__ void k_cell_fill(int n, const int* cell_of, const int* cell_start, int* cell_fill,
                             int* cell_rods, const Ctl* ctl) {
   if (ctl->err || !ctl->rebuild) return;
@@ -191,35 +148,16 @@ __global__ void k_cell_fill(int n, const int* cell_of, const int* cell_start, in
   }
 }
 
-__global__ void k_zero_cells(int* cnt, int* fill, int ncells, const Ctl* ctl) {
+__global__ void k_zero_cells(int* cnt, int* fill, int ncells, int* nbr_cnt, int n, const Ctl* ctl) {
   if (ctl->err || !ctl->rebuild) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= ncells; i += gridDim.x * blockDim.x) {
-    cnt[i] = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= ncells || i < n; i += gridDim.x * blockDim.x) {
+    if (i <= ncells) cnt[i] = 0;
     if (i < ncells) fill[i] = 0;
+    if (i < n) nbr_cnt[i] = 0;
   }
 }
 
-// Insert j into the ascending list [list, list+cnt); returns new count.
-__device__ inline int list_insert(int* list, int cnt, int cap, int j, int* overflow) {
-  if (cnt >= cap) {
-    *overflow = 1;
-    return cnt;
-  }
-  int k = cnt;
-  while (k > 0 && list[k - 1] > j) {
-    list[k] = list[k - 1];
-    --k;
-  }
-  list[k] = j;
-  return cnt + 1;
-}
-
-constexpr int kTile = 128;
-
-// One block per home cell.  Each neighbour cell is staged in shared memory in
-// tiles of kTile segment records; every thread tests its home rod against the
-// tile.  Acceptance: min-image centre distance within cut_center, then the
-// FP64 closest distance below rsum + margin + skin.
+// One block per home cell (see build_cell).
 __global__ void __launch_bounds__(kTile) k_build_lists(const Seg* seg, int n, const GridDev* gdev, Box box,
                                                        const int* cell_start, const int* cell_rods,
                                                        double margin, double skin, double cut_center,
@@ -227,93 +165,29 @@ __global__ void __launch_bounds__(kTile) k_build_lists(const Seg* seg, int n, co
                                                        int maxnb, Ctl* ctl) {
   if (ctl->err || !ctl->rebuild) return;
   const GridDev g = *gdev;
-  __shared__ Seg tile[kTile];
-  __shared__ int tidx[kTile];
-  __shared__ int ncl[27];
-  __shared__ int nn;
+  __shared__ BuildSmem sm;
   int overflow = 0;
-  for (int cell = blockIdx.x; cell < g.ncells; cell += gridDim.x) {
-    int cx = cell % g.n[0], cy = (cell / g.n[0]) % g.n[1], cz = cell / (g.n[0] * g.n[1]);
-    if (threadIdx.x == 0) {
-      int cnt = 0;
-      int lo[3], hi[3];
-      int c3[3] = {cx, cy, cz};
-      for (int k = 0; k < 3; ++k) {
-        if (box.pbc && (g.n[k] < 3 || all_pairs)) {
-          lo[k] = 0; hi[k] = g.n[k] - 1;
-        } else {
-          lo[k] = c3[k] - 1; hi[k] = c3[k] + 1;
-        }
-      }
-      for (int z = lo[2]; z <= hi[2]; ++z)
-        for (int y = lo[1]; y <= hi[1]; ++y)
-          for (int x = lo[0]; x <= hi[0]; ++x) {
-            int X = x, Y = y, Z = z;
-            if (box.pbc) {
-              X = (X + g.n[0]) % g.n[0]; Y = (Y + g.n[1]) % g.n[1]; Z = (Z + g.n[2]) % g.n[2];
-            } else if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) {
-              continue;
-            }
-            if (cnt < 27) ncl[cnt++] = (Z * g.n[1] + Y) * g.n[0] + X;
-          }
-      nn = cnt;
-    }
-    __syncthreads();
-    int hs = cell_start[cell], he = cell_start[cell + 1];
-    for (int base = hs; base < he; base += blockDim.x) {
-      int hi = base + threadIdx.x;
-      bool act = hi < he;
-      int i = act ? cell_rods[hi] : -1;
-      Seg A;
-      if (act) A = seg[i];
-      int cnt = 0;
-      int* list = act ? nbr + (size_t)i * maxnb : nullptr;
-      for (int c = 0; c < nn; ++c) {
-        int ns = cell_start[ncl[c]], ne = cell_start[ncl[c] + 1];
-        for (int t0 = ns; t0 < ne; t0 += kTile) {
-          __syncthreads();
-          int k = t0 + threadIdx.x;
-          if (k < ne) {
-            int j = cell_rods[k];
-            tidx[threadIdx.x] = j;
-            tile[threadIdx.x] = seg[j];
-          }
-          __syncthreads();
-          int m = ne - t0 < kTile ? ne - t0 : kTile;
-          if (act) {
-            for (int u = 0; u < m; ++u) {
-              int j = tidx[u];
-              if (j <= i) continue;
-              const Seg& B = tile[u];
-              if (!all_pairs) {
-                d3 d{B.cx - A.cx, B.cy - A.cy, B.cz - A.cz};
-                d3 sh = min_image_shift(box, mk3(A.cx, A.cy, A.cz), mk3(B.cx, B.cy, B.cz));
-                d = d + sh;
-                double cc = A.h + B.h + A.r + B.r + margin + skin;
-                if (dot(d, d) > cc * cc * (1.0 + 1e-12)) continue;
-                Narrow nr = narrow_pair(A, B, box);
-                double lim = A.r + B.r + margin + skin;
-                if (!(nr.d2 < lim * lim)) continue;
-              }
-              cnt = list_insert(list, cnt, maxnb, j, &overflow);
-            }
-          }
-        }
-      }
-      if (act) nbr_cnt[i] = cnt;
-    }
-    __syncthreads();
-  }
+  double invL[3] = {1.0, 1.0, 1.0};
+  for (int k = 0; k < 3; ++k)
+    if (box.L[k] > 0.0) invL[k] = 1.0 / box.L[k];
+  for (int cell = blockIdx.x; cell < g.ncells; cell += gridDim.x)
+    build_cell_pairs(seg, g, box, invL, cell_start, cell_rods, margin, skin, all_pairs, nbr_cnt, nbr, maxnb,
+                     cell, sm, overflow);
   if (overflow) atomicOr(&ctl->err, ERR_NBR_CAP);
+  (void)n;
+  (void)cut_center;
 }
 
-__global__ void k_save_ref(const Seg* seg, int n, double* ref, Ctl* ctl) {
+__global__ void k_save_ref(const Seg* seg, int n, double* ref, int* nbr, int* nbr_cnt, int maxnb, Ctl* ctl) {
   if (ctl->err || !ctl->rebuild) return;
+  int overflow = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    sort_list(nbr, nbr_cnt, maxnb, i, overflow);
     Seg s = seg[i];
     ref[i] = s.cx; ref[n + i] = s.cy; ref[2 * n + i] = s.cz;
     ref[3 * n + i] = s.ux; ref[4 * n + i] = s.uy; ref[5 * n + i] = s.uz;
   }
+  if (overflow) atomicOr(&ctl->err, ERR_NBR_CAP);
 }
 
 __global__ void k_build_done(Ctl* ctl) {
@@ -325,15 +199,6 @@ __global__ void k_build_done(Ctl* ctl) {
   ctl->maxdisp = 0.0;
 }
 
-// Bounding box of the centres for open (non-periodic) systems.
-__device__ inline unsigned long long ord_key(double v) {
-  unsigned long long b = (unsigned long long)__double_as_longlong(v);
-  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
-}
-__device__ inline double ord_val(unsigned long long k) {
-  unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
-  return __longlong_as_double((long long)b);
-}
 __global__ void k_bounds(const Seg* seg, int n, unsigned long long* mn, unsigned long long* mx,
                          const Ctl* ctl) {
   if (ctl->err || !ctl->rebuild) return;
@@ -347,19 +212,7 @@ __global__ void k_bounds(const Seg* seg, int n, unsigned long long* mn, unsigned
 __global__ void k_open_grid(const unsigned long long* mn, const unsigned long long* mx, double cut,
                             int maxdim, GridDev* g, const Ctl* ctl) {
   if (ctl->err || !ctl->rebuild) return;
-  int total = 1;
-  for (int k = 0; k < 3; ++k) {
-    double lo = ord_val(mn[k]), hi = ord_val(mx[k]);
-    double span = hi - lo;
-    int d = (int)floor(span / cut);
-    d = d < 1 ? 1 : (d > maxdim ? maxdim : d);
-    g->lo[k] = lo;
-    g->cell[k] = span > 0 ? span / d : 1.0;
-    if (g->cell[k] < cut) g->cell[k] = cut;
-    g->n[k] = d;
-    total *= d;
-  }
-  g->ncells = total;
+  open_grid(mn, mx, cut, maxdim, g);
 }
 
 // Reads the device grid descriptor into each thread (open systems).
@@ -385,36 +238,8 @@ __global__ void k_narrow_count(const Seg* seg, State st, Box box, double delta, 
                                const int* nbr, int maxnb, int words, unsigned long long* mask,
                                int* hit_cnt, const Ctl* ctl) {
   if (ctl->err) return;
-  const int n = st.n;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int cnt = nbr_cnt[i];
-    const int* list = nbr + (size_t)i * maxnb;
-    Seg A = seg[i];
-    bool a_static = !(st.inv_mass[i] > 0.0);
-    int hits = 0;
-    unsigned long long wbits = 0;
-    int w = 0;
-    for (int k = 0; k < cnt; ++k) {
-      int j = list[k];
-      bool hit = false;
-      if (!(a_static && !(st.inv_mass[j] > 0.0))) {
-        Seg B = seg[j];
-        Narrow nr = narrow_pair(A, B, box);
-        hit = contact_test(nr.d2, A.r + B.r, delta);
-      }
-      if (hit) {
-        wbits |= 1ull << (k & 63);
-        ++hits;
-      }
-      if ((k & 63) == 63) {
-        mask[(size_t)i * words + w] = wbits;
-        wbits = 0;
-        ++w;
-      }
-    }
-    if (w < words && (cnt & 63)) mask[(size_t)i * words + w] = wbits;
-    hit_cnt[i] = hits;
-  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x)
+    hit_cnt[i] = narrow_count_rod(i, seg, st.inv_mass, box, delta, nbr_cnt, nbr, maxnb, words, mask);
 }
 
 __global__ void k_narrow_write(const Seg* seg, int n, Box box, const int* nbr_cnt, const int* nbr,
@@ -428,30 +253,8 @@ __global__ void k_narrow_write(const Seg* seg, int n, Box box, const int* nbr_cn
   }
   if (total > con.cap) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int cnt = nbr_cnt[i];
-    int o = hit_off[i];
-    if (hit_off[i + 1] == o) continue;
-    const int* list = nbr + (size_t)i * maxnb;
-    Seg A = seg[i];
-    for (int k = 0; k < cnt; ++k) {
-      if (!((mask[(size_t)i * words + (k >> 6)] >> (k & 63)) & 1ull)) continue;
-      int j = list[k];
-      Seg B = seg[j];
-      Narrow nr = narrow_pair(A, B, box);
-      double dist = sqrt(nr.d2);
-      d3 diff = nr.pb - nr.pa;
-      d3 nv = dist > 1e-10 ? diff / dist : mk3(1, 0, 0);
-      con.a[o] = i;
-      con.b[o] = j;
-      con.type[o] = contact_type(nr.s, nr.t);
-      con.comp(0)[o] = nr.pa.x; con.comp(1)[o] = nr.pa.y; con.comp(2)[o] = nr.pa.z;
-      con.comp(3)[o] = nr.pb.x; con.comp(4)[o] = nr.pb.y; con.comp(5)[o] = nr.pb.z;
-      con.comp(6)[o] = nv.x; con.comp(7)[o] = nv.y; con.comp(8)[o] = nv.z;
-      con.comp(9)[o] = nr.sh.x; con.comp(10)[o] = nr.sh.y; con.comp(11)[o] = nr.sh.z;
-      con.comp(12)[o] = dist;
-      con.comp(13)[o] = A.r + B.r;
-      ++o;
-    }
+    if (hit_off[i + 1] == hit_off[i]) continue;
+    narrow_write_rod(i, hit_off[i], seg, box, nbr_cnt, nbr, maxnb, words, mask, con);
   }
 }
 
@@ -474,7 +277,7 @@ void Contacts::free_() {
 // ---------------------------------------------------------------------------
 struct DetDev {  // device-resident grid descriptor and scratch
   GridDev grid;
-  unsigned long long mn[3], mx[3];
+  unsigned long long mn[3], mx[3];  // contiguous: bounds[0..2] min, [3..5] max
   int n;       // body count (scan length for per-rod arrays)
   int ncells;  // cell count (scan length for cell arrays)
 };
@@ -482,6 +285,8 @@ static DetDev* det_dev(rg_system* s) {
   return reinterpret_cast<DetDev*>(s->det.ref + 6 * (size_t)s->n);
 }
 const int* detector_n_dev(rg_system* s) { return &det_dev(s)->n; }
+GridDev* detector_grid(rg_system* s) { return &det_dev(s)->grid; }
+unsigned long long* detector_bounds(rg_system* s) { return det_dev(s)->mn; }
 
 __global__ void k_grid_ncells(DetDev* dd, const Ctl* ctl) {
   if (ctl->err || !ctl->rebuild) return;
@@ -588,7 +393,8 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild) {
     RGL k_open_grid<<<1, 1, 0, st>>>(dd->mn, dd->mx, d.cut_center, 64, &dd->grid, ctl);
     RGL k_grid_ncells<<<1, 1, 0, st>>>(dd, ctl);
   }
-  RGL k_zero_cells<<<grid_for(d.ncells + 1, bs), bs, 0, st>>>(d.cell_cnt, d.cell_fill, d.ncells, ctl);
+  RGL k_zero_cells<<<grid_for((d.ncells + 1 > n ? d.ncells + 1 : n), bs), bs, 0, st>>>(d.cell_cnt, d.cell_fill, d.ncells,
+                                                                                     d.nbr_cnt, n, ctl);
   RGL k_cell_count_dyn<<<g, bs, 0, st>>>(d.seg, n, &dd->grid, s->box.pbc, d.cell_of, d.cell_cnt, ctl);
   s->scan.run(d.cell_cnt, d.cell_start, &dd->ncells, st);
   RGL k_cell_fill<<<g, bs, 0, st>>>(n, d.cell_of, d.cell_start, d.cell_fill, d.cell_rods, ctl);
@@ -596,7 +402,7 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild) {
   RGL k_build_lists<<<gb, kTile, 0, st>>>(d.seg, n, &dd->grid, s->box, d.cell_start, d.cell_rods,
                                        d.margin, d.skin, d.cut_center, d.all_pairs ? 1 : 0,
                                        d.nbr_cnt, d.nbr, d.maxnb, ctl);
-  RGL k_save_ref<<<g, bs, 0, st>>>(d.seg, n, d.ref, ctl);
+  RGL k_save_ref<<<g, bs, 0, st>>>(d.seg, n, d.ref, d.nbr, d.nbr_cnt, d.maxnb, ctl);
   RGL k_build_done<<<1, 1, 0, st>>>(ctl);
   // --- narrow phase ---
   RGL k_narrow_count<<<g, bs, 0, st>>>(d.seg, s->st, s->box, delta, d.nbr_cnt, d.nbr, d.maxnb,

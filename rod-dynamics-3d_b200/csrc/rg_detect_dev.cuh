@@ -1,0 +1,311 @@
+// rg_detect_dev.cuh - device bodies of the broad and narrow phase, shared
+// by the multi-kernel detection (rg_detect.cu) and the persistent NSC step
+// kernel (rg_nsc.cu).  See rg_detect.cu for the algorithm and its reference.
+#pragma once
+#include "rg_internal.cuh"
+
+namespace rg {
+
+constexpr int kTile = 256;  // threads per block; segment records per shared-memory tile
+
+__device__ inline int cell_coord(double x, double lo, double cell, int nc, int pbc) {
+  int c = (int)floor((x - lo) / cell);
+  if (pbc) {
+    c %= nc;
+    if (c < 0) c += nc;
+  } else {
+    c = c < 0 ? 0 : (c >= nc ? nc - 1 : c);
+  }
+  return c;
+}
+
+struct GridDev {
+  double lo[3], cell[3];
+  int n[3], ncells;
+};
+
+
+// Bounding box of the centres for open (non-periodic) systems.
+__device__ inline unsigned long long ord_key(double v) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ inline double ord_val(unsigned long long k) {
+  unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+// Cell grid over the bounding box of the centres (open systems).
+__device__ inline void open_grid(const unsigned long long* mn, const unsigned long long* mx, double cut,
+                                 int maxdim, GridDev* g) {
+  int total = 1;
+  for (int k = 0; k < 3; ++k) {
+    double lo = ord_val(mn[k]), hi = ord_val(mx[k]);
+    double span = hi - lo;
+    int d = (int)floor(span / cut);
+    d = d < 1 ? 1 : (d > maxdim ? maxdim : d);
+    g->lo[k] = lo;
+    g->cell[k] = span > 0 ? span / d : 1.0;
+    if (g->cell[k] < cut) g->cell[k] = cut;
+    g->n[k] = d;
+    total *= d;
+  }
+  g->ncells = total;
+}
+
+struct BuildSmem {
+  Seg tile[kTile];
+  int tidx[kTile];
+  Seg home[kTile];
+  int hidx[kTile];
+  int ncl[27];
+  int nn;
+};
+
+__device__ inline int list_insert(int* list, int cnt, int cap, int j, int& overflow) {
+  if (cnt >= cap) {
+    overflow = 1;
+    return cnt;
+  }
+  int k = cnt;
+  while (k > 0 && list[k - 1] > j) {
+    list[k] = list[k - 1];
+    --k;
+  }
+  list[k] = j;
+  return cnt + 1;
+}
+
+// Conservative minimum-image centre offset B - A without divisions (for list
+// building only; the exact narrow phase uses min_image_shift).
+__device__ inline d3 centre_offset(const Seg& A, const Seg& B, const Box& box, const double* invL) {
+  d3 d{B.cx - A.cx, B.cy - A.cy, B.cz - A.cz};
+  if (box.pbc) {
+    if (box.L[0] > 0.0) d.x -= box.L[0] * rint(d.x * invL[0]);
+    if (box.L[1] > 0.0) d.y -= box.L[1] * rint(d.y * invL[1]);
+    if (box.L[2] > 0.0) d.z -= box.L[2] * rint(d.z * invL[2]);
+  }
+  return d;
+}
+
+// Pair-parallel list build for one home cell (all block threads call it):
+// home rods and each neighbour cell are staged in shared memory and the
+// block's threads split the (home rod, neighbour rod) pairs.  Accepted j > i
+// are appended with an atomic per-rod counter (nbr_cnt zeroed beforehand);
+// sort_lists() orders every list afterwards.  Acceptance is the same
+// conservative test as build_cell.
+__device__ inline void build_cell_pairs(const Seg* seg, const GridDev& g, const Box& box, const double* invL,
+                                        const int* cell_start, const int* cell_rods, double margin,
+                                        double skin, int all_pairs, int* nbr_cnt, int* nbr, int maxnb,
+                                        int cell, BuildSmem& sm, int& overflow) {
+  int cx = cell % g.n[0], cy = (cell / g.n[0]) % g.n[1], cz = cell / (g.n[0] * g.n[1]);
+  if (threadIdx.x == 0) {
+    int cnt = 0;
+    int lo[3], hi[3];
+    int c3[3] = {cx, cy, cz};
+    for (int k = 0; k < 3; ++k) {
+      if (box.pbc && (g.n[k] < 3 || all_pairs)) {
+        lo[k] = 0; hi[k] = g.n[k] - 1;
+      } else {
+        lo[k] = c3[k] - 1; hi[k] = c3[k] + 1;
+      }
+    }
+    for (int z = lo[2]; z <= hi[2]; ++z)
+      for (int y = lo[1]; y <= hi[1]; ++y)
+        for (int x = lo[0]; x <= hi[0]; ++x) {
+          int X = x, Y = y, Z = z;
+          if (box.pbc) {
+            X = (X + g.n[0]) % g.n[0]; Y = (Y + g.n[1]) % g.n[1]; Z = (Z + g.n[2]) % g.n[2];
+          } else if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) {
+            continue;
+          }
+          if (cnt < 27) sm.ncl[cnt++] = (Z * g.n[1] + Y) * g.n[0] + X;
+        }
+    sm.nn = cnt;
+  }
+  __syncthreads();
+  const int nn = sm.nn;
+  const int hs = cell_start[cell], he = cell_start[cell + 1];
+  for (int h0 = hs; h0 < he; h0 += kTile) {
+    const int H = he - h0 < kTile ? he - h0 : kTile;
+    __syncthreads();
+    if ((int)threadIdx.x < H) {
+      int i = cell_rods[h0 + threadIdx.x];
+      sm.hidx[threadIdx.x] = i;
+      sm.home[threadIdx.x] = seg[i];
+    }
+    for (int c = 0; c < nn; ++c) {
+      int ns = cell_start[sm.ncl[c]], ne = cell_start[sm.ncl[c] + 1];
+      for (int t0 = ns; t0 < ne; t0 += kTile) {
+        const int m = ne - t0 < kTile ? ne - t0 : kTile;
+        __syncthreads();
+        if ((int)threadIdx.x < m) {
+          int j = cell_rods[t0 + threadIdx.x];
+          sm.tidx[threadIdx.x] = j;
+          sm.tile[threadIdx.x] = seg[j];
+        }
+        __syncthreads();
+        const int pairs = H * m;
+        for (int q = threadIdx.x; q < pairs; q += blockDim.x) {
+          const int h = q / m, u = q - h * m;
+          const int i = sm.hidx[h], j = sm.tidx[u];
+          if (j <= i) continue;
+          if (!all_pairs) {
+            const Seg& A = sm.home[h];
+            const Seg& B = sm.tile[u];
+            d3 d = centre_offset(A, B, box, invL);
+            double cc = A.h + B.h + A.r + B.r + margin + skin;
+            if (dot(d, d) > cc * cc * (1.0 + 1e-9)) continue;
+            Narrow nr = narrow_pair(A, B, box);
+            double lim = A.r + B.r + margin + skin;
+            if (!(nr.d2 < lim * lim)) continue;
+          }
+          int pos = atomicAdd(&nbr_cnt[i], 1);
+          if (pos < maxnb) nbr[(size_t)i * maxnb + pos] = j;
+          else overflow = 1;
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Sorts rod i's neighbour list ascending (insertion sort; lists are short).
+__device__ inline void sort_list(int* nbr, int* nbr_cnt, int maxnb, int i, int& overflow) {
+  int cnt = nbr_cnt[i];
+  if (cnt > maxnb) {
+    overflow = 1;
+    cnt = maxnb;
+    nbr_cnt[i] = cnt;
+  }
+  int* L = nbr + (size_t)i * maxnb;
+  for (int k = 1; k < cnt; ++k) {
+    int v = L[k];
+    int m = k;
+    while (m > 0 && L[m - 1] > v) {
+      L[m] = L[m - 1];
+      --m;
+    }
+    L[m] = v;
+  }
+}
+
+// Narrow-phase count with G lanes per rod (G divides 32): lane l tests list
+// entries l, l+G, ...; contacts set bits in the rod's mask words (zeroed by
+// lane 0 first) and the group's hit count is returned to every lane.
+template <int G>
+__device__ inline int narrow_count_lanes(int i, bool valid, const Seg* seg, const double* inv_mass,
+                                         const Box& box, double delta, const int* nbr_cnt, const int* nbr,
+                                         int maxnb, int words, unsigned long long* mask) {
+  const int l = threadIdx.x & (G - 1);
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (threadIdx.x & 31 & ~(G - 1)));
+  int cnt = valid ? nbr_cnt[i] : 0;
+  if (valid && l == 0)
+    for (int w = 0; w < words && w * 64 < cnt; ++w) mask[(size_t)i * words + w] = 0ull;
+  __syncwarp();
+  int hits = 0;
+  if (valid) {
+    const int* list = nbr + (size_t)i * maxnb;
+    Seg A = seg[i];
+    bool a_static = !(inv_mass[i] > 0.0);
+    for (int k = l; k < cnt; k += G) {
+      int j = list[k];
+      if (a_static && !(inv_mass[j] > 0.0)) continue;
+      Seg B = seg[j];
+      Narrow nr = narrow_pair(A, B, box);
+      if (contact_test(nr.d2, A.r + B.r, delta)) {
+        atomicOr(&mask[(size_t)i * words + (k >> 6)], 1ull << (k & 63));
+        ++hits;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) hits += __shfl_xor_sync(0xffffffffu, hits, o);
+  (void)gmask;
+  return hits;
+}
+
+// Exact FP64 narrow phase of rod i against its list: sets one mask bit per
+// contacting list entry and returns the number of contacts.
+__device__ inline int narrow_count_rod(int i, const Seg* seg, const double* inv_mass, const Box& box,
+                                       double delta, const int* nbr_cnt, const int* nbr, int maxnb,
+                                       int words, unsigned long long* mask) {
+  int cnt = nbr_cnt[i];
+  const int* list = nbr + (size_t)i * maxnb;
+  Seg A = seg[i];
+  bool a_static = !(inv_mass[i] > 0.0);
+  int hits = 0;
+  unsigned long long wbits = 0;
+  int w = 0;
+  for (int k = 0; k < cnt; ++k) {
+    int j = list[k];
+    bool hit = false;
+    if (!(a_static && !(inv_mass[j] > 0.0))) {
+      Seg B = seg[j];
+      Narrow nr = narrow_pair(A, B, box);
+      hit = contact_test(nr.d2, A.r + B.r, delta);
+    }
+    if (hit) {
+      wbits |= 1ull << (k & 63);
+      ++hits;
+    }
+    if ((k & 63) == 63) {
+      mask[(size_t)i * words + w] = wbits;
+      wbits = 0;
+      ++w;
+    }
+  }
+  if (w < words && (cnt & 63)) mask[(size_t)i * words + w] = wbits;
+  return hits;
+}
+
+// Writes the contacts of rod i (in list order: ascending b) from slot o on.
+__device__ inline void narrow_write_rod(int i, int o, const Seg* seg, const Box& box, const int* nbr_cnt,
+                                        const int* nbr, int maxnb, int words,
+                                        const unsigned long long* mask, const Contacts& con) {
+  int cnt = nbr_cnt[i];
+  const int* list = nbr + (size_t)i * maxnb;
+  Seg A = seg[i];
+  for (int k = 0; k < cnt; ++k) {
+    if (!((mask[(size_t)i * words + (k >> 6)] >> (k & 63)) & 1ull)) continue;
+    int j = list[k];
+    Seg B = seg[j];
+    Narrow nr = narrow_pair(A, B, box);
+    double dist = sqrt(nr.d2);
+    d3 diff = nr.pb - nr.pa;
+    d3 nv = dist > 1e-10 ? diff / dist : mk3(1, 0, 0);
+    con.a[o] = i;
+    con.b[o] = j;
+    con.type[o] = contact_type(nr.s, nr.t);
+    con.comp(0)[o] = nr.pa.x; con.comp(1)[o] = nr.pa.y; con.comp(2)[o] = nr.pa.z;
+    con.comp(3)[o] = nr.pb.x; con.comp(4)[o] = nr.pb.y; con.comp(5)[o] = nr.pb.z;
+    con.comp(6)[o] = nv.x; con.comp(7)[o] = nv.y; con.comp(8)[o] = nv.z;
+    con.comp(9)[o] = nr.sh.x; con.comp(10)[o] = nr.sh.y; con.comp(11)[o] = nr.sh.z;
+    con.comp(12)[o] = dist;
+    con.comp(13)[o] = A.r + B.r;
+    ++o;
+  }
+}
+
+__device__ inline Seg make_seg(const State& st, int i) {
+  dq q = st.q.ld(i);
+  d3 u = axis_y(q);
+  Seg s;
+  s.cx = st.x.x[i]; s.cy = st.x.y[i]; s.cz = st.x.z[i]; s.h = st.h[i];
+  s.ux = u.x; s.uy = u.y; s.uz = u.z; s.r = st.r[i];
+  return s;
+}
+
+// |Δx| + h|Δu| since the last list build (non-finite state -> huge).
+__device__ inline double seg_disp(const Seg& s, const double* ref, int n, int i, const Box& box) {
+  d3 dx{s.cx - ref[i], s.cy - ref[n + i], s.cz - ref[2 * n + i]};
+  if (box.pbc) {
+    if (box.L[0] > 0.0) dx.x -= floor(dx.x / box.L[0] + 0.5) * box.L[0];
+    if (box.L[1] > 0.0) dx.y -= floor(dx.y / box.L[1] + 0.5) * box.L[1];
+    if (box.L[2] > 0.0) dx.z -= floor(dx.z / box.L[2] + 0.5) * box.L[2];
+  }
+  d3 du{s.ux - ref[3 * n + i], s.uy - ref[4 * n + i], s.uz - ref[5 * n + i]};
+  double d = len(dx) + s.h * len(du);
+  return (d == d) ? d : 1e300;
+}
+
+}  // namespace rg

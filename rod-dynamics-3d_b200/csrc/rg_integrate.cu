@@ -5,23 +5,9 @@
 // flight and position update of App::physicsStep (src/app/main.cpp:4397-4408,
 // :4469-4483) and its PBC wrap (:4508-4517).  State is structure-of-arrays
 // FP64, so every load and store is a fully coalesced 8-byte access.
-#include "rg_internal.cuh"
+#include "rg_nsc_dev.cuh"
 
 namespace rg {
-
-__device__ inline void wrap_pos(const Box& box, d3& p) {
-  if (!box.pbc) return;
-  double* c[3] = {&p.x, &p.y, &p.z};
-  for (int k = 0; k < 3; ++k) {
-    double L = box.L[k];
-    if (L <= 0.0) continue;
-    double x = *c[k];
-    // bounded: a finite coordinate is at most a few boxes outside
-    for (int it = 0; x < box.lo[k] && it < 64; ++it) x += L;
-    for (int it = 0; x >= box.hi[k] && it < 64; ++it) x -= L;
-    *c[k] = x;
-  }
-}
 
 __device__ inline d3 ang_accel(const State& st, int i, dq q, d3 w, d3 tau) {
   d3 I = st.I.ld(i), Iinv = st.Iinv.ld(i);
@@ -99,58 +85,22 @@ __global__ void k_clear_forces(State st, const Ctl* ctl) {
 __global__ void k_nsc_free_flight(State st, rg_config cfg, const Ctl* ctl) {
   if (ctl->err) return;
   const d3 g{cfg.gravity[0], cfg.gravity[1], cfg.gravity[2]};
-  const double dt = cfg.dt;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
-    double im = st.inv_mass[i];
-    if (!(im > 0)) continue;
-    dq q = st.q.ld(i);
-    d3 w = st.w.ld(i);
-    d3 v = st.v.ld(i) + (st.f.ld(i) * im + g) * dt;
-    d3 Iw_w = rot_diag_apply(q, st.I.ld(i), w);
-    d3 gyro = cross(w, Iw_w);
-    w = w + rot_diag_apply(q, st.Iinv.ld(i), st.tau.ld(i) - gyro) * dt;
-    st.v.st(i, v);
-    st.w.st(i, w);
-  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x)
+    nsc_free_flight_body(st, i, g, cfg.dt);
 }
 
 __global__ void k_nsc_position_update(State st, rg_config cfg, Ctl* ctl) {
   if (ctl->err) return;
-  const double dt = cfg.dt;
-  const double ld = 1.0 - cfg.lin_damp * dt, ad = 1.0 - cfg.ang_damp * dt;
   int bad = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
-    d3 v = st.v.ld(i), w = st.w.ld(i);
-    d3 x = st.x.ld(i) + v * dt;
-    dq q = st.q.ld(i);
-    d3 hw = w * (0.5 * dt);
-    dq wq{0.0, hw.x, hw.y, hw.z};
-    dq d = qmul(wq, q);
-    q = qnormalize(dq{q.w + d.w, q.x + d.x, q.y + d.y, q.z + d.z});
-    v = v * ld;
-    w = w * ad;
-    double wl = len(w);
-    if (wl > cfg.w_max) w = w * (cfg.w_max / wl);
-    st.x.st(i, x);
-    st.q.st(i, q);
-    st.v.st(i, v);
-    st.w.st(i, w);
-    if (!(x.x == x.x && x.y == x.y && x.z == x.z && v.x == v.x)) bad = 1;
-  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x)
+    bad |= nsc_position_update_body(st, i, cfg);
   if (bad) atomicOr(&ctl->err, ERR_NONFINITE);
 }
 
 __global__ void k_wrap_clear(State st, Box box, const Ctl* ctl) {
   if (ctl->err) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
-    if (box.pbc) {
-      d3 x = st.x.ld(i);
-      wrap_pos(box, x);
-      st.x.st(i, x);
-    }
-    st.f.st(i, mk3(0, 0, 0));
-    st.tau.st(i, mk3(0, 0, 0));
-  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x)
+    wrap_clear_body(st, box, i);
 }
 
 static inline int body_grid(rg_system* s) { return grid_for(s->n, 256, s->sm_count * 8); }

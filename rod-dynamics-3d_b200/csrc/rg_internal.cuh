@@ -41,7 +41,8 @@ struct Ctl {
   double jn_sum, jt_sum, pe;
   long long row_sweeps; // Σ contacts x sweeps (cumulative)
   int vel_contacts;     // NSC: contacts of the last velocity solve (lastHitCount)
-  int pad2;
+  int prof_phases;      // 1: the persistent step records phase times
+  long long phase_ns[12];  // persistent-step phase time accumulators
   int rec_n;            // MLP records stored
   int pad;
   unsigned int bar_count, bar_gen;  // grid barrier
@@ -116,6 +117,17 @@ struct Nsc {
   double* dx = nullptr;   // 6n: dx(3n), dθ(3n)
   double* prow = nullptr; // kPosComps * ccap
   int* pactive = nullptr; // ccap
+  // colouring scratch of the persistent step (per body)
+  unsigned long long* pmax = nullptr;   // 2n priority maxima (two rounds)
+  unsigned long long* cmask = nullptr;  // n colour masks
+  int* owner = nullptr;                 // n lowest contact index per body
+  int* cursor = nullptr;                // kMaxColors+1
+  int* remaining = nullptr;             // colouring rounds
+  int* blk = nullptr;                   // per-block scan scratch
+  int* slot_of = nullptr;               // n per-body local slots (-1)
+  unsigned int* bar = nullptr;          // team barrier words
+  void* view_dev = nullptr;             // device copy of the step view
+  void* team_dev = nullptr;             // device team descriptor
 };
 constexpr int kRowComps = 42;
 constexpr int kPosComps = 12;
@@ -171,6 +183,7 @@ struct rg_system {
   float* d_pred = nullptr;    // 3 * ccap scratch
 
   int coop_blocks = 0;        // co-resident blocks for the persistent kernels
+  int team_blocks = 0;        // blocks of the NSC team (0: automatic)
   cudaGraphExec_t graph = nullptr;
   int graph_kind = -1;
 
@@ -253,8 +266,10 @@ void nsc_free_flight_launch(rg_system* s);
 void nsc_position_update_launch(rg_system* s);
 void wrap_launch(rg_system* s);
 // rg_nsc.cu
-void nsc_step_launch(rg_system* s);
-void color_launch(rg_system* s);
+void nsc_run_launch(rg_system* s, int nsteps);
+int nsc_team_blocks(const rg_system* s);
+size_t nsc_view_bytes();
+size_t nsc_team_bytes();
 // rg_mlp.cu
 void mlp_warm_launch(rg_system* s);
 void mlp_record_launch(rg_system* s);

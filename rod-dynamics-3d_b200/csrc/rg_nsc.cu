@@ -1,573 +1,548 @@
-// rg_nsc.cu - non-smooth contact: colouring, manifolds, PSOR, projection.
+// rg_nsc.cu - the non-smooth-contact (PSOR) step as one persistent kernel.
 //
 // NscContactSolver (src/physics/nsc_contact.cpp):
 //   detectAndBuildManifolds :239-321, buildTangentBasis :78-85,
 //   computeDiag :106-117, solveVelocities :325-655 (warm start :344-380,
 //   sweeps :385-552, residual :546-551, cache :646-654),
-//   projectPositions :659-880 (multi-body path :698-879).
-// Step order of App::physicsStep (src/app/main.cpp:4383-4528).
+//   projectPositions :659-880 (multi-body path :698-879);
+// step order of App::physicsStep (src/app/main.cpp:4383-4528).
 //
-// Gauss-Seidel runs graph-coloured: contacts are coloured (Jones-Plassmann,
-// first fit) so that no two contacts of one colour share a dynamic body;
-// a sweep visits the colours in order and the contacts of a colour in
-// parallel.  This equals sequential Gauss-Seidel over the colour-major
-// permutation of the (a,b)-sorted contacts, bit for bit.  Rows are stored in
-// colour-major slots so a colour is a contiguous, coalesced range.
-// The sweep loop is one persistent kernel; colour phases are separated by a
-// bounded grid barrier among only as many blocks as the largest colour needs
-// (a single block synchronises with __syncthreads), and the per-sweep
-// residual max (warp shuffles, then one atomic per block) decides the exit on
-// the device.
-#include "rg_internal.cuh"
+// Execution model.  A "team" of co-resident blocks (cooperative launch) runs
+// every phase of one system's step - free flight, detection, colouring,
+// manifold rows, PSOR sweeps, position update, projection, wrap - for
+// nsteps steps in ONE launch.  Phases are separated by a bounded team
+// barrier instead of kernel boundaries.  Independent systems run as separate
+// teams of one launch (batching).
+//
+// Gauss-Seidel is graph-coloured: Jones-Plassmann first-fit colouring of the
+// contacts (no two contacts of a colour share a dynamic body), computed with
+// per-body atomic maxima of contact priorities and per-body colour masks
+// instead of adjacency lists.  A sweep visits colours in order and the
+// contacts of a colour in parallel; this is sequential Gauss-Seidel over the
+// colour-major permutation of the (a,b)-sorted contacts, bit for bit.  Rows
+// live in colour-major slots so each colour is a contiguous, coalesced range;
+// the per-sweep residual max is a warp-shuffle reduction plus one atomic per
+// block, and the exit test runs on the device.
+#include <cstring>
+
+#include "rg_nsc_dev.cuh"
 
 namespace rg {
 
-const int* detector_n_dev(rg_system* s);
+GridDev* detector_grid(rg_system* s);
+unsigned long long* detector_bounds(rg_system* s);
 
-__device__ inline unsigned long long jp_priority(unsigned c) {
-  unsigned h = c * 0x9E3779B1u;
-  h ^= h >> 16;
-  h *= 0x85EBCA6Bu;
-  h ^= h >> 13;
-  h *= 0xC2B2AE35u;
-  h ^= h >> 16;
-  return ((unsigned long long)h << 32) | (unsigned long long)c;
+// ---------------------------------------------------------------------------
+// Teams and team barriers.
+// ---------------------------------------------------------------------------
+struct TeamDesc {
+  int b0, nb, sys, pad;
+  unsigned int* bar;  // 4 words: full-team count/gen, subset count/gen
+};
+
+struct Team {
+  int b0, nb;
+  unsigned int* bar;
+  int* err;
+  __device__ int rank() const { return (int)blockIdx.x - b0; }
+  __device__ int tid() const { return rank() * (int)blockDim.x + (int)threadIdx.x; }
+  __device__ int size() const { return nb * (int)blockDim.x; }
+};
+
+__device__ inline bool team_sync(const Team& T) {
+  GridBar g{T.bar, T.bar + 1, T.err};
+  return grid_sync(g, (unsigned)T.nb);
+}
+// Barrier among the first nsub blocks of the team (the others must not call it).
+__device__ inline bool team_sync_sub(const Team& T, int nsub) {
+  GridBar g{T.bar + 2, T.bar + 3, T.err};
+  return grid_sync(g, (unsigned)nsub);
 }
 
-__device__ inline double block_max(double v, double* sm) {
+__device__ inline double block_reduce_max(double v, double* sm) {
   v = warp_max(v);
+  __syncthreads();
   if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
   __syncthreads();
-  double r = 0;
-  if (threadIdx.x < 32) {
-    r = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
-    r = warp_max(r);
-  }
+  double r = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+  if (threadIdx.x < 32) r = warp_max(r);
+  return r;  // valid in thread 0
+}
+__device__ inline int block_reduce_sum_i(int v, int* sm) {
+  v = warp_sum_i(v);
   __syncthreads();
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  int r = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0;
+  if (threadIdx.x < 32) r = warp_sum_i(r);
   return r;  // valid in thread 0
 }
 
+// Phase timers (team rank 0, thread 0; %globaltimer in ns) when enabled.
 // ---------------------------------------------------------------------------
-// Colouring + colour-major order (one persistent kernel).
-// ---------------------------------------------------------------------------
-struct ColorIO {
-  const int *ca, *cb;
-  const double* inv_mass;
-  const int *off, *ent;
-  int *col, *tmp, *order, *cnt, *coff;
-  int* remaining;  // kMaxRounds slots
+__device__ inline unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+struct PhaseClock {
+  Ctl* ctl;
+  bool on;
+  unsigned long long t;
+  __device__ PhaseClock(Ctl* c, bool enabled) : ctl(c), on(enabled), t(enabled ? gtimer() : 0) {}
+  __device__ void mark(int k) {
+    if (!on) return;
+    unsigned long long u = gtimer();
+    ctl->phase_ns[k] += (long long)(u - t);
+    t = u;
+  }
 };
-constexpr int kMaxRounds = 512;
 
-__global__ void k_color(ColorIO io, Ctl* ctl, GridBar gb) {
-  if (ctl->err) return;
-  const int C = ctl->contacts;
-  const unsigned nb = gridDim.x;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  __shared__ int s_rem;
-  // init
-  for (int c = tid; c < C; c += stride) io.col[c] = -1;
-  if (tid < kMaxRounds) io.remaining[tid] = 0;
-  if (tid <= kMaxColors) io.cnt[tid] = 0;
-  if (!grid_sync(gb, nb)) return;
-  int* cin = io.col;
-  int* cout = io.tmp;
+struct SmemNsc {
+  BuildSmem build;
+  double red_d[32];
+  int red_i[32];
+  int scan_w[32];
+  int pre[32];
+  int coff[kMaxColors + 1];
+  int bcast;
+};
+
+// Every block computes Σ blk[0..rank) and Σ blk[0..nb).
+__device__ inline void block_prefix(const int* blk, int nb, int rank, int& prefix, int& total, SmemNsc& sm) {
+  int a = 0, b = 0;
+  for (int r = threadIdx.x; r < nb; r += blockDim.x) {
+    int v = *(volatile const int*)&blk[r];
+    b += v;
+    if (r < rank) a += v;
+  }
+  int pa = warp_sum_i(a), pb = warp_sum_i(b);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    sm.pre[threadIdx.x >> 5] = pa;
+    sm.red_i[threadIdx.x >> 5] = pb;
+  }
+  __syncthreads();
+  int x = 0, y = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    x += sm.pre[w];
+    y += sm.red_i[w];
+  }
+  prefix = x;
+  total = y;
+  __syncthreads();
+}
+
+// Exclusive scan of in[0..m) into out[0..m], out[m] = total (team, blocked).
+__device__ inline bool team_excl_scan(const Team& T, const int* in, int* out, int m, int* blk, SmemNsc& sm) {
+  const int rank = T.rank();
+  const int seg = (m + T.nb - 1) / T.nb;
+  const int lo = rank * seg < m ? rank * seg : m;
+  const int hi = lo + seg < m ? lo + seg : m;
+  int s = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) s += in[i];
+  int bsum = block_reduce_sum_i(s, sm.red_i);
+  if (threadIdx.x == 0) blk[rank] = bsum;
+  if (!team_sync(T)) return false;
+  int prefix, total;
+  block_prefix(blk, T.nb, rank, prefix, total, sm);
+  int run = prefix;
+  for (int base = lo; base < hi; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    int v = i < hi ? in[i] : 0;
+    int tot;
+    int ex = block_excl_scan(v, sm.scan_w, tot);
+    if (i < hi) out[i] = run + ex;
+    run += tot;
+  }
+  if (rank == 0 && threadIdx.x == 0) out[m] = total;
+  return team_sync(T);
+}
+
+// ---------------------------------------------------------------------------
+// Detection inside the persistent kernel.
+// ---------------------------------------------------------------------------
+__device__ __noinline__ bool rebuild_phase(const Team& T, const NscView& V, SmemNsc& sm) {
+  Ctl* ctl = V.ctl;
+  const int n = V.st.n;
+  const int tid = T.tid(), TS = T.size(), rank = T.rank();
+  if (!V.box.pbc) {
+    if (rank == 0 && threadIdx.x < 3) {
+      V.bounds[threadIdx.x] = ~0ull;
+      V.bounds[3 + threadIdx.x] = 0ull;
+    }
+    if (!team_sync(T)) return false;
+    for (int i = tid; i < n; i += TS) {
+      Seg s = V.seg[i];
+      atomicMin(&V.bounds[0], ord_key(s.cx)); atomicMax(&V.bounds[3], ord_key(s.cx));
+      atomicMin(&V.bounds[1], ord_key(s.cy)); atomicMax(&V.bounds[4], ord_key(s.cy));
+      atomicMin(&V.bounds[2], ord_key(s.cz)); atomicMax(&V.bounds[5], ord_key(s.cz));
+    }
+    if (!team_sync(T)) return false;
+    if (rank == 0 && threadIdx.x == 0) open_grid(V.bounds, V.bounds + 3, V.cut_center, 64, V.grid);
+    if (!team_sync(T)) return false;
+  }
+  GridDev g;
+  {
+    const volatile GridDev* vg = V.grid;
+    for (int k = 0; k < 3; ++k) {
+      g.lo[k] = vg->lo[k];
+      g.cell[k] = vg->cell[k];
+      g.n[k] = vg->n[k];
+    }
+    g.ncells = vg->ncells;
+  }
+  unsigned long long t_start = (ctl->prof_phases && rank == 0 && threadIdx.x == 0) ? gtimer() : 0;
+  for (int c = tid; c <= g.ncells; c += TS) {
+    V.cell_cnt[c] = 0;
+    V.cell_fill[c] = 0;
+  }
+  for (int i = tid; i < n; i += TS) V.nbr_cnt[i] = 0;
+  if (!team_sync(T)) return false;
+  for (int i = tid; i < n; i += TS) {
+    Seg s = V.seg[i];
+    int cx = cell_coord(s.cx, g.lo[0], g.cell[0], g.n[0], V.box.pbc);
+    int cy = cell_coord(s.cy, g.lo[1], g.cell[1], g.n[1], V.box.pbc);
+    int cz = cell_coord(s.cz, g.lo[2], g.cell[2], g.n[2], V.box.pbc);
+    int c = (cz * g.n[1] + cy) * g.n[0] + cx;
+    V.cell_of[i] = c;
+    atomicAdd(&V.cell_cnt[c], 1);
+  }
+  if (!team_sync(T)) return false;
+  if (!team_excl_scan(T, V.cell_cnt, V.cell_start, g.ncells, V.blk, sm)) return false;
+  for (int i = tid; i < n; i += TS) {
+    int c = V.cell_of[i];
+    V.cell_rods[V.cell_start[c] + atomicAdd(&V.cell_fill[c], 1)] = i;
+  }
+  if (!team_sync(T)) return false;
+  int overflow = 0;
+  double invL[3] = {1.0, 1.0, 1.0};
+  for (int k = 0; k < 3; ++k)
+    if (V.box.L[k] > 0.0) invL[k] = 1.0 / V.box.L[k];
+  for (int cell = rank; cell < g.ncells; cell += T.nb)
+    build_cell_pairs(V.seg, g, V.box, invL, V.cell_start, V.cell_rods, V.margin, V.skin, V.all_pairs,
+                     V.nbr_cnt, V.nbr, V.maxnb, cell, sm.build, overflow);
+  if (!team_sync(T)) return false;
+  for (int i = tid; i < n; i += TS) {
+    sort_list(V.nbr, V.nbr_cnt, V.maxnb, i, overflow);
+    Seg s = V.seg[i];
+    V.ref[i] = s.cx; V.ref[n + i] = s.cy; V.ref[2 * n + i] = s.cz;
+    V.ref[3 * n + i] = s.ux; V.ref[4 * n + i] = s.uy; V.ref[5 * n + i] = s.uz;
+  }
+  if (overflow) atomicOr(&ctl->err, ERR_NBR_CAP);
+  if (!team_sync(T)) return false;
+  if (*(volatile int*)&ctl->err) return false;
+  if (rank == 0 && threadIdx.x == 0) {
+    ctl->rebuild = 0;
+    ctl->rebuilds += 1;
+    if (t_start) ctl->phase_ns[9] += (long long)(gtimer() - t_start);
+  }
+  return true;
+}
+
+// Contacts at the current segment records (V.seg current, ctl->maxdisp
+// accumulated by the caller, all blocks past a team barrier).  Returns the
+// contact count, or -1 on error.
+__device__ __noinline__ int detect_phase(const Team& T, const NscView& V, double delta, SmemNsc& sm) {
+  Ctl* ctl = V.ctl;
+  const int n = V.st.n;
+  const int rank = T.rank();
+  const bool need = *(volatile int*)&ctl->rebuild ||
+                    (!V.all_pairs && *(volatile double*)&ctl->maxdisp >= 0.5 * V.skin * (1.0 - 1e-9));
+  if (need && !rebuild_phase(T, V, sm)) return -1;
+  const int seg = (n + T.nb - 1) / T.nb;
+  const int lo = rank * seg < n ? rank * seg : n;
+  const int hi = lo + seg < n ? lo + seg : n;
+  constexpr int G = 4;  // lanes per rod
+  int mine = 0;
+  for (int base = lo; base < hi; base += blockDim.x / G) {
+    int i = base + threadIdx.x / G;
+    bool valid = i < hi;
+    int c = narrow_count_lanes<G>(i, valid, V.seg, V.st.inv_mass, V.box, delta, V.nbr_cnt, V.nbr, V.maxnb,
+                                  V.words, V.mask);
+    if (valid && (threadIdx.x & (G - 1)) == 0) {
+      V.hit_cnt[i] = c;
+      mine += c;
+    }
+  }
+  int run = block_reduce_sum_i(mine, sm.red_i);
+  if (threadIdx.x == 0) V.blk[rank] = run;
+  if (!team_sync(T)) return -1;
+  if (rank == 0 && threadIdx.x == 0) ctl->maxdisp = 0.0;  // every block has read it
+  int prefix, total;
+  block_prefix(V.blk, T.nb, rank, prefix, total, sm);
+  if (total > V.ccap) {
+    if (rank == 0 && threadIdx.x == 0) atomicOr(&ctl->err, ERR_CONTACT_CAP);
+    return -1;
+  }
+  run = prefix;
+  for (int base = lo; base < hi; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    int c = i < hi ? V.hit_cnt[i] : 0;
+    int tot;
+    int ex = block_excl_scan(c, sm.scan_w, tot);
+    if (c) narrow_write_rod(i, run + ex, V.seg, V.box, V.nbr_cnt, V.nbr, V.maxnb, V.words, V.mask, V.con);
+    run += tot;
+  }
+  if (rank == 0 && threadIdx.x == 0) ctl->contacts = total;
+  if (!team_sync(T)) return -1;
+  return total;
+}
+
+// ---------------------------------------------------------------------------
+// Colouring: Jones-Plassmann first fit with per-body priority maxima.
+// ---------------------------------------------------------------------------
+__device__ __noinline__ bool color_phase(const Team& T, const NscView& V, int C, SmemNsc& sm) {
+  Ctl* ctl = V.ctl;
+  const int n = V.st.n;
+  const int tid = T.tid(), TS = T.size(), rank = T.rank();
+  const double* im = V.st.inv_mass;
+  for (int c = tid; c < C; c += TS) {
+    int x[2] = {V.con.a[c], V.con.b[c]};
+    for (int k = 0; k < 2; ++k) {
+      if (!(im[x[k]] > 0.0)) continue;
+      V.pmax[x[k]] = 0;
+      V.pmax[n + x[k]] = 0;
+      V.cmask[x[k]] = 0;
+      V.owner[x[k]] = 0x7fffffff;
+    }
+    V.color[c] = -1;
+  }
+  if (rank == 0) {
+    for (int k = threadIdx.x; k <= kMaxColors; k += blockDim.x) {
+      V.color_cnt[k] = 0;
+      V.cursor[k] = 0;
+    }
+    for (int r = threadIdx.x; r < kMaxRounds; r += blockDim.x) V.remaining[r] = 0;
+    if (threadIdx.x == 0) ctl->colors = 0;
+  }
+  if (!team_sync(T)) return false;
   int round = 0;
-  int maxc = 0;
   for (; round < kMaxRounds; ++round) {
-    if (threadIdx.x == 0) s_rem = 0;
-    __syncthreads();
-    int rem = 0;
-    for (int c = tid; c < C; c += stride) {
-      int cc = cin[c];
-      if (cc >= 0) {
-        cout[c] = cc;
-        continue;
+    unsigned long long* pm = V.pmax + (size_t)(round & 1) * n;
+    unsigned long long* pn = V.pmax + (size_t)((round + 1) & 1) * n;
+    for (int c = tid; c < C; c += TS) {
+      if (V.color[c] >= 0) continue;
+      int x[2] = {V.con.a[c], V.con.b[c]};
+      unsigned long long p = jp_priority((unsigned)c);
+      for (int k = 0; k < 2; ++k) {
+        if (!(im[x[k]] > 0.0)) continue;
+        atomicMax(&pm[x[k]], p);
+        if (round == 0) atomicMin(&V.owner[x[k]], c);
       }
-      unsigned long long pc = jp_priority((unsigned)c);
-      bool best = true;
+    }
+    if (!team_sync(T)) return false;
+    int rem = 0, maxc = 0;
+    for (int c = tid; c < C; c += TS) {
+      if (V.color[c] >= 0) continue;
+      int x[2] = {V.con.a[c], V.con.b[c]};
+      unsigned long long p = jp_priority((unsigned)c);
+      bool win = true;
       unsigned long long used = 0;
-      for (int side = 0; side < 2; ++side) {
-        int bd = side ? io.cb[c] : io.ca[c];
-        if (!(io.inv_mass[bd] > 0.0)) continue;
-        for (int k = io.off[bd]; k < io.off[bd + 1]; ++k) {
-          int o = io.ent[k] >> 1;
-          if (o == c) continue;
-          int co = cin[o];
-          if (co >= 0) used |= 1ull << co;
-          else if (jp_priority((unsigned)o) > pc) best = false;
-        }
+      for (int k = 0; k < 2; ++k) {
+        if (!(im[x[k]] > 0.0)) continue;
+        if (*(volatile unsigned long long*)&pm[x[k]] != p) win = false;
+        used |= *(volatile unsigned long long*)&V.cmask[x[k]];
+        pn[x[k]] = 0;
       }
-      if (best) {
-        int k = __ffsll((long long)~used) - 1;
+      if (win) {
+        int col = __ffsll((long long)~used) - 1;
         if (used == ~0ull) {
           atomicOr(&ctl->err, ERR_COLOR);
-          k = kMaxColors - 1;
+          col = kMaxColors - 1;
         }
-        cout[c] = k;
-        maxc = k + 1 > maxc ? k + 1 : maxc;
+        V.color[c] = col;
+        for (int k = 0; k < 2; ++k)
+          if (im[x[k]] > 0.0) atomicOr(&V.cmask[x[k]], 1ull << col);
+        atomicAdd(&V.color_cnt[col], 1);
+        maxc = col + 1 > maxc ? col + 1 : maxc;
       } else {
-        cout[c] = -1;
         ++rem;
       }
     }
-    rem = warp_sum_i(rem);
-    if ((threadIdx.x & 31) == 0 && rem) atomicAdd(&s_rem, rem);
-    __syncthreads();
-    if (threadIdx.x == 0 && s_rem) atomicAdd(&io.remaining[round], s_rem);
-    if (!grid_sync(gb, nb)) return;
-    int* t = cin; cin = cout; cout = t;
-    if (*(volatile int*)&io.remaining[round] == 0) break;
+    int br = block_reduce_sum_i(rem, sm.red_i);
+    if (threadIdx.x == 0 && br) atomicAdd(&V.remaining[round], br);
+    if (maxc) atomicMax(&ctl->colors, maxc);
+    if (!team_sync(T)) return false;
+    if (*(volatile int*)&V.remaining[round] == 0) break;
   }
   if (round >= kMaxRounds) {
-    if (tid == 0) atomicOr(&ctl->err, ERR_COLOR);
-    return;
+    if (rank == 0 && threadIdx.x == 0) atomicOr(&ctl->err, ERR_COLOR);
+    return false;
   }
-  // final colours are in cin; copy to io.col if needed, count per colour
-  for (int c = tid; c < C; c += stride) {
-    int k = cin[c];
-    if (cin != io.col) io.col[c] = k;
-    atomicAdd(&io.cnt[k], 1);
-  }
-  if (maxc) atomicMax(&ctl->colors, maxc);
-  if (!grid_sync(gb, nb)) return;
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
     int acc = 0;
     for (int k = 0; k <= kMaxColors; ++k) {
-      int v = k < kMaxColors ? io.cnt[k] : 0;
-      io.coff[k] = acc;
-      acc += v;
-      if (k < kMaxColors) io.cnt[k] = 0;
+      sm.coff[k] = acc;
+      if (k < kMaxColors) acc += *(volatile int*)&V.color_cnt[k];
     }
   }
-  if (!grid_sync(gb, nb)) return;
-  for (int c = tid; c < C; c += stride) {
-    int k = io.col[c];
-    io.order[io.coff[k] + atomicAdd(&io.cnt[k], 1)] = c;
+  __syncthreads();
+  if (rank == 0)
+    for (int k = threadIdx.x; k <= kMaxColors; k += blockDim.x) V.color_off[k] = sm.coff[k];
+  for (int c = tid; c < C; c += TS) {
+    int k = V.color[c];
+    V.order[sm.coff[k] + atomicAdd(&V.cursor[k], 1)] = c;
   }
-}
-
-__global__ void k_zero_ctl_colors(Ctl* ctl) {
-  if (ctl->err) return;
-  ctl->colors = 0;
-  ctl->bar_count = 0;
-}
-
-static void launch_coop(const void* fn, int grid, int block, void** args, cudaStream_t st) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(block);
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  RGL cudaLaunchKernelExC(&cfg, fn, args);
-}
-
-static GridBar bar_of(rg_system* s) {
-  GridBar g;
-  g.count = &s->d_ctl->bar_count;
-  g.gen = &s->d_ctl->bar_gen;
-  g.err = &s->d_ctl->err;
-  return g;
-}
-
-void color_launch(rg_system* s) {
-  RGL k_zero_ctl_colors<<<1, 1, 0, s->stream>>>(s->d_ctl);
-  ColorIO io;
-  io.ca = s->con.a; io.cb = s->con.b; io.inv_mass = s->st.inv_mass;
-  io.off = s->csr.off; io.ent = s->csr.ent;
-  io.col = s->nsc.color; io.tmp = s->nsc.color_tmp; io.order = s->nsc.order;
-  io.cnt = s->nsc.color_cnt; io.coff = s->nsc.color_off;
-  io.remaining = s->nsc.color_tmp + s->ccap;  // kMaxRounds slots after tmp
-  Ctl* ctl = s->d_ctl;
-  GridBar gb = bar_of(s);
-  void* args[] = {&io, &ctl, &gb};
-  launch_coop((const void*)k_color, s->coop_blocks, 256, args, s->stream);
+  return team_sync(T);
 }
 
 // ---------------------------------------------------------------------------
-// Manifold build (rows in colour-major slots) and warm start.
+// PSOR sweeps.
 // ---------------------------------------------------------------------------
-struct RowIO {
-  double* row;  // kRowComps * ccap
-  double* lam;  // 3 * ccap (slot order)
-  int ccap;
-  __device__ double& r(int k, int p) const { return row[(size_t)k * ccap + p]; }
-  __device__ d3 r3(int k, int p) const { return {r(k, p), r(k + 1, p), r(k + 2, p)}; }
-  __device__ void w3(int k, int p, d3 v) const { r(k, p) = v.x; r(k + 1, p) = v.y; r(k + 2, p) = v.z; }
-};
-enum { R_N = 0, R_T1 = 3, R_T2 = 6, R_RA = 9, R_RB = 12, R_IAN = 15, R_IAT1 = 18, R_IAT2 = 21,
-       R_IBN = 24, R_IBT1 = 27, R_IBT2 = 30, R_IMA = 33, R_IMB = 34, R_GN = 35, R_GT1 = 36,
-       R_GT2 = 37, R_BN = 38, R_BREST = 39, R_PHI = 40, R_VNPRE = 41 };
-
-__device__ inline d3 iinv_apply(const State& st, int i, d3 v) {
-  if (st.inv_mass[i] <= 0.0) return {0, 0, 0};
-  return rot_diag_apply(st.q.ld(i), st.Iinv.ld(i), v);
-}
-__device__ inline double diag_of(const State& st, int a, int b, d3 ra, d3 rb, d3 d, double cfm) {
-  d3 rad = cross(ra, d), rbd = cross(rb, d);
-  double g = st.inv_mass[a] + st.inv_mass[b] + dot(rad, iinv_apply(st, a, rad)) +
-             dot(rbd, iinv_apply(st, b, rbd)) + cfm;
-  return smax(g, 1e-12);
-}
-
-__device__ inline int lower_bound_key(const unsigned long long* k, int n, unsigned long long v) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    int m = (lo + hi) >> 1;
-    if (k[m] < v) lo = m + 1;
-    else hi = m;
-  }
-  return lo;
-}
-
-__global__ void k_manifolds(State st, Contacts con, rg_config cfg, const int* order, RowIO R,
-                            const unsigned long long* wkey, const double* wlam, const int* wn,
-                            int wcap, Ctl* ctl) {
-  if (ctl->err) return;
-  const int C = ctl->contacts;
-  const double beta = cfg.nsc_position_stabilization ? cfg.nsc_beta * 0.01 : cfg.nsc_beta;
-  const int W = *wn;
-  long long coll = 0;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < C; p += gridDim.x * blockDim.x) {
-    const int c = order[p];
-    const int a = con.a[c], b = con.b[c];
-    d3 pa{con.comp(0)[c], con.comp(1)[c], con.comp(2)[c]};
-    d3 pb{con.comp(3)[c], con.comp(4)[c], con.comp(5)[c]};
-    d3 n{con.comp(6)[c], con.comp(7)[c], con.comp(8)[c]};
-    d3 sh{con.comp(9)[c], con.comp(10)[c], con.comp(11)[c]};
-    double phi = con.comp(12)[c] - con.comp(13)[c];
-    d3 ref = fabs(n.x) < 0.9 ? mk3(1, 0, 0) : mk3(0, 1, 0);
-    d3 cr = cross(n, ref);
-    d3 t1 = cr / len(cr);
-    d3 t2 = cross(n, t1);
-    d3 ra = pa - st.x.ld(a);
-    d3 rb = pb - (st.x.ld(b) + sh);
-    R.w3(R_N, p, n); R.w3(R_T1, p, t1); R.w3(R_T2, p, t2);
-    R.w3(R_RA, p, ra); R.w3(R_RB, p, rb);
-    R.r(R_GN, p) = diag_of(st, a, b, ra, rb, n, cfg.nsc_cfm);
-    R.r(R_GT1, p) = diag_of(st, a, b, ra, rb, t1, cfg.nsc_cfm);
-    R.r(R_GT2, p) = diag_of(st, a, b, ra, rb, t2, cfg.nsc_cfm);
-    R.r(R_IMA, p) = st.inv_mass[a];
-    R.r(R_IMB, p) = st.inv_mass[b];
-    R.w3(R_IAN, p, iinv_apply(st, a, cross(ra, n)));
-    R.w3(R_IAT1, p, iinv_apply(st, a, cross(ra, t1)));
-    R.w3(R_IAT2, p, iinv_apply(st, a, cross(ra, t2)));
-    R.w3(R_IBN, p, iinv_apply(st, b, cross(rb, n)));
-    R.w3(R_IBT1, p, iinv_apply(st, b, cross(rb, t1)));
-    R.w3(R_IBT2, p, iinv_apply(st, b, cross(rb, t2)));
-    d3 vrel = (st.v.ld(b) + cross(st.w.ld(b), rb)) - (st.v.ld(a) + cross(st.w.ld(a), ra));
-    double vnp = dot(n, vrel);
-    double e = smin(st.rest[a], st.rest[b]);
-    R.r(R_BN, p) = phi < 0.0 ? beta * phi / cfg.dt : 0.0;
-    R.r(R_BREST, p) = vnp < 0.0 ? e * vnp : 0.0;
-    R.r(R_PHI, p) = phi;
-    R.r(R_VNPRE, p) = vnp;
-    if (vnp < -1e-6) ++coll;
-    double l0 = 0, l1 = 0, l2 = 0;
-    if (cfg.nsc_warm_start == RG_WARM_CACHE && W > 0) {
-      unsigned long long k = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
-      int q = lower_bound_key(wkey, W, k);
-      if (q < W && wkey[q] == k) {
-        l0 = smax(0.0, wlam[q]);
-        l1 = wlam[wcap + q];
-        l2 = wlam[2 * wcap + q];
-      }
-    }
-    R.lam[p] = l0;
-    R.lam[R.ccap + p] = l1;
-    R.lam[2 * R.ccap + p] = l2;
-  }
-  if (coll) atomicAdd((unsigned long long*)&ctl->collisions, (unsigned long long)coll);
-}
-
-// ---------------------------------------------------------------------------
-// PSOR sweeps (persistent).
-// ---------------------------------------------------------------------------
-struct Vel {
-  Vec3A v, w;
-};
-
-__device__ inline void apply_imp(const Vel& V, int a, int b, d3 d, d3 IA, d3 IB, double ima,
-                                 double imb, double l) {
-  V.v.st(a, V.v.ld(a) - d * (l * ima));
-  V.w.st(a, V.w.ld(a) - IA * l);
-  V.v.st(b, V.v.ld(b) + d * (l * imb));
-  V.w.st(b, V.w.ld(b) + IB * l);
-}
-
-__device__ inline double psor_row(const RowIO& R, const Vel& V, int p, int a, int b, double omega,
-                                  double cfm, double mu) {
-  d3 n = R.r3(R_N, p), t1 = R.r3(R_T1, p), t2 = R.r3(R_T2, p);
-  d3 ra = R.r3(R_RA, p), rb = R.r3(R_RB, p);
-  d3 IAn = R.r3(R_IAN, p), IAt1 = R.r3(R_IAT1, p), IAt2 = R.r3(R_IAT2, p);
-  d3 IBn = R.r3(R_IBN, p), IBt1 = R.r3(R_IBT1, p), IBt2 = R.r3(R_IBT2, p);
-  double ima = R.r(R_IMA, p), imb = R.r(R_IMB, p);
-  double ln = R.lam[p], lt1 = R.lam[R.ccap + p], lt2 = R.lam[2 * R.ccap + p];
-  d3 vA = V.v.ld(a), wA = V.w.ld(a), vB = V.v.ld(b), wB = V.w.ld(b);
-  d3 vrel = (vB + cross(wB, rb)) - (vA + cross(wA, ra));
-  double wn = dot(n, vrel) + R.r(R_BN, p) + R.r(R_BREST, p) + cfm * ln;
-  double dn_ = -(omega / R.r(R_GN, p)) * wn;
-  double old = ln;
-  ln = smax(0.0, old + dn_);
-  double dn = ln - old;
-  if (dn != 0.0) {
-    d3 dvA = n * (dn * ima);
-    vA = vA - dvA;
-    wA = wA - IAn * dn;
-    vrel = vrel + (dvA + cross(IAn * dn, ra));
-    d3 dvB = n * (dn * imb);
-    vB = vB + dvB;
-    wB = wB + IBn * dn;
-    vrel = vrel + (dvB + cross(IBn * dn, rb));
-  }
-  double mf = mu * ln;
-  double lim1 = sqrt(smax(0.0, mf * mf - lt2 * lt2));
-  double w1 = dot(t1, vrel) + cfm * lt1;
-  double d1_ = -(omega / R.r(R_GT1, p)) * w1;
-  double o1 = lt1;
-  lt1 = smin(smax(o1 + d1_, -lim1), lim1);
-  double d1 = lt1 - o1;
-  if (d1 != 0.0) {
-    d3 dvA = t1 * (d1 * ima);
-    vA = vA - dvA;
-    wA = wA - IAt1 * d1;
-    vrel = vrel + (dvA + cross(IAt1 * d1, ra));
-    d3 dvB = t1 * (d1 * imb);
-    vB = vB + dvB;
-    wB = wB + IBt1 * d1;
-    vrel = vrel + (dvB + cross(IBt1 * d1, rb));
-  }
-  double lim2 = sqrt(smax(0.0, mf * mf - lt1 * lt1));
-  double w2 = dot(t2, vrel) + cfm * lt2;
-  double d2_ = -(omega / R.r(R_GT2, p)) * w2;
-  double o2 = lt2;
-  lt2 = smin(smax(o2 + d2_, -lim2), lim2);
-  double d2 = lt2 - o2;
-  if (d2 != 0.0) {
-    vA = vA - t2 * (d2 * ima);
-    wA = wA - IAt2 * d2;
-    vB = vB + t2 * (d2 * imb);
-    wB = wB + IBt2 * d2;
-  }
-  if (dn != 0.0 || d1 != 0.0 || d2 != 0.0) {
-    V.v.st(a, vA); V.w.st(a, wA);
-    V.v.st(b, vB); V.w.st(b, wB);
-    R.lam[p] = ln; R.lam[R.ccap + p] = lt1; R.lam[2 * R.ccap + p] = lt2;
-  }
-  return fabs(dn) + fabs(d1) + fabs(d2);
-}
-
-__device__ inline unsigned active_blocks(const int* coff, int ncol, int bs, unsigned grid) {
+__device__ inline int active_blocks(const int* coff, int ncol, int bs, int nb) {
   int m = 0;
   for (int k = 0; k < ncol; ++k) {
     int c = coff[k + 1] - coff[k];
     m = c > m ? c : m;
   }
-  unsigned need = (unsigned)((m + bs - 1) / bs);
+  int need = (m + bs - 1) / bs;
   if (need < 1) need = 1;
-  return need < grid ? need : grid;
+  return need < nb ? need : nb;
 }
 
-__global__ void k_psor(State st, rg_config cfg, const int* order, const int* ca, const int* cb,
-                       RowIO R, const int* coff, Ctl* ctl, GridBar gb) {
-  if (ctl->err) return;
-  const int C = ctl->contacts;
-  const int K = ctl->colors;
-  __shared__ double sm[32];
-  if (C == 0) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      ctl->sweeps_last = 0;
-      ctl->residual = 0.0;
-    }
-    return;
-  }
-  const unsigned nb = active_blocks(coff, K, blockDim.x, gridDim.x);
-  if (blockIdx.x >= nb) return;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = nb * blockDim.x;
-  Vel V{st.v, st.w};
-  const double omega = cfg.nsc_omega, cfm = cfg.nsc_cfm, mu = cfg.nsc_mu;
-  const int iters = cfg.nsc_velocity_iters;
-  for (int i = tid; i < iters; i += stride) ctl->res_sweep[i] = 0.0;
-  // warm start, colour by colour (nsc_contact.cpp:344-380)
-  if (cfg.nsc_warm_start != RG_WARM_NONE) {
-    for (int k = 0; k < K; ++k) {
-      for (int p = coff[k] + tid; p < coff[k + 1]; p += stride) {
-        int c = order[p];
-        int a = ca[c], b = cb[c];
-        double ima = R.r(R_IMA, p), imb = R.r(R_IMB, p);
-        double ln = R.lam[p], l1 = R.lam[R.ccap + p], l2 = R.lam[2 * R.ccap + p];
-        if (ln != 0.0) apply_imp(V, a, b, R.r3(R_N, p), R.r3(R_IAN, p), R.r3(R_IBN, p), ima, imb, ln);
-        if (l1 != 0.0) apply_imp(V, a, b, R.r3(R_T1, p), R.r3(R_IAT1, p), R.r3(R_IBT1, p), ima, imb, l1);
-        if (l2 != 0.0) apply_imp(V, a, b, R.r3(R_T2, p), R.r3(R_IAT2, p), R.r3(R_IBT2, p), ima, imb, l2);
+__device__ __noinline__ bool psor_phase(const Team& T, const NscView& V, int C, SmemNsc& sm) {
+  Ctl* ctl = V.ctl;
+  const int K = *(volatile int*)&ctl->colors;
+  const int rank = T.rank();
+  const rg_config& cfg = V.cfg;
+  if (C > 0) {
+    const int na = active_blocks(V.color_off, K, blockDim.x, T.nb);
+    if (rank < na) {
+      const int tid = rank * blockDim.x + threadIdx.x, stride = na * blockDim.x;
+      RowIO R{V.row, V.lam, V.ccap};
+      Vel Vv{V.st.v, V.st.w};
+      const double omega = cfg.nsc_omega, cfm = cfg.nsc_cfm, mu = cfg.nsc_mu;
+      const int iters = cfg.nsc_velocity_iters;
+      const int* coff = V.color_off;
+      for (int i = tid; i < iters; i += stride) ctl->res_sweep[i] = 0.0;
+      if (cfg.nsc_warm_start != RG_WARM_NONE) {
+        for (int k = 0; k < K; ++k) {
+          for (int p = coff[k] + tid; p < coff[k + 1]; p += stride) {
+            int c = V.order[p];
+            warm_apply(R, Vv, p, V.con.a[c], V.con.b[c]);
+          }
+          if (!team_sync_sub(T, na)) return false;
+        }
+      } else if (!team_sync_sub(T, na)) {
+        return false;
       }
-      if (!grid_sync(gb, nb)) return;
-    }
-  } else {
-    if (!grid_sync(gb, nb)) return;
-  }
-  double res = 0.0;
-  int sweeps = 0;
-  for (int it = 0; it < iters; ++it) {
-    double loc = 0.0;
-    for (int k = 0; k < K; ++k) {
-      for (int p = coff[k] + tid; p < coff[k + 1]; p += stride) {
-        int c = order[p];
-        loc = fmax(loc, psor_row(R, V, p, ca[c], cb[c], omega, cfm, mu));
+      double res = 0.0;
+      int sweeps = 0;
+      for (int it = 0; it < iters; ++it) {
+        double loc = 0.0;
+        for (int k = 0; k < K; ++k) {
+          for (int p = coff[k] + tid; p < coff[k + 1]; p += stride) {
+            int c = V.order[p];
+            loc = fmax(loc, psor_row(R, Vv, p, V.con.a[c], V.con.b[c], omega, cfm, mu));
+          }
+          if (k + 1 < K && !team_sync_sub(T, na)) return false;
+        }
+        double bm = block_reduce_max(loc, sm.red_d);
+        if (threadIdx.x == 0) atomic_max_nonneg(&ctl->res_sweep[it], bm);
+        if (!team_sync_sub(T, na)) return false;
+        res = *(volatile double*)&ctl->res_sweep[it];
+        sweeps = it + 1;
+        if (res < cfg.nsc_tol) break;
       }
-      if (k + 1 < K && !grid_sync(gb, nb)) return;
+      if (tid == 0) {
+        ctl->residual = res;
+        ctl->sweeps_last = sweeps;
+        ctl->sweeps_sum += sweeps;
+        ctl->row_sweeps += (long long)C * sweeps;
+        if (res >= cfg.nsc_tol) ctl->not_conv += 1;
+        if (res > ctl->max_residual) ctl->max_residual = res;
+      }
     }
-    double bm = block_max(loc, sm);
-    if (threadIdx.x == 0) atomic_max_nonneg(&ctl->res_sweep[it], bm);
-    if (!grid_sync(gb, nb)) return;
-    res = *(volatile double*)&ctl->res_sweep[it];
-    sweeps = it + 1;
-    if (res < cfg.nsc_tol) break;
+  } else if (rank == 0 && threadIdx.x == 0) {
+    ctl->residual = 0.0;
+    ctl->sweeps_last = 0;
   }
-  if (tid == 0) {
-    ctl->residual = res;
-    ctl->sweeps_last = sweeps;
-    ctl->sweeps_sum += sweeps;
-    ctl->row_sweeps += (long long)C * sweeps;
-    if (res >= cfg.nsc_tol) ctl->not_conv += 1;
-    if (res > ctl->max_residual) ctl->max_residual = res;
-  }
-}
-
-// Warm cache for the next step (contact order, so keys stay sorted) and
-// impulse statistics.
-__global__ void k_warm_save(Contacts con, const int* order, const int* color, RowIO R,
-                            unsigned long long* wkey, double* wlam, int* wn, int wcap, Ctl* ctl) {
-  if (ctl->err) return;
-  const int C = ctl->contacts;
-  __shared__ double sm[32];
-  double jn = 0, jt = 0;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < C; p += gridDim.x * blockDim.x) {
-    int c = order[p];
-    double l0 = R.lam[p], l1 = R.lam[R.ccap + p], l2 = R.lam[2 * R.ccap + p];
-    wkey[c] = ((unsigned long long)(unsigned)con.a[c] << 32) | (unsigned)con.b[c];
-    wlam[c] = l0; wlam[wcap + c] = l1; wlam[2 * wcap + c] = l2;
-    reinterpret_cast<int*>(wlam + 3 * (size_t)wcap)[c] = color[c];
-    jn += l0;
-    jt += sqrt(l1 * l1 + l2 * l2);
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    *wn = C;
-    ctl->vel_contacts = C;
-  }
-  jn = warp_sum(jn);
-  jt = warp_sum(jt);
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&ctl->jn_sum, jn);
-    atomicAdd(&ctl->jt_sum, jt);
-  }
-  (void)sm;
-}
-
-__global__ void k_nsc_begin(Ctl* ctl) {
-  if (ctl->err) return;
-  ctl->collisions = 0;
-  ctl->jn_sum = 0;
-  ctl->jt_sum = 0;
+  return team_sync(T);
 }
 
 // ---------------------------------------------------------------------------
-// Position projection (persistent): rows from the pass-0 detection, then
-// narrow phase on the cached pairs in later passes.
+// Position projection (rows from the pass-0 detection, then narrow phase on
+// the cached pairs in later passes).  Runs on the na active blocks.
 // ---------------------------------------------------------------------------
-enum { P_N = 0, P_RA = 3, P_RB = 6, P_PHI = 9, P_G = 10, P_L = 11 };
-
-__global__ void k_project(State st, rg_config cfg, Box box, Contacts con, const int* order,
-                          const int* coff, const int* off, const int* ent, double* prow, int* pact,
-                          double* dxb, int ccap, Ctl* ctl, GridBar gb) {
-  if (ctl->err) return;
-  const int C = ctl->contacts;
-  const int K = ctl->colors;
-  if (C == 0 || !cfg.nsc_position_stabilization) return;
-  const unsigned nb = active_blocks(coff, K, blockDim.x, gridDim.x);
-  if (blockIdx.x >= nb) return;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = nb * blockDim.x;
+__device__ __noinline__ bool project_rows(const NscView& V, int C, int K, int na, int rank, const Team& T, SmemNsc& sm) {
+  Ctl* ctl = V.ctl;
+  const rg_config& cfg = V.cfg;
+  const State& st = V.st;
   const int n = st.n;
+  const int tid = rank * blockDim.x + threadIdx.x, stride = na * blockDim.x;
   const double omega = cfg.nsc_omega, cfm = cfg.nsc_cfm, slop = cfg.nsc_slop;
-  __shared__ double sm[32];
-  __shared__ int s_cnt;
-  auto P = [&](int k, int p) -> double& { return prow[(size_t)k * ccap + p]; };
-  Vec3A DX{dxb, dxb + n, dxb + 2 * n}, DT{dxb + 3 * n, dxb + 4 * n, dxb + 5 * n};
-  double* slots = ctl->res_sweep;  // reused: [0..iters) per-sweep max, then counters
+  const int* coff = V.color_off;
+  const size_t ccap = (size_t)V.ccap;
+  double* PR = V.prow;
+  Vec3A DX{V.dx, V.dx + n, V.dx + 2 * n}, DT{V.dx + 3 * n, V.dx + 4 * n, V.dx + 5 * n};
+  double* slots = ctl->res_sweep;
   const int piters = cfg.nsc_position_psor_iters;
   for (int outer = 0; outer < cfg.nsc_position_iters; ++outer) {
     for (int i = tid; i < piters + 1; i += stride) slots[i] = 0.0;
-    if (threadIdx.x == 0) s_cnt = 0;
-    if (!grid_sync(gb, nb)) return;
+    if (!team_sync_sub(T, na)) return false;
     int cnt = 0;
     for (int p = tid; p < C; p += stride) {
-      const int c = order[p];
-      const int a = con.a[c], b = con.b[c];
+      const int c = V.order[p];
+      const int a = V.con.a[c], b = V.con.b[c];
       d3 xa = st.x.ld(a), xb = st.x.ld(b);
       d3 nv, ra, rb;
       double phi;
       if (outer == 0) {
-        phi = con.comp(12)[c] - con.comp(13)[c];
-        nv = mk3(con.comp(6)[c], con.comp(7)[c], con.comp(8)[c]);
-        d3 pa{con.comp(0)[c], con.comp(1)[c], con.comp(2)[c]};
-        d3 pb{con.comp(3)[c], con.comp(4)[c], con.comp(5)[c]};
-        d3 sh{con.comp(9)[c], con.comp(10)[c], con.comp(11)[c]};
+        phi = V.con.comp(12)[c] - V.con.comp(13)[c];
+        nv = mk3(V.con.comp(6)[c], V.con.comp(7)[c], V.con.comp(8)[c]);
+        d3 pa{V.con.comp(0)[c], V.con.comp(1)[c], V.con.comp(2)[c]};
+        d3 pb{V.con.comp(3)[c], V.con.comp(4)[c], V.con.comp(5)[c]};
+        d3 sh{V.con.comp(9)[c], V.con.comp(10)[c], V.con.comp(11)[c]};
         ra = pa - xa;
         rb = pb - (xb + sh);
       } else {
-        Seg A, B;
-        d3 ua = axis_y(st.q.ld(a)), ub = axis_y(st.q.ld(b));
-        A.cx = xa.x; A.cy = xa.y; A.cz = xa.z; A.h = st.h[a]; A.ux = ua.x; A.uy = ua.y; A.uz = ua.z; A.r = st.r[a];
-        B.cx = xb.x; B.cy = xb.y; B.cz = xb.z; B.h = st.h[b]; B.ux = ub.x; B.uy = ub.y; B.uz = ub.z; B.r = st.r[b];
-        Narrow nr = narrow_pair(A, B, box);
+        Seg A = make_seg(st, a), B = make_seg(st, b);
+        Narrow nr = narrow_pair(A, B, V.box);
         d3 diff = nr.pb - nr.pa;
         double dist = len(diff);
-        phi = dist - con.comp(13)[c];
+        phi = dist - V.con.comp(13)[c];
         nv = dist > 1e-10 ? diff / dist : mk3(1, 0, 0);
         ra = nr.pa - xa;
         rb = nr.pb - (xb + nr.sh);
       }
       int act = phi < -slop ? 1 : 0;
-      pact[p] = act;
+      V.pactive[p] = act;
       if (act) {
         ++cnt;
-        P(P_N, p) = nv.x; P(P_N + 1, p) = nv.y; P(P_N + 2, p) = nv.z;
-        P(P_RA, p) = ra.x; P(P_RA + 1, p) = ra.y; P(P_RA + 2, p) = ra.z;
-        P(P_RB, p) = rb.x; P(P_RB + 1, p) = rb.y; P(P_RB + 2, p) = rb.z;
-        P(P_PHI, p) = phi + slop;
-        P(P_G, p) = diag_of(st, a, b, ra, rb, nv, cfm);
-        P(P_L, p) = 0.0;
+        PR[P_N * ccap + p] = nv.x; PR[(P_N + 1) * ccap + p] = nv.y; PR[(P_N + 2) * ccap + p] = nv.z;
+        PR[P_RA * ccap + p] = ra.x; PR[(P_RA + 1) * ccap + p] = ra.y; PR[(P_RA + 2) * ccap + p] = ra.z;
+        PR[P_RB * ccap + p] = rb.x; PR[(P_RB + 1) * ccap + p] = rb.y; PR[(P_RB + 2) * ccap + p] = rb.z;
+        PR[P_PHI * ccap + p] = phi + slop;
+        PR[P_G * ccap + p] = diag_of(st, a, b, ra, rb, nv, cfm);
+        PR[P_L * ccap + p] = 0.0;
       }
       DX.st(a, mk3(0, 0, 0)); DT.st(a, mk3(0, 0, 0));
       DX.st(b, mk3(0, 0, 0)); DT.st(b, mk3(0, 0, 0));
     }
-    cnt = warp_sum_i(cnt);
-    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&s_cnt, cnt);
-    __syncthreads();
-    if (threadIdx.x == 0 && s_cnt) atomicAdd((unsigned long long*)&slots[piters], (unsigned long long)s_cnt);
-    if (!grid_sync(gb, nb)) return;
-    if (*(volatile unsigned long long*)&slots[piters] == 0ull) return;  // nothing penetrates
+    int bc = block_reduce_sum_i(cnt, sm.red_i);
+    if (threadIdx.x == 0 && bc)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&slots[piters]), (unsigned long long)bc);
+    if (!team_sync_sub(T, na)) return false;
+    if (*(volatile unsigned long long*)&slots[piters] == 0ull) return true;  // nothing penetrates
     for (int it = 0; it < piters; ++it) {
       double loc = 0.0;
       for (int k = 0; k < K; ++k) {
         for (int p = coff[k] + tid; p < coff[k + 1]; p += stride) {
-          if (!pact[p]) continue;
-          const int c = order[p];
-          const int a = con.a[c], b = con.b[c];
-          d3 nv{P(P_N, p), P(P_N + 1, p), P(P_N + 2, p)};
-          d3 ra{P(P_RA, p), P(P_RA + 1, p), P(P_RA + 2, p)};
-          d3 rb{P(P_RB, p), P(P_RB + 1, p), P(P_RB + 2, p)};
-          double l = P(P_L, p);
+          if (!V.pactive[p]) continue;
+          const int c = V.order[p];
+          const int a = V.con.a[c], b = V.con.b[c];
+          d3 nv{PR[P_N * ccap + p], PR[(P_N + 1) * ccap + p], PR[(P_N + 2) * ccap + p]};
+          d3 ra{PR[P_RA * ccap + p], PR[(P_RA + 1) * ccap + p], PR[(P_RA + 2) * ccap + p]};
+          d3 rb{PR[P_RB * ccap + p], PR[(P_RB + 1) * ccap + p], PR[(P_RB + 2) * ccap + p]};
+          double l = PR[P_L * ccap + p];
           double corr = dot(nv, ((DX.ld(b) + cross(DT.ld(b), rb)) - DX.ld(a)) - cross(DT.ld(a), ra));
-          double r = corr + P(P_PHI, p) + cfm * l;
-          double d = -(omega / P(P_G, p)) * r;
+          double r = corr + PR[P_PHI * ccap + p] + cfm * l;
+          double d = -(omega / PR[P_G * ccap + p]) * r;
           double nl = smax(0.0, l + d);
           double dl = nl - l;
           if (dl != 0.0) {
-            P(P_L, p) = nl;
+            PR[P_L * ccap + p] = nl;
             d3 rAxn = cross(ra, nv);
             DX.st(a, DX.ld(a) - nv * (dl * st.inv_mass[a]));
             DT.st(a, DT.ld(a) - iinv_apply(st, a, rAxn) * dl);
@@ -577,21 +552,19 @@ __global__ void k_project(State st, rg_config cfg, Box box, Contacts con, const 
           }
           loc = fmax(loc, fabs(dl));
         }
-        if (k + 1 < K && !grid_sync(gb, nb)) return;
+        if (k + 1 < K && !team_sync_sub(T, na)) return false;
       }
-      double bm = block_max(loc, sm);
+      double bm = block_reduce_max(loc, sm.red_d);
       if (threadIdx.x == 0) atomic_max_nonneg(&slots[it], bm);
-      if (!grid_sync(gb, nb)) return;
+      if (!team_sync_sub(T, na)) return false;
       if (*(volatile double*)&slots[it] < 1e-8) break;
     }
-    // apply corrections: each body once, by the contact owning its first
-    // CSR entry
+    // apply: each body once, by the lowest-index contact touching it
     for (int p = tid; p < C; p += stride) {
-      const int c = order[p];
+      const int c = V.order[p];
       for (int side = 0; side < 2; ++side) {
-        int bd = side ? con.b[c] : con.a[c];
-        if (ent[off[bd]] != 2 * c + side) continue;
-        if (st.inv_mass[bd] <= 0.0) continue;
+        int bd = side ? V.con.b[c] : V.con.a[c];
+        if (st.inv_mass[bd] <= 0.0 || V.owner[bd] != c) continue;
         st.x.st(bd, st.x.ld(bd) + DX.ld(bd));
         d3 th = DT.ld(bd);
         double ang = len(th);
@@ -601,101 +574,598 @@ __global__ void k_project(State st, rg_config cfg, Box box, Contacts con, const 
         }
       }
     }
-    if (!grid_sync(gb, nb)) return;
+    if (!team_sync_sub(T, na)) return false;
   }
+  return true;
+}
+
+__device__ __noinline__ bool project_phase(const Team& T, const NscView& V, int C, SmemNsc& sm) {
+  const int rank = T.rank();
+  const int K = *(volatile int*)&V.ctl->colors;
+  if (C > 0 && V.cfg.nsc_position_stabilization) {
+    const int na = active_blocks(V.color_off, K, blockDim.x, T.nb);
+    if (rank < na && !project_rows(V, C, K, na, rank, T, sm)) return false;
+  }
+  return team_sync(T);
+}
+
+
+// ---------------------------------------------------------------------------
+// Small contact sets (C <= kSmallC): one block solves everything in shared
+// memory.  Contact c is owned by thread c; its bodies get compact local slots
+// (a per-body slot map in global memory, reset afterwards), so colouring
+// scratch, body velocities, manifold rows and impulses all live on chip and
+// phases synchronise with __syncthreads.  Same arithmetic, same order as the
+// team path and the oracle.
+// ---------------------------------------------------------------------------
+constexpr int kSmallC = kTile;       // one contact per thread
+constexpr int kSmallB = 2 * kTile;   // local body slots
+
+struct SmallSmem {
+  double row[kRowComps * kSmallC];   // manifold rows (or projection rows)
+  double lam[3 * kSmallC];
+  double vel[6 * kSmallB];           // v, w (or dx, dθ) per local slot
+  unsigned long long pmax[2 * kSmallB];
+  unsigned long long cmask[kSmallB];
+  int body[kSmallB];                 // body of a slot (-1: unused)
+  int dyn[kSmallB];                  // 1: dynamic body
+  int la[kSmallC], lb[kSmallC];      // local slots of contact c
+  int color[kSmallC], order[kSmallC];
+  int cnt[kMaxColors + 1], coff[kMaxColors + 1], cur[kMaxColors + 1];
+  int nloc, rem, ncol, act;
+  double red[32];
+};
+
+__device__ inline double small_block_max(double v, SmallSmem& S) {
+  v = warp_max(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) S.red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, S.red[w]);
+  return r;  // every thread
+}
+
+// Local slots for the bodies of contacts 0..C-1 (C <= blockDim).
+__device__ __noinline__ void small_map(const NscView& V, int C, SmallSmem& S) {
+  const int t = threadIdx.x;
+  if (t == 0) S.nloc = 0;
+  __syncthreads();
+  if (t < C) {
+    int x[2] = {V.con.a[t], V.con.b[t]};
+    int sl[2];
+    for (int k = 0; k < 2; ++k) {
+      int idx = atomicAdd(&S.nloc, 1);
+      int old = atomicCAS(&V.slot_of[x[k]], -1, idx);
+      S.body[idx] = old == -1 ? x[k] : -1;
+      sl[k] = old == -1 ? idx : old;
+    }
+    S.la[t] = sl[0];
+    S.lb[t] = sl[1];
+  }
+  __syncthreads();
+  for (int s = t; s < S.nloc; s += blockDim.x) {
+    int x = S.body[s];
+    S.dyn[s] = (x >= 0 && V.st.inv_mass[x] > 0.0) ? 1 : 0;
+  }
+  __syncthreads();
+}
+__device__ void small_unmap(const NscView& V, SmallSmem& S) {
+  for (int s = threadIdx.x; s < S.nloc; s += blockDim.x)
+    if (S.body[s] >= 0) V.slot_of[S.body[s]] = -1;
+}
+
+// Jones-Plassmann first fit on local slots; fills S.color / S.order /
+// S.coff and the global colour arrays.  Returns the colour count or -1.
+__device__ __noinline__ int small_color(const NscView& V, int C, SmallSmem& S) {
+  const int t = threadIdx.x;
+  for (int s = t; s < S.nloc; s += blockDim.x) {
+    S.pmax[s] = 0; S.pmax[kSmallB + s] = 0; S.cmask[s] = 0;
+  }
+  for (int k = t; k <= kMaxColors; k += blockDim.x) { S.cnt[k] = 0; S.cur[k] = 0; }
+  if (t < C) S.color[t] = -1;
+  if (t == 0) S.ncol = 0;
+  __syncthreads();
+  int round = 0;
+  for (; round < kMaxRounds; ++round) {
+    unsigned long long* pm = S.pmax + (round & 1) * kSmallB;
+    unsigned long long* pn = S.pmax + ((round + 1) & 1) * kSmallB;
+    if (t == 0) S.rem = 0;
+    if (t < C && S.color[t] < 0) {
+      unsigned long long p = jp_priority((unsigned)t);
+      if (S.dyn[S.la[t]]) atomicMax(&pm[S.la[t]], p);
+      if (S.dyn[S.lb[t]]) atomicMax(&pm[S.lb[t]], p);
+    }
+    __syncthreads();
+    if (t < C && S.color[t] < 0) {
+      unsigned long long p = jp_priority((unsigned)t);
+      int sl[2] = {S.la[t], S.lb[t]};
+      bool win = true;
+      unsigned long long used = 0;
+      for (int k = 0; k < 2; ++k) {
+        if (!S.dyn[sl[k]]) continue;
+        if (pm[sl[k]] != p) win = false;
+        used |= S.cmask[sl[k]];
+        pn[sl[k]] = 0;
+      }
+      if (win) {
+        int col = __ffsll((long long)~used) - 1;
+        if (used == ~0ull) {
+          atomicOr(&V.ctl->err, ERR_COLOR);
+          col = kMaxColors - 1;
+        }
+        S.color[t] = col;
+        for (int k = 0; k < 2; ++k)
+          if (S.dyn[sl[k]]) atomicOr(&S.cmask[sl[k]], 1ull << col);
+        atomicAdd(&S.cnt[col], 1);
+        atomicMax(&S.ncol, col + 1);
+      } else {
+        atomicAdd(&S.rem, 1);
+      }
+    }
+    __syncthreads();
+    int rem = S.rem;
+    __syncthreads();
+    if (rem == 0) break;
+  }
+  if (round >= kMaxRounds) {
+    if (t == 0) atomicOr(&V.ctl->err, ERR_COLOR);
+    return -1;
+  }
+  if (t == 0) {
+    int acc = 0;
+    for (int k = 0; k <= kMaxColors; ++k) {
+      S.coff[k] = acc;
+      if (k < kMaxColors) acc += S.cnt[k];
+    }
+    V.ctl->colors = S.ncol;
+  }
+  __syncthreads();
+  if (t < C) {
+    int k = S.color[t];
+    int p = S.coff[k] + atomicAdd(&S.cur[k], 1);
+    S.order[p] = t;
+    V.order[p] = t;
+    V.color[t] = k;
+  }
+  for (int k = t; k <= kMaxColors; k += blockDim.x) V.color_off[k] = S.coff[k];
+  __syncthreads();
+  return S.ncol;
+}
+
+// Colouring, manifold rows, PSOR and the warm cache for C <= kSmallC.
+__device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, PhaseClock& pc) {
+  Ctl* ctl = V.ctl;
+  const rg_config& cfg = V.cfg;
+  const int t = threadIdx.x;
+  small_map(V, C, S);
+  pc.mark(10);
+  int K = small_color(V, C, S);
+  if (K < 0) return false;
+  pc.mark(2);
+  // body velocities on chip
+  for (int s = t; s < S.nloc; s += blockDim.x) {
+    int x = S.body[s];
+    if (x < 0) continue;
+    d3 v = V.st.v.ld(x), w = V.st.w.ld(x);
+    S.vel[s] = v.x; S.vel[kSmallB + s] = v.y; S.vel[2 * kSmallB + s] = v.z;
+    S.vel[3 * kSmallB + s] = w.x; S.vel[4 * kSmallB + s] = w.y; S.vel[5 * kSmallB + s] = w.z;
+  }
+  RowIO R{S.row, S.lam, kSmallC};
+  const int W = *(volatile int*)V.wn;
+  int coll = 0;
+  if (t < C) coll = build_row(V.st, V.con, cfg, S.order[t], t, R, V.wkey, V.wlam, W, V.wcap);
+  int bcoll = __syncthreads_count(coll);
+  if (t == 0 && bcoll) atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->collisions), (unsigned long long)bcoll);
+  pc.mark(3);
+  Vel Vv{Vec3A{S.vel, S.vel + kSmallB, S.vel + 2 * kSmallB},
+         Vec3A{S.vel + 3 * kSmallB, S.vel + 4 * kSmallB, S.vel + 5 * kSmallB}};
+  const double omega = cfg.nsc_omega, cfm = cfg.nsc_cfm, mu = cfg.nsc_mu;
+  const int p = t;
+  const int c = p < C ? S.order[p] : 0;
+  int my_color = -1;
+  if (p < C)
+    for (int k = 0; k < K; ++k)
+      if (p >= S.coff[k] && p < S.coff[k + 1]) my_color = k;
+  if (cfg.nsc_warm_start != RG_WARM_NONE) {
+    for (int k = 0; k < K; ++k) {
+      if (my_color == k) warm_apply(R, Vv, p, S.la[c], S.lb[c]);
+      __syncthreads();
+    }
+  }
+  double res = 0.0;
+  int sweeps = 0;
+  for (int it = 0; C > 0 && it < cfg.nsc_velocity_iters; ++it) {
+    double loc = 0.0;
+    for (int k = 0; k < K; ++k) {
+      if (my_color == k) loc = psor_row(R, Vv, p, S.la[c], S.lb[c], omega, cfm, mu);
+      __syncthreads();
+    }
+    res = small_block_max(loc, S);
+    sweeps = it + 1;
+    if (res < cfg.nsc_tol) break;
+  }
+  __syncthreads();
+  pc.mark(4);
+  // velocities back; warm cache and impulse sums (contact order)
+  for (int s = t; s < S.nloc; s += blockDim.x) {
+    int x = S.body[s];
+    if (x < 0) continue;
+    V.st.v.st(x, mk3(S.vel[s], S.vel[kSmallB + s], S.vel[2 * kSmallB + s]));
+    V.st.w.st(x, mk3(S.vel[3 * kSmallB + s], S.vel[4 * kSmallB + s], S.vel[5 * kSmallB + s]));
+  }
+  small_unmap(V, S);
+  double jn = 0, jt = 0;
+  if (p < C) {
+    double l0 = S.lam[p], l1 = S.lam[kSmallC + p], l2 = S.lam[2 * kSmallC + p];
+    V.wkey[c] = ((unsigned long long)(unsigned)V.con.a[c] << 32) | (unsigned)V.con.b[c];
+    V.wlam[c] = l0;
+    V.wlam[V.wcap + c] = l1;
+    V.wlam[2 * V.wcap + c] = l2;
+    reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = S.color[c];
+    jn = l0;
+    jt = sqrt(l1 * l1 + l2 * l2);
+  }
+  jn = warp_sum(jn);
+  jt = warp_sum(jt);
+  if ((t & 31) == 0 && (jn != 0.0 || jt != 0.0)) {
+    atomicAdd(&ctl->jn_sum, jn);
+    atomicAdd(&ctl->jt_sum, jt);
+  }
+  if (t == 0) {
+    *V.wn = C;
+    ctl->vel_contacts = C;
+    ctl->residual = res;
+    ctl->sweeps_last = sweeps;
+    if (C > 0) {
+      ctl->sweeps_sum += sweeps;
+      ctl->row_sweeps += (long long)C * sweeps;
+      if (res >= cfg.nsc_tol) ctl->not_conv += 1;
+      if (res > ctl->max_residual) ctl->max_residual = res;
+    }
+  }
+  return true;
+}
+
+// Position projection for C <= kSmallC (nsc_contact.cpp:698-879).
+__device__ __noinline__ bool small_project(const NscView& V, int C, SmallSmem& S) {
+  const rg_config& cfg = V.cfg;
+  const State& st = V.st;
+  const int t = threadIdx.x;
+  small_map(V, C, S);
+  int K = small_color(V, C, S);
+  if (K < 0) return false;
+  const double omega = cfg.nsc_omega, cfm = cfg.nsc_cfm, slop = cfg.nsc_slop;
+  double* PR = S.row;  // kPosComps x kSmallC
+  double* DX = S.vel;  // 6 x kSmallB: dx, dθ per local slot
+  const int p = t;
+  const int c = p < C ? S.order[p] : 0;
+  int my_color = -1;
+  if (p < C)
+    for (int k = 0; k < K; ++k)
+      if (p >= S.coff[k] && p < S.coff[k + 1]) my_color = k;
+  const int sa = p < C ? S.la[c] : 0, sb = p < C ? S.lb[c] : 0;
+  const int a = p < C ? V.con.a[c] : 0, b = p < C ? V.con.b[c] : 0;
+  for (int outer = 0; outer < cfg.nsc_position_iters; ++outer) {
+    int act = 0;
+    if (p < C) {
+      d3 xa = st.x.ld(a), xb = st.x.ld(b);
+      d3 nv, ra, rb;
+      double phi;
+      if (outer == 0) {
+        phi = V.con.comp(12)[c] - V.con.comp(13)[c];
+        nv = mk3(V.con.comp(6)[c], V.con.comp(7)[c], V.con.comp(8)[c]);
+        d3 pa{V.con.comp(0)[c], V.con.comp(1)[c], V.con.comp(2)[c]};
+        d3 pb{V.con.comp(3)[c], V.con.comp(4)[c], V.con.comp(5)[c]};
+        d3 sh{V.con.comp(9)[c], V.con.comp(10)[c], V.con.comp(11)[c]};
+        ra = pa - xa;
+        rb = pb - (xb + sh);
+      } else {
+        Seg A = make_seg(st, a), B = make_seg(st, b);
+        Narrow nr = narrow_pair(A, B, V.box);
+        d3 diff = nr.pb - nr.pa;
+        double dist = len(diff);
+        phi = dist - V.con.comp(13)[c];
+        nv = dist > 1e-10 ? diff / dist : mk3(1, 0, 0);
+        ra = nr.pa - xa;
+        rb = nr.pb - (xb + nr.sh);
+      }
+      act = phi < -slop ? 1 : 0;
+      if (act) {
+        PR[P_N * kSmallC + p] = nv.x; PR[(P_N + 1) * kSmallC + p] = nv.y; PR[(P_N + 2) * kSmallC + p] = nv.z;
+        PR[P_RA * kSmallC + p] = ra.x; PR[(P_RA + 1) * kSmallC + p] = ra.y; PR[(P_RA + 2) * kSmallC + p] = ra.z;
+        PR[P_RB * kSmallC + p] = rb.x; PR[(P_RB + 1) * kSmallC + p] = rb.y; PR[(P_RB + 2) * kSmallC + p] = rb.z;
+        PR[P_PHI * kSmallC + p] = phi + slop;
+        PR[P_G * kSmallC + p] = diag_of(st, a, b, ra, rb, nv, cfm);
+        PR[P_L * kSmallC + p] = 0.0;
+      }
+    }
+    for (int s = t; s < S.nloc; s += blockDim.x)
+      for (int k = 0; k < 6; ++k) DX[k * kSmallB + s] = 0.0;
+    int nact = __syncthreads_count(act);
+    if (nact == 0) break;  // nothing penetrates
+    for (int it = 0; it < cfg.nsc_position_psor_iters; ++it) {
+      double loc = 0.0;
+      for (int k = 0; k < K; ++k) {
+        if (my_color == k && act) {
+          d3 nv{PR[P_N * kSmallC + p], PR[(P_N + 1) * kSmallC + p], PR[(P_N + 2) * kSmallC + p]};
+          d3 ra{PR[P_RA * kSmallC + p], PR[(P_RA + 1) * kSmallC + p], PR[(P_RA + 2) * kSmallC + p]};
+          d3 rb{PR[P_RB * kSmallC + p], PR[(P_RB + 1) * kSmallC + p], PR[(P_RB + 2) * kSmallC + p]};
+          d3 dxa{DX[sa], DX[kSmallB + sa], DX[2 * kSmallB + sa]};
+          d3 dta{DX[3 * kSmallB + sa], DX[4 * kSmallB + sa], DX[5 * kSmallB + sa]};
+          d3 dxb{DX[sb], DX[kSmallB + sb], DX[2 * kSmallB + sb]};
+          d3 dtb{DX[3 * kSmallB + sb], DX[4 * kSmallB + sb], DX[5 * kSmallB + sb]};
+          double l = PR[P_L * kSmallC + p];
+          double corr = dot(nv, ((dxb + cross(dtb, rb)) - dxa) - cross(dta, ra));
+          double r = corr + PR[P_PHI * kSmallC + p] + cfm * l;
+          double d = -(omega / PR[P_G * kSmallC + p]) * r;
+          double nl = smax(0.0, l + d);
+          double dl = nl - l;
+          if (dl != 0.0) {
+            PR[P_L * kSmallC + p] = nl;
+            d3 rAxn = cross(ra, nv);
+            dxa = dxa - nv * (dl * st.inv_mass[a]);
+            dta = dta - iinv_apply(st, a, rAxn) * dl;
+            d3 rBxn = cross(rb, nv);
+            dxb = dxb + nv * (dl * st.inv_mass[b]);
+            dtb = dtb + iinv_apply(st, b, rBxn) * dl;
+            DX[sa] = dxa.x; DX[kSmallB + sa] = dxa.y; DX[2 * kSmallB + sa] = dxa.z;
+            DX[3 * kSmallB + sa] = dta.x; DX[4 * kSmallB + sa] = dta.y; DX[5 * kSmallB + sa] = dta.z;
+            DX[sb] = dxb.x; DX[kSmallB + sb] = dxb.y; DX[2 * kSmallB + sb] = dxb.z;
+            DX[3 * kSmallB + sb] = dtb.x; DX[4 * kSmallB + sb] = dtb.y; DX[5 * kSmallB + sb] = dtb.z;
+          }
+          loc = fabs(dl);
+        }
+        __syncthreads();
+      }
+      double res = small_block_max(loc, S);
+      if (res < 1e-8) break;
+    }
+    __syncthreads();
+    for (int s = t; s < S.nloc; s += blockDim.x) {
+      int x = S.body[s];
+      if (x < 0 || !S.dyn[s]) continue;
+      st.x.st(x, st.x.ld(x) + mk3(DX[s], DX[kSmallB + s], DX[2 * kSmallB + s]));
+      d3 th{DX[3 * kSmallB + s], DX[4 * kSmallB + s], DX[5 * kSmallB + s]};
+      double ang = len(th);
+      if (ang > 1e-8) {
+        d3 ax = th / ang;
+        st.q.st(x, qnormalize(qmul(angle_axis(ang, ax), st.q.ld(x))));
+      }
+    }
+    __syncthreads();
+  }
+  small_unmap(V, S);
+  return true;
 }
 
 // ---------------------------------------------------------------------------
-// Step.
+// One NSC step of one system by one team.
 // ---------------------------------------------------------------------------
-void nsc_step_launch(rg_system* s) {
-  cudaStream_t st = s->stream;
-  const int bs = 256;
-  const int gc = grid_for(s->ccap, bs, s->sm_count * 8);
-  Ctl* ctl = s->d_ctl;
-  GridBar gb = bar_of(s);
-  RowIO R{s->nsc.row, s->nsc.lam, s->ccap};
-  RGL k_nsc_begin<<<1, 1, 0, st>>>(ctl);
-  // 1) free flight
-  {
-    ProfScope p(s, ST_INTEGRATE);
-    nsc_free_flight_launch(s);
+__device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem& S) {
+  Ctl* ctl = V.ctl;
+  const State& st = V.st;
+  const rg_config& cfg = V.cfg;
+  const int n = st.n;
+  const int tid = T.tid(), TS = T.size(), rank = T.rank();
+  if (*(volatile int*)&ctl->err) return false;
+  PhaseClock pc(ctl, rank == 0 && threadIdx.x == 0 && ctl->prof_phases);
+  if (rank == 0 && threadIdx.x == 0) {
+    ctl->collisions = 0;
+    ctl->jn_sum = 0;
+    ctl->jt_sum = 0;
   }
-  // 2) detection, colouring, manifolds
+  // 1) free flight (main.cpp:4397-4408) + segment records + displacement
   {
-    ProfScope p(s, ST_DETECT);
-    detect_launch(s, 0.0, true);
-    csr_launch(s);
+    const d3 g{cfg.gravity[0], cfg.gravity[1], cfg.gravity[2]};
+    double dmax = 0.0;
+    for (int i = tid; i < n; i += TS) {
+      nsc_free_flight_body(st, i, g, cfg.dt);
+      Seg s = make_seg(st, i);
+      V.seg[i] = s;
+      dmax = fmax(dmax, seg_disp(s, V.ref, n, i, V.box));
+    }
+    double bm = block_reduce_max(dmax, sm.red_d);
+    if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
+    if (!team_sync(T)) return false;
   }
-  {
-    ProfScope p(s, ST_COLOR);
-    color_launch(s);
-  }
-  ProfScope pm(s, ST_MANIFOLDS);
-  if (s->cfg.nsc_warm_start == RG_WARM_MLP && s->mlp_ready) {
-    RGL k_manifolds<<<gc, bs, 0, st>>>(s->st, s->con, s->cfg, s->nsc.order, R, s->nsc.wkey, s->nsc.wlam,
-                                   s->nsc.wn, s->nsc.wcap, ctl);
-    mlp_warm_launch(s);
+  pc.mark(0);
+  // 2) detection, colouring, manifold rows
+  int C = detect_phase(T, V, 0.0, sm);
+  if (C < 0) return false;
+  pc.mark(1);
+  const bool small = C <= kSmallC;
+  if (small) {
+    // colouring, rows, PSOR and warm cache in one block, on chip
+    bool ok = true;
+    if (rank == 0) ok = small_solve(V, C, S, pc);
+    if (!ok) atomicOr(&ctl->err, ERR_COLOR);
+    pc.mark(10);
+    if (!team_sync(T)) return false;
+    pc.mark(11);
   } else {
-    RGL k_manifolds<<<gc, bs, 0, st>>>(s->st, s->con, s->cfg, s->nsc.order, R, s->nsc.wkey, s->nsc.wlam,
-                                   s->nsc.wn, s->nsc.wcap, ctl);
+  if (!color_phase(T, V, C, sm)) return false;
+  pc.mark(2);
+  {
+    RowIO R{V.row, V.lam, V.ccap};
+    const int W = *(volatile int*)V.wn;
+    int coll = 0;
+    for (int p = tid; p < C; p += TS)
+      coll += build_row(st, V.con, cfg, V.order[p], p, R, V.wkey, V.wlam, W, V.wcap);
+    int bcoll = block_reduce_sum_i(coll, sm.red_i);
+    if (threadIdx.x == 0 && bcoll)
+      atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->collisions), (unsigned long long)bcoll);
+    if (!team_sync(T)) return false;
   }
-  if (s->recording) mlp_record_launch(s);  // features at the warm-start point
-  pm.end();
+  pc.mark(3);
   // 3) PSOR
+  if (!psor_phase(T, V, C, sm)) return false;
+  pc.mark(4);
+  }
+  // 4) warm cache and impulse sums (large path); position update + segments
   {
-    ProfScope p(s, ST_PSOR);
-    State stt = s->st;
-    rg_config cfg = s->cfg;
-    const int* order = s->nsc.order;
-    const int* ca = s->con.a;
-    const int* cb = s->con.b;
-    const int* coff = s->nsc.color_off;
-    void* args[] = {&stt, &cfg, &order, &ca, &cb, &R, &coff, &ctl, &gb};
-    launch_coop((const void*)k_psor, s->coop_blocks, 256, args, st);
-  }
-  if (s->recording) mlp_record_launch(s);  // targets: converged impulses
-  ProfScope pw(s, ST_MANIFOLDS);
-  RGL k_warm_save<<<gc, bs, 0, st>>>(s->con, s->nsc.order, s->nsc.color, R, s->nsc.wkey, s->nsc.wlam, s->nsc.wn,
-                                 s->nsc.wcap, ctl);
-  pw.end();
-  // 4) position update
-  {
-    ProfScope p(s, ST_INTEGRATE);
-    nsc_position_update_launch(s);
-  }
-  // 5) projection
-  if (s->cfg.nsc_position_stabilization) {
-    {
-      ProfScope p(s, ST_DETECT);
-      detect_launch(s, 0.0, true);
-      csr_launch(s);
+    RowIO R{V.row, V.lam, V.ccap};
+    double jn = 0, jt = 0;
+    for (int p = tid; !small && p < C; p += TS) {
+      int c = V.order[p];
+      double l0 = R.lam[p], l1 = R.lam[R.ccap + p], l2 = R.lam[2 * R.ccap + p];
+      V.wkey[c] = ((unsigned long long)(unsigned)V.con.a[c] << 32) | (unsigned)V.con.b[c];
+      V.wlam[c] = l0;
+      V.wlam[V.wcap + c] = l1;
+      V.wlam[2 * V.wcap + c] = l2;
+      reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = V.color[c];
+      jn += l0;
+      jt += sqrt(l1 * l1 + l2 * l2);
     }
-    {
-      ProfScope p(s, ST_COLOR);
-      color_launch(s);
+    jn = warp_sum(jn);
+    jt = warp_sum(jt);
+    if ((threadIdx.x & 31) == 0 && (jn != 0.0 || jt != 0.0)) {
+      atomicAdd(&ctl->jn_sum, jn);
+      atomicAdd(&ctl->jt_sum, jt);
     }
-    ProfScope p(s, ST_PROJECT);
-    State stt = s->st;
-    rg_config cfg = s->cfg;
-    Box box = s->box;
-    Contacts con = s->con;
-    const int* order = s->nsc.order;
-    const int* coff = s->nsc.color_off;
-    const int* off = s->csr.off;
-    const int* ent = s->csr.ent;
-    double* prow = s->nsc.prow;
-    int* pact = s->nsc.pactive;
-    double* dxb = s->nsc.dx;
-    int ccap = s->ccap;
-    void* args[] = {&stt, &cfg, &box, &con, &order, &coff, &off, &ent, &prow, &pact, &dxb, &ccap,
-                    &ctl, &gb};
-    launch_coop((const void*)k_project, s->coop_blocks, 256, args, st);
+    if (tid == 0 && !small) {
+      *V.wn = C;
+      ctl->vel_contacts = C;
+    }
+    int bad = 0;
+    double dmax = 0.0;
+    for (int i = tid; i < n; i += TS) {
+      bad |= nsc_position_update_body(st, i, cfg);
+      Seg s = make_seg(st, i);
+      V.seg[i] = s;
+      dmax = fmax(dmax, seg_disp(s, V.ref, n, i, V.box));
+    }
+    if (bad) atomicOr(&ctl->err, ERR_NONFINITE);
+    double bm = block_reduce_max(dmax, sm.red_d);
+    if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
+    if (!team_sync(T)) return false;
   }
-  // 6) wrap + clear forces
-  ProfScope p(s, ST_INTEGRATE);
-  wrap_launch(s);
+  pc.mark(5);
+  // 5) position projection (nsc_contact.cpp:659-880)
+  if (cfg.nsc_position_stabilization) {
+    int C2 = detect_phase(T, V, 0.0, sm);
+    if (C2 < 0) return false;
+    pc.mark(6);
+    if (C2 <= kSmallC) {
+      bool ok = true;
+      if (rank == 0) ok = small_project(V, C2, S);
+      if (!ok) atomicOr(&ctl->err, ERR_COLOR);
+      if (!team_sync(T)) return false;
+    } else {
+      if (!color_phase(T, V, C2, sm)) return false;
+      pc.mark(7);
+      if (!project_phase(T, V, C2, sm)) return false;
+    }
+    pc.mark(8);
+  }
+  // 6) PBC wrap + clear forces (main.cpp:4508-4527); the next step touches
+  // rod i from this same thread, so no barrier is needed here.
+  for (int i = tid; i < n; i += TS) wrap_clear_body(st, V.box, i);
+  return true;
+}
+
+#ifndef RG_NSC_BLOCK
+#define RG_NSC_BLOCK (2 * kTile)
+#endif
+constexpr int kBlock = RG_NSC_BLOCK;  // threads per block of the persistent step
+
+__global__ void __launch_bounds__(kBlock, 1) k_nsc_run(const NscView* views, const TeamDesc* teams, int nteams,
+                                                   int nsteps) {
+  __shared__ SmemNsc sm;
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  SmallSmem& S = *reinterpret_cast<SmallSmem*>(dyn_smem);
+  int k = -1;
+  for (int t = 0; t < nteams; ++t)
+    if ((int)blockIdx.x >= teams[t].b0 && (int)blockIdx.x < teams[t].b0 + teams[t].nb) {
+      k = t;
+      break;
+    }
+  if (k < 0) return;
+  const TeamDesc td = teams[k];
+  const NscView& V = views[td.sys];
+  Team T{td.b0, td.nb, td.bar, &V.ctl->err};
+  for (int s = 0; s < nsteps; ++s)
+    if (!nsc_step(T, V, sm, S)) break;
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+NscView make_view(rg_system* s) {
+  NscView V;
+  std::memset(&V, 0, sizeof(V));
+  V.st = s->st;
+  V.box = s->box;
+  V.cfg = s->cfg;
+  V.ctl = s->d_ctl;
+  const Detector& d = s->det;
+  V.seg = d.seg; V.nbr_cnt = d.nbr_cnt; V.nbr = d.nbr; V.maxnb = d.maxnb; V.ref = d.ref;
+  V.words = d.mask_words; V.mask = d.hit_mask; V.hit_cnt = d.hit_cnt;
+  V.cell_of = d.cell_of; V.cell_cnt = d.cell_cnt; V.cell_start = d.cell_start;
+  V.cell_fill = d.cell_fill; V.cell_rods = d.cell_rods;
+  V.grid = detector_grid(s);
+  V.bounds = detector_bounds(s);
+  V.skin = d.skin; V.margin = d.margin; V.cut_center = d.cut_center; V.all_pairs = d.all_pairs ? 1 : 0;
+  V.con = s->con;
+  const Nsc& N = s->nsc;
+  V.row = N.row; V.lam = N.lam; V.color = N.color; V.order = N.order;
+  V.color_cnt = N.color_cnt; V.color_off = N.color_off; V.cursor = N.cursor; V.remaining = N.remaining;
+  V.pmax = N.pmax; V.cmask = N.cmask; V.owner = N.owner;
+  V.wkey = N.wkey; V.wlam = N.wlam; V.wn = N.wn; V.wcap = N.wcap;
+  V.dx = N.dx; V.prow = N.prow; V.pactive = N.pactive;
+  V.ccap = s->ccap;
+  V.blk = N.blk;
+  V.slot_of = N.slot_of;
+  return V;
+}
+
+int nsc_team_blocks(const rg_system* s) {
+  int nb = s->team_blocks;  // explicit team size (autotuner / tests)
+  if (nb <= 0) nb = (s->n + 1023) / 1024;
+  if (nb < 1) nb = 1;
+  if (nb > s->coop_blocks) nb = s->coop_blocks;
+  return nb;
+}
+
+static void launch_coop(const void* fn, int grid, int block, void** args, cudaStream_t st,
+                        size_t smem = 0) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  RGL cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+// nsteps NSC steps of one system as one persistent cooperative launch.
+void nsc_run_launch(rg_system* s, int nsteps) {
+  NscView V = make_view(s);
+  const int nb = nsc_team_blocks(s);
+  TeamDesc td{0, nb, 0, 0, s->nsc.bar};
+  cudaMemcpyAsync(s->nsc.view_dev, &V, sizeof(NscView), cudaMemcpyHostToDevice, s->stream);
+  cudaMemcpyAsync(s->nsc.team_dev, &td, sizeof(TeamDesc), cudaMemcpyHostToDevice, s->stream);
+  cudaMemsetAsync(s->nsc.bar, 0, 4 * sizeof(unsigned int), s->stream);
+  const NscView* views = reinterpret_cast<const NscView*>(s->nsc.view_dev);
+  const TeamDesc* teams = reinterpret_cast<const TeamDesc*>(s->nsc.team_dev);
+  int nteams = 1;
+  void* args[] = {&views, &teams, &nteams, &nsteps};
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute((const void*)k_nsc_run, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(SmallSmem));
+    attr_set = true;
+  }
+  ProfScope p(s, ST_OTHER);
+  launch_coop((const void*)k_nsc_run, nb, kBlock, args, s->stream, sizeof(SmallSmem));
   s->contacts_fresh = false;
 }
+
+size_t nsc_view_bytes() { return sizeof(NscView); }
+size_t nsc_team_bytes() { return sizeof(TeamDesc); }
 
 }  // namespace rg

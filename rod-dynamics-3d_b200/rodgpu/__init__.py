@@ -43,7 +43,8 @@ class RgConfig(ctypes.Structure):
         ("nsc_mu", _d), ("nsc_beta", _d), ("nsc_cfm", _d), ("nsc_omega", _d), ("nsc_slop", _d),
         ("nsc_tol", _d), ("nsc_velocity_iters", _i), ("nsc_position_stabilization", _i),
         ("nsc_position_iters", _i), ("nsc_position_psor_iters", _i), ("nsc_warm_start", _i),
-        ("psor_order", _i), ("skin", _d), ("max_neighbors", _i), ("reserved", _i * 7),
+        ("psor_order", _i), ("skin", _d), ("max_neighbors", _i), ("team_blocks", _i),
+        ("reserved", _i * 6),
     ]
 
 
@@ -70,7 +71,7 @@ ABI_SYMBOLS = [
     "rg_abi_version", "rg_config_default", "rg_status_string", "rg_last_error", "rg_create",
     "rg_destroy", "rg_get_config", "rg_set_bodies", "rg_set_state", "rg_get_state", "rg_step",
     "rg_detect", "rg_get_impulses", "rg_compute_forces", "rg_get_history", "rg_set_profiling",
-    "rg_get_profile",
+    "rg_get_profile", "rg_get_phase_times",
     "rg_mlp_param_count", "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_record",
     "rg_mlp_records", "rg_mlp_train", "rg_mlp_infer", "rg_batch_create", "rg_batch_destroy",
     "rg_batch_set_bodies", "rg_batch_set_state", "rg_batch_get_state", "rg_batch_step",
@@ -107,6 +108,7 @@ def lib():
                                      ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L.rg_set_profiling.argtypes = [P, ctypes.c_int]
         L.rg_get_profile.argtypes = [P, dp, ctypes.POINTER(ctypes.c_int64)]
+        L.rg_get_phase_times.argtypes = [P, dp, ctypes.c_int]
         L.rg_mlp_param_count.restype = ctypes.c_size_t
         fp = ctypes.POINTER(ctypes.c_float)
         L.rg_mlp_set_params.argtypes = [P, fp, ctypes.c_size_t]
@@ -254,7 +256,7 @@ class System:
         self._check(self._lib.rg_compute_forces(self._h, ptr(f), ptr(t), ctypes.byref(pe)), "compute_forces")
         return f, t, pe.value
 
-    STAGES = ["integrate", "detect", "color", "manifolds", "psor", "project", "forces", "other"]
+    STAGES = ["integrate", "detect", "color", "manifolds", "psor", "project", "forces", "nsc_step"]
 
     def set_profiling(self, on=True):
         self._check(self._lib.rg_set_profiling(self._h, int(on)), "set_profiling")
@@ -264,6 +266,15 @@ class System:
         cnt = np.zeros(8, np.int64)
         self._check(self._lib.rg_get_profile(self._h, ptr(ms), ptr(cnt, ctypes.c_int64)), "profile")
         return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.STAGES)}
+
+    PHASES = ["free_flight", "detect", "color", "manifolds", "psor", "position_update",
+              "proj_detect", "proj_color", "proj_sweeps", "list_rebuild", "small_map_writeback",
+              "small_sync"]
+
+    def phase_times(self):
+        ms = np.zeros(12)
+        self._check(self._lib.rg_get_phase_times(self._h, ptr(ms), 12), "phase_times")
+        return {k: float(ms[i]) for i, k in enumerate(self.PHASES)}
 
     def history(self):
         n = ctypes.c_size_t()

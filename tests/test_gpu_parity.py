@@ -155,6 +155,30 @@ def test_nsc_multi_step_with_warm_start():
     assert rel_err(lg, lo) < TOL
 
 
+@pytest.mark.parametrize("team", [1, 3, 16])
+def test_nsc_team_sizes_agree(team):
+    # the persistent step gives the oracle's result for any team size
+    sc = packed_scene(3000, d=0.05, phi=0.2, seed=14, squeeze=0.97)
+    g, o = make_pair(sc, model="nsc", dt=5e-4, nsc_velocity_iters=500, team_blocks=team)
+    sg = g.step(3)
+    so = o.step(3)
+    a, b = g.get_state(), o.get_state()
+    for k in ("x", "q", "v", "w"):
+        assert rel_err(a[k], b[k]) < TOL, k
+    assert sg["psor_sweeps"] == so["psor_sweeps"]
+    assert sg["contacts"] == so["contacts"]
+
+
+def test_nsc_open_box_steps():
+    sc = packed_scene(1500, d=0.1, phi=0.1, seed=15, squeeze=0.97)
+    g, o = make_pair(sc, model="nsc", dt=5e-4, nsc_velocity_iters=200, pbc_enabled=0, team_blocks=4)
+    g.step(2)
+    o.step(2)
+    a, b = g.get_state(), o.get_state()
+    for k in ("x", "q", "v", "w"):
+        assert rel_err(a[k], b[k]) < TOL, k
+
+
 def test_list_rebuild_keeps_exact_contacts():
     # large velocities force neighbour-list rebuilds within a few steps
     sc = packed_scene(800, d=0.1, phi=0.1, seed=13, squeeze=0.97, sigma_v=20.0, sigma_w=5.0)
