@@ -215,6 +215,40 @@ int rg_get_profile(const rg_system* sys, double* ms, int64_t* launches);
  * 8 projection sweeps. */
 int rg_get_phase_times(const rg_system* sys, double* ms, int n);
 
+/* ---- detection without device allocation --------------------------------- */
+/* No counterpart in the reference: this entry point exists for callers that
+ * cannot call cudaMalloc themselves or let a library do it (code running
+ * under another framework's device allocator or inside a fixed memory
+ * budget).  It finds the contacts rg_detect finds - same pairs (a < b,
+ * sorted), same geometry, bit for bit - from DEVICE buffers the caller
+ * owns, and allocates nothing: all intermediate data lives in one fixed
+ * file-scope __device__ array sized for RG_NOALLOC_MAX_BODIES bodies
+ * (about 0.6 MB), which every GPU that loads the library keeps until the
+ * process exits.
+ *
+ *   x[3n], q[4n] (w,x,y,z), radius[n], half_height[n]: device, AoS.
+ *   inv_mass[n]: device or NULL (NULL: every body dynamic); pairs of two
+ *     static bodies are skipped as in rg_detect.
+ *   pbc_min / pbc_max: HOST arrays of 3 (ignored when pbc_enabled == 0).
+ *   pairs[2*cap], geom[12*cap] (may be NULL): device outputs, layout of
+ *     rg_detect; count[1]: device, receives the contact count even when it
+ *     exceeds cap (then only cap contacts are written).
+ *   stream: a cudaStream_t (NULL: the default stream).  The call only
+ *     enqueues work; synchronise the stream before reading the outputs.
+ * Returns RG_ERR_CAPACITY when n > RG_NOALLOC_MAX_BODIES and RG_ERR_ARG for
+ * bad arguments, before any device work.  The first call on a device looks
+ * the scratch address up with cudaGetSymbolAddress (once per device, with
+ * that device current); make that first call before any stream capture.
+ * Every call on a device shares the one scratch array: calls that overlap
+ * on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller. */
+#define RG_NOALLOC_MAX_BODIES 8192
+int rg_detect_noalloc(const double* x, const double* q, const double* radius,
+                      const double* half_height, const double* inv_mass, int n,
+                      int pbc_enabled, const double* pbc_min, const double* pbc_max,
+                      double delta, int32_t* pairs, double* geom, int cap,
+                      int32_t* count, void* stream);
+
 /* ---- learned PSOR warm start ------------------------------------------- */
 /* MLP 8 -> 128 -> 128 -> 128 -> 3 (SiLU), BF16 weights and activations,
  * FP32 accumulation.  Features per contact (in this order): gap φ, v_n,

@@ -71,7 +71,7 @@ ABI_SYMBOLS = [
     "rg_abi_version", "rg_config_default", "rg_status_string", "rg_last_error", "rg_create",
     "rg_destroy", "rg_get_config", "rg_set_bodies", "rg_set_state", "rg_get_state", "rg_step",
     "rg_detect", "rg_get_impulses", "rg_compute_forces", "rg_get_history", "rg_set_profiling",
-    "rg_get_profile", "rg_get_phase_times",
+    "rg_get_profile", "rg_get_phase_times", "rg_detect_noalloc",
     "rg_mlp_param_count", "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_record",
     "rg_mlp_records", "rg_mlp_train", "rg_mlp_infer", "rg_batch_create", "rg_batch_destroy",
     "rg_batch_set_bodies", "rg_batch_set_state", "rg_batch_get_state", "rg_batch_step",
@@ -109,6 +109,8 @@ def lib():
         L.rg_set_profiling.argtypes = [P, ctypes.c_int]
         L.rg_get_profile.argtypes = [P, dp, ctypes.POINTER(ctypes.c_int64)]
         L.rg_get_phase_times.argtypes = [P, dp, ctypes.c_int]
+        L.rg_detect_noalloc.argtypes = [P, P, P, P, P, ctypes.c_int, ctypes.c_int, dp, dp, _d, P, P,
+                                        ctypes.c_int, P, P]
         L.rg_mlp_param_count.restype = ctypes.c_size_t
         fp = ctypes.POINTER(ctypes.c_float)
         L.rg_mlp_set_params.argtypes = [P, fp, ctypes.c_size_t]
