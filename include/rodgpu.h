@@ -134,7 +134,8 @@ typedef struct rg_step_stats {
   double device_ms;         /* device time of the call (CUDA events, stream)  */
   int64_t psor_row_sweeps;  /* NSC: Σ over steps of contacts x sweeps         */
   int64_t kernel_launches;  /* kernels this library launched during the call  */
-  int64_t reserved[3];
+  int64_t contact_steps;    /* NSC: Σ over steps of velocity-solve contacts   */
+  int64_t reserved[2];
 } rg_step_stats;
 
 /* Stage timers (CUDA events on the system's stream), enabled per system.
@@ -267,11 +268,21 @@ int rg_mlp_get_params(const rg_system* sys, float* params, size_t n);
 int rg_mlp_record(rg_system* sys, int enable, size_t cap);
 int rg_mlp_records(const rg_system* sys, float* features, float* targets,
                    size_t cap, size_t* n);
-/* Trains on host records with the device forward/backward kernels (Adam). */
+/* Trains on host records with the device forward/backward kernels (Adam,
+ * FP32 master weights, BF16 copies for the GEMMs): initialises the
+ * normalisation from the records and the weights from seed, then runs
+ * `epochs` passes of shuffled minibatches of `batch` records.  final_loss is
+ * the mean squared error of the last epoch in normalised units. */
 int rg_mlp_train(rg_system* sys, const float* features, const float* targets,
                  size_t n, int epochs, int batch, float lr, uint64_t seed,
                  float* final_loss);
-/* Inference: out[3*n] = MLP(features[8*n]). */
+/* Loss and gradient (rg_mlp_param_count floats, parameter layout; the
+ * normalisation entries get 0) of the current weights on n records, by the
+ * same device kernels as one training step.  For gradient checks. */
+int rg_mlp_grad(rg_system* sys, const float* features, const float* targets,
+                size_t n, float* grad, float* loss);
+/* Inference with the in-step tensor-core routine: out[3*n] = predicted
+ * impulses (previous impulse + predicted change) for features[8*n]. */
 int rg_mlp_infer(rg_system* sys, const float* features, float* out, size_t n);
 
 /* ---- batched independent systems ---------------------------------------- */
@@ -289,8 +300,28 @@ int rg_batch_set_state(rg_batch* b, int k, const double* x, const double* q,
                        const double* v, const double* w);
 int rg_batch_get_state(const rg_batch* b, int k, double* x, double* q,
                        double* v, double* w);
+/* nsteps steps of every member; per_system (optional) gets n_systems stats,
+ * each with device_ms = the whole batch call. */
 int rg_batch_step(rg_batch* b, int nsteps, rg_step_stats* per_system);
+/* Loads the same network into every NSC member. */
 int rg_batch_set_mlp(rg_batch* b, const float* params, size_t n);
+int rg_batch_size(const rg_batch* b);
+/* Member k as a system handle (all single-system calls apply; it shares
+ * the batch's stream and is destroyed with the batch). */
+rg_system* rg_batch_member(rg_batch* b, int k);
+const char* rg_batch_last_error(const rg_batch* b);
+/* Schedule of the persistent launch: NSC members of at least 1.5 R bodies
+ * get a team of round(n/R) blocks, the rest share single-block teams
+ * (R = rods_per_block; 0 = all single-block).  use_graph: replay the launch
+ * from a CUDA graph. */
+int rg_batch_set_schedule(rg_batch* b, int rods_per_block, int use_graph);
+int rg_batch_get_schedule(const rg_batch* b, int* rods_per_block, int* grid,
+                          int* nteams);
+/* Autotuner: times trial_steps steps per candidate R from the current state
+ * (state put back after each trial), selects the fastest; ms_out
+ * (optional) gets n_cand times. */
+int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand,
+                      int trial_steps, int* best, double* ms_out);
 
 #ifdef __cplusplus
 }

@@ -16,7 +16,7 @@
 
 using namespace rg;
 
-namespace {
+namespace rg {
 
 const char* kStatus[] = {"ok", "bad argument", "CUDA error", "capacity exceeded",
                          "non-finite state", "PSOR not converged", "no CUDA device",
@@ -166,11 +166,17 @@ __global__ void k_ke(State st, Ctl* ctl, double* out) {
   (void)ctl;
 }
 
-struct Snapshot {
-  std::vector<char> ctl;
-  int hist_cur = 0;
-  int wn = 0;
-};
+double kinetic_energy(rg_system* s) {
+  const int g = 64;
+  if (!s->d_ke && cudaMalloc(&s->d_ke, sizeof(double) * g) != cudaSuccess) return NAN;
+  RGL k_ke<<<g, 256, 0, s->stream>>>(s->st, s->d_ctl, s->d_ke);
+  double hp[g];
+  cudaMemcpyAsync(hp, s->d_ke, sizeof(double) * g, cudaMemcpyDeviceToHost, s->stream);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return NAN;
+  double ke = 0;
+  for (int i = 0; i < g; ++i) ke += hp[i];
+  return ke;
+}
 
 // Device snapshot of everything a step mutates: state, control words,
 // current history table and the NSC warm cache.
@@ -226,7 +232,7 @@ cudaError_t restore_snapshot(rg_system* s, const Snapshot& sn) {
   return cudaMemcpy(s->d_ctl, sn.ctl.data(), s->ctl_bytes, cudaMemcpyHostToDevice);
 }
 
-}  // namespace
+}  // namespace rg
 
 extern "C" {
 
@@ -326,7 +332,8 @@ int rg_destroy(rg_system* s) {
   cudaFree(s->d_state); cudaFree(s->d_props); cudaFree(s->d_ctl); cudaFree(s->d_snap);
   cudaFree(s->snap_hkey); cudaFree(s->snap_hval); cudaFree(s->snap_hframe);
   cudaFree(s->snap_wkey); cudaFree(s->snap_wlam);
-  cudaFree(s->d_mlp); cudaFree(s->d_rec_x); cudaFree(s->d_rec_y);
+  mlp_free(s);
+  cudaFree(s->d_rec_x); cudaFree(s->d_rec_y); cudaFree(s->d_ke);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
   if (s->h_stage) cudaFreeHost(s->h_stage);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
@@ -426,7 +433,7 @@ int rg_get_state(const rg_system* s, double* x, double* q, double* v, double* w,
 
 }  // extern "C"
 
-namespace {
+namespace rg {
 
 void launch_steps(rg_system* s, int nsteps) {
   const int model = s->cfg.model;
@@ -508,28 +515,78 @@ bool grow(rg_system* s, int err) {
   return grew;
 }
 
-}  // namespace
+// Per-call counters start from the snapshot's control words.
+cudaError_t reset_call_ctl(rg_system* s, const Snapshot& sn) {
+  Ctl* h = s->h_ctl;
+  std::memcpy(h, sn.ctl.data(), s->ctl_bytes);
+  h->err = 0;
+  h->rebuilds = 0;
+  h->sweeps_sum = 0;
+  h->not_conv = 0;
+  h->max_residual = 0;
+  h->row_sweeps = 0;
+  h->contact_steps = 0;
+  h->bar_count = 0;
+  return cudaMemcpyAsync(s->d_ctl, h, s->ctl_bytes, cudaMemcpyHostToDevice, s->stream);
+}
+
+// Turns the error bits of a finished call into a status.  Capacity errors
+// restore the snapshot, grow the buffers and ask for a retry (RG_OK with
+// *retry set).
+int resolve_call(rg_system* s, Snapshot& sn, int err, bool* retry) {
+  *retry = false;
+  if (!err) return RG_OK;
+  if (err & ERR_TIMEOUT) return fail(s, RG_ERR_TIMEOUT, "a device-side barrier timed out");
+  if (err & ERR_NONFINITE) return fail(s, RG_ERR_NONFINITE, "non-finite body state");
+  if (err & ERR_COLOR) return fail(s, RG_ERR_CAPACITY, "contact graph needs more than 64 colours");
+  cudaError_t e = restore_snapshot(s, sn);
+  if (e) return cuda_fail(s, e, "restore");
+  if (!grow(s, err)) return fail(s, RG_ERR_CAPACITY, "could not grow device buffers");
+  e = take_snapshot(s, sn);
+  if (e) return cuda_fail(s, e, "snapshot");
+  reinterpret_cast<Ctl*>(sn.ctl.data())->rebuild = 1;
+  s->contacts_fresh = false;
+  *retry = true;
+  return RG_OK;
+}
+
+void fill_stats(rg_system* s, int nsteps, rg_step_stats* stats) {
+  Ctl* h = s->h_ctl;
+  std::memset(stats, 0, sizeof(*stats));
+  stats->steps = nsteps;
+  stats->contacts = s->cfg.model == RG_MODEL_NSC ? h->vel_contacts : h->contacts;
+  stats->collisions = h->collisions;
+  stats->psor_sweeps = h->sweeps_sum;
+  stats->psor_sweeps_last = h->sweeps_last;
+  stats->list_rebuilds = h->rebuilds;
+  stats->colors = h->colors;
+  stats->history_size = h->hist_n;
+  stats->residual = h->residual;
+  stats->jn_sum = h->jn_sum;
+  stats->jt_sum = h->jt_sum;
+  stats->potential_energy = h->pe;
+  stats->max_residual = h->max_residual;
+  stats->not_converged = h->not_conv;
+  stats->device_ms = s->last_call_ms;
+  stats->psor_row_sweeps = h->row_sweeps;
+  stats->kernel_launches = s->last_call_launches;
+  stats->contact_steps = h->contact_steps;
+  stats->kinetic_energy = kinetic_energy(s);
+}
+
+}  // namespace rg
 
 extern "C" {
 
 int rg_step(rg_system* s, int nsteps, rg_step_stats* stats) {
   if (!s || nsteps < 0) return RG_ERR_ARG;
   if (!s->bodies_set || !s->state_set) return fail(s, RG_ERR_STATE, "set bodies and state before stepping");
+  if (s->cfg.model == RG_MODEL_NSC && s->cfg.nsc_warm_start == RG_WARM_MLP && !s->mlp_ready)
+    return fail(s, RG_ERR_STATE, "learned warm start selected but no network is loaded (rg_mlp_train or rg_mlp_set_params)");
   Snapshot sn;
   RG_TRY(take_snapshot(s, sn), "snapshot");
-  const bool fresh0 = s->contacts_fresh;
   for (int attempt = 0; attempt < 8; ++attempt) {
-    // reset per-call counters
-    Ctl* h = s->h_ctl;
-    std::memcpy(h, sn.ctl.data(), s->ctl_bytes);
-    h->err = 0;
-    h->rebuilds = 0;
-    h->sweeps_sum = 0;
-    h->not_conv = 0;
-    h->max_residual = 0;
-    h->row_sweeps = 0;
-    h->bar_count = 0;
-    RG_TRY(cudaMemcpyAsync(s->d_ctl, h, s->ctl_bytes, cudaMemcpyHostToDevice, s->stream), "ctl upload");
+    RG_TRY(reset_call_ctl(s, sn), "ctl upload");
     s->rec_stage.clear(); s->rec_a.clear(); s->rec_b.clear(); s->ev_used = 0;
     int ev0 = prof_event(s), ev1 = prof_event(s);
     const long long l0 = g_launches;
@@ -538,64 +595,24 @@ int rg_step(rg_system* s, int nsteps, rg_step_stats* stats) {
     cudaEventRecord(s->ev_pool[ev1], s->stream);
     cudaError_t e = cudaGetLastError();
     if (e) return cuda_fail(s, e, "kernel launch");
+    Ctl* h = s->h_ctl;
     RG_TRY(cudaMemcpyAsync(h, s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost, s->stream), "ctl download");
     RG_TRY(cudaStreamSynchronize(s->stream), "step");
-    int err = h->err;
     float call_ms = 0;
     cudaEventElapsedTime(&call_ms, s->ev_pool[ev0], s->ev_pool[ev1]);
     s->last_call_ms = call_ms;
     s->last_call_launches = g_launches - l0;
-    if (!err) {
+    if (!h->err) {
       prof_resolve(s);
       break;
     }
     s->rec_stage.clear(); s->rec_a.clear(); s->rec_b.clear(); s->ev_used = 0;
-    if (err & ERR_TIMEOUT) return fail(s, RG_ERR_TIMEOUT, "a device-side barrier timed out");
-    if (err & ERR_NONFINITE) return fail(s, RG_ERR_NONFINITE, "non-finite body state");
-    if (err & ERR_COLOR) return fail(s, RG_ERR_CAPACITY, "contact graph needs more than 64 colours");
-    // capacity: restore the snapshot, grow, retry
-    RG_TRY(restore_snapshot(s, sn), "restore");
-    if (!grow(s, err)) return fail(s, RG_ERR_CAPACITY, "could not grow device buffers");
-    RG_TRY(take_snapshot(s, sn), "snapshot");
-    reinterpret_cast<Ctl*>(sn.ctl.data())->rebuild = 1;
-    s->contacts_fresh = false;
-    (void)fresh0;
+    bool retry = false;
+    int rc = resolve_call(s, sn, h->err, &retry);
+    if (rc != RG_OK) return rc;
     if (attempt == 7) return fail(s, RG_ERR_CAPACITY, "capacity retries exhausted");
   }
-  if (stats) {
-    Ctl* h = s->h_ctl;
-    std::memset(stats, 0, sizeof(*stats));
-    stats->steps = nsteps;
-    stats->contacts = s->cfg.model == RG_MODEL_NSC ? h->vel_contacts : h->contacts;
-    stats->collisions = h->collisions;
-    stats->psor_sweeps = h->sweeps_sum;
-    stats->psor_sweeps_last = h->sweeps_last;
-    stats->list_rebuilds = h->rebuilds;
-    stats->colors = h->colors;
-    stats->history_size = h->hist_n;
-    stats->residual = h->residual;
-    stats->jn_sum = h->jn_sum;
-    stats->jt_sum = h->jt_sum;
-    stats->potential_energy = h->pe;
-    stats->max_residual = h->max_residual;
-    stats->not_converged = h->not_conv;
-    stats->device_ms = s->last_call_ms;
-    stats->psor_row_sweeps = h->row_sweeps;
-    stats->kernel_launches = s->last_call_launches;
-    // kinetic energy (deterministic two-level sum)
-    double* part = nullptr;
-    const int g = 64;
-    if (cudaMalloc(&part, sizeof(double) * g) == cudaSuccess) {
-      RGL k_ke<<<g, 256, 0, s->stream>>>(s->st, s->d_ctl, part);
-      std::vector<double> hp(g);
-      cudaMemcpyAsync(hp.data(), part, sizeof(double) * g, cudaMemcpyDeviceToHost, s->stream);
-      cudaStreamSynchronize(s->stream);
-      double ke = 0;
-      for (int i = 0; i < g; ++i) ke += hp[i];
-      stats->kinetic_energy = ke;
-      cudaFree(part);
-    }
-  }
+  if (stats) fill_stats(s, nsteps, stats);
   return RG_OK;
 }
 

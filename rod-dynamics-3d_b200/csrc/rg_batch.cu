@@ -1,0 +1,410 @@
+// rg_batch.cu - many independent systems of uneven size in one persistent
+// launch.
+//
+// No reference counterpart: the reference steps one system per process
+// (App::physicsStep, src/app/main.cpp:4333-4858; its CUDA state is a
+// file-static singleton, src/physics/cuda_broadphase.cu:658).  A batch owns
+// one rg_system per member (its own box, model, dt, friction, buffers and
+// error words) on one shared stream.  NSC members run as teams of the
+// persistent step kernel in ONE cooperative launch for all requested
+// steps; that launch (with the reset of the team barriers) is captured in a
+// CUDA graph and replayed.  Members with the Verlet models run their
+// multi-kernel step on the same stream after it.
+//
+// Schedule: members of at least 1.5 R bodies (R = bodies per block) get a
+// team of round(n/R) blocks to themselves; the rest share single-block teams,
+// assigned longest-first to the least-loaded block.  rg_batch_autotune times
+// a few R on the live systems (from a snapshot, restored afterwards) and
+// keeps the fastest.  The schedule changes time only: every member's
+// results are the same for any schedule.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "rg_internal.cuh"
+#include "rg_nsc_dev.cuh"
+
+using namespace rg;
+
+struct rg_batch {
+  int n = 0;
+  std::vector<rg_system*> sys;
+  cudaStream_t stream = nullptr;
+  int coop_blocks = 0;
+  // schedule
+  int rods_per_block = 0;  // 0: every NSC member in single-block teams
+  bool use_graph = true;
+  bool plan_dirty = true;
+  std::vector<TeamDesc> teams;
+  std::vector<int> members;
+  int grid = 0;
+  NscView* d_views = nullptr;
+  TeamDesc* d_teams = nullptr;
+  int* d_members = nullptr;
+  unsigned int* d_bars = nullptr;
+  int cap_members = 0, cap_teams = 0;
+  // graph of (barrier reset + persistent launch) for graph_steps steps
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = -1;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
+  std::string err;
+};
+
+namespace {
+
+int bfail(rg_batch* b, int code, const std::string& msg) {
+  b->err = msg;
+  return code;
+}
+
+// Team plan for the NSC members in `which` with R bodies per block.
+void plan(rg_batch* b, const std::vector<int>& which, int R, std::vector<TeamDesc>& teams,
+          std::vector<int>& members, int& grid) {
+  teams.clear();
+  members.clear();
+  const int budget = b->coop_blocks;
+  std::vector<int> big, small;
+  for (int k : which) {
+    if (R > 0 && b->sys[k]->n >= (3 * R) / 2) big.push_back(k);
+    else small.push_back(k);
+  }
+  if ((int)big.size() > budget / 2) {  // too many large members: pack everything
+    small.insert(small.end(), big.begin(), big.end());
+    big.clear();
+  }
+  std::sort(big.begin(), big.end(), [&](int x, int y) { return b->sys[x]->n > b->sys[y]->n; });
+  std::sort(small.begin(), small.end(), [&](int x, int y) {
+    return b->sys[x]->n != b->sys[y]->n ? b->sys[x]->n > b->sys[y]->n : x < y;
+  });
+  std::vector<int> nb(big.size());
+  long long want = 0;
+  for (size_t i = 0; i < big.size(); ++i) {
+    nb[i] = std::max(1, (int)((b->sys[big[i]]->n + R / 2) / R));
+    want += nb[i];
+  }
+  const int reserve = small.empty() ? 0 : std::min<int>((int)small.size(), std::max(1, budget / 8));
+  const int avail = std::max<int>((int)big.size(), budget - reserve);
+  if (want > avail) {  // scale the large teams down to fit
+    for (size_t i = 0; i < big.size(); ++i) nb[i] = std::max(1, (int)((long long)nb[i] * avail / want));
+    want = std::accumulate(nb.begin(), nb.end(), 0LL);
+    for (size_t i = 0; want > avail && i < big.size(); ++i)
+      while (nb[i] > 1 && want > avail) { --nb[i]; --want; }
+  }
+  int b0 = 0;
+  for (size_t i = 0; i < big.size(); ++i) {
+    teams.push_back(TeamDesc{b0, nb[i], (int)members.size(), 1, nullptr});
+    members.push_back(big[i]);
+    b0 += nb[i];
+  }
+  const int nsb = std::min<int>((int)small.size(), std::max(1, budget - b0));
+  if (!small.empty()) {
+    std::vector<std::vector<int>> bins(nsb);
+    std::vector<long long> load(nsb, 0);
+    for (int k : small) {
+      int m = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      bins[m].push_back(k);
+      load[m] += b->sys[k]->n;
+    }
+    for (int i = 0; i < nsb; ++i) {
+      teams.push_back(TeamDesc{b0, 1, (int)members.size(), (int)bins[i].size(), nullptr});
+      for (int k : bins[i]) members.push_back(k);
+      ++b0;
+    }
+  }
+  grid = b0;
+}
+
+cudaError_t ensure_dev(rg_batch* b, size_t nteams, size_t nmembers) {
+  cudaError_t e = cudaSuccess;
+  if ((int)nmembers > b->cap_members) {
+    cudaFree(b->d_views);
+    cudaFree(b->d_members);
+    b->cap_members = (int)std::max<size_t>(nmembers, (size_t)b->n);
+    if ((e = cudaMalloc(&b->d_views, sizeof(NscView) * b->cap_members))) return e;
+    if ((e = cudaMalloc(&b->d_members, sizeof(int) * b->cap_members))) return e;
+  }
+  if ((int)nteams > b->cap_teams) {
+    cudaFree(b->d_teams);
+    cudaFree(b->d_bars);
+    b->cap_teams = (int)std::max<size_t>(nteams, (size_t)b->coop_blocks);
+    if ((e = cudaMalloc(&b->d_teams, sizeof(TeamDesc) * b->cap_teams))) return e;
+    if ((e = cudaMalloc(&b->d_bars, sizeof(unsigned int) * 4 * b->cap_teams))) return e;
+  }
+  return e;
+}
+
+// Uploads the views of all members (buffer addresses change when buffers
+// grow) and the team plan.  The views array is indexed by member number.
+cudaError_t upload(rg_batch* b, std::vector<TeamDesc>& teams, const std::vector<int>& members) {
+  cudaError_t e = ensure_dev(b, teams.size(), members.size());
+  if (e) return e;
+  std::vector<NscView> views(b->n);
+  for (int k = 0; k < b->n; ++k)
+    if (b->sys[k]->cfg.model == RG_MODEL_NSC) views[k] = make_view(b->sys[k]);
+  for (size_t t = 0; t < teams.size(); ++t) teams[t].bar = b->d_bars + 4 * t;
+  cudaMemcpyAsync(b->d_views, views.data(), sizeof(NscView) * b->n, cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync(b->d_teams, teams.data(), sizeof(TeamDesc) * teams.size(), cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync(b->d_members, members.data(), sizeof(int) * members.size(), cudaMemcpyHostToDevice, b->stream);
+  return cudaStreamSynchronize(b->stream);
+}
+
+void drop_graph(rg_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->graph_steps = -1;
+}
+
+// Barrier reset + persistent launch, through the graph when enabled.
+cudaError_t launch_nsc(rg_batch* b, int nteams, int grid, int nsteps, bool graph_ok) {
+  if (grid <= 0 || nsteps <= 0) return cudaSuccess;
+  if (!(graph_ok && b->use_graph)) {
+    cudaMemsetAsync(b->d_bars, 0, sizeof(unsigned int) * 4 * nteams, b->stream);
+    nsc_batch_launch(b->d_views, b->d_teams, nteams, b->d_members, grid, nsteps, b->stream);
+    return cudaGetLastError();
+  }
+  if (!b->graph || b->graph_steps != nsteps) {
+    drop_graph(b);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e) return e;
+    cudaMemsetAsync(b->d_bars, 0, sizeof(unsigned int) * 4 * nteams, b->stream);
+    nsc_batch_launch(b->d_views, b->d_teams, nteams, b->d_members, grid, nsteps, b->stream);
+    e = cudaStreamEndCapture(b->stream, &g);
+    if (e) return e;
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e) { b->graph = nullptr; return e; }
+    b->graph_steps = nsteps;
+  }
+  RGL cudaGraphLaunch(b->graph, b->stream);
+  return cudaGetLastError();
+}
+
+// One batch call: snapshot, launch, error resolution with replay of the
+// members that need larger buffers.  With restore_after (autotuner trials)
+// every member is put back to its state at the start of the call and its
+// neighbour lists are rebuilt at the next step.
+int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after = false) {
+  for (int k = 0; k < b->n; ++k) {
+    rg_system* s = b->sys[k];
+    if (!s->bodies_set || !s->state_set) return bfail(b, RG_ERR_STATE, "member " + std::to_string(k) + ": set bodies and state before stepping");
+    if (s->cfg.model == RG_MODEL_NSC && s->cfg.nsc_warm_start == RG_WARM_MLP && !s->mlp_ready)
+      return bfail(b, RG_ERR_STATE, "member " + std::to_string(k) + ": learned warm start without a network");
+  }
+  std::vector<Snapshot> sn(b->n);
+  for (int k = 0; k < b->n; ++k)
+    if (take_snapshot(b->sys[k], sn[k])) return bfail(b, RG_ERR_CUDA, "snapshot");
+  std::vector<int> todo(b->n);
+  std::iota(todo.begin(), todo.end(), 0);
+  double total_ms = 0;
+  for (int attempt = 0; attempt < 8 && !todo.empty(); ++attempt) {
+    for (int k : todo)
+      if (reset_call_ctl(b->sys[k], sn[k])) return bfail(b, RG_ERR_CUDA, "ctl upload");
+    std::vector<int> nsc;
+    for (int k : todo)
+      if (b->sys[k]->cfg.model == RG_MODEL_NSC) nsc.push_back(k);
+    const bool full = attempt == 0;
+    std::vector<TeamDesc> teams;
+    std::vector<int> members;
+    int grid = 0;
+    if (full && !b->plan_dirty) {
+      teams = b->teams;
+      members = b->members;
+      grid = b->grid;
+    } else {
+      plan(b, nsc, b->rods_per_block, teams, members, grid);
+      if (full) {
+        b->teams = teams;
+        b->members = members;
+        b->grid = grid;
+        b->plan_dirty = false;
+        drop_graph(b);
+      }
+    }
+    if (upload(b, teams, members)) return bfail(b, RG_ERR_CUDA, "upload views");
+    const long long l0 = g_launches;
+    cudaEventRecord(b->ev0, b->stream);
+    cudaError_t e = launch_nsc(b, (int)teams.size(), grid, nsteps, full);
+    if (e) return bfail(b, RG_ERR_CUDA, std::string("persistent launch: ") + cudaGetErrorString(e));
+    for (int k : todo)
+      if (b->sys[k]->cfg.model != RG_MODEL_NSC) launch_steps(b->sys[k], nsteps);
+    cudaEventRecord(b->ev1, b->stream);
+    if ((e = cudaGetLastError())) return bfail(b, RG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    for (int k : todo)
+      cudaMemcpyAsync(b->sys[k]->h_ctl, b->sys[k]->d_ctl, b->sys[k]->ctl_bytes, cudaMemcpyDeviceToHost, b->stream);
+    if ((e = cudaStreamSynchronize(b->stream))) return bfail(b, RG_ERR_CUDA, std::string("step: ") + cudaGetErrorString(e));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    total_ms += ms;
+    const long long launches = g_launches - l0;
+    std::vector<int> again;
+    for (int k : todo) {
+      rg_system* s = b->sys[k];
+      s->last_call_ms = ms;
+      s->last_call_launches = launches;
+      const int err = s->h_ctl->err;
+      if (!err) continue;
+      bool retry = false;
+      int rc = resolve_call(s, sn[k], err, &retry);
+      if (rc != RG_OK) return bfail(b, rc, "member " + std::to_string(k) + ": " + s->err_text);
+      again.push_back(k);
+    }
+    todo.swap(again);
+  }
+  if (!todo.empty()) return bfail(b, RG_ERR_CAPACITY, "capacity retries exhausted");
+  b->last_ms = total_ms;
+  if (restore_after) {
+    for (int k = 0; k < b->n; ++k) {
+      rg_system* s = b->sys[k];
+      const int one = 1;
+      if (restore_snapshot(s, sn[k]) || cudaMemcpy(&s->d_ctl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice))
+        return bfail(b, RG_ERR_CUDA, "restore");
+      s->contacts_fresh = false;
+    }
+    return RG_OK;
+  }
+  if (per)
+    for (int k = 0; k < b->n; ++k) {
+      fill_stats(b->sys[k], nsteps, &per[k]);
+      per[k].device_ms = total_ms;
+    }
+  return RG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rg_batch_create(const rg_config* cfgs, int n_systems, rg_batch** out) {
+  if (!cfgs || n_systems <= 0 || !out) return RG_ERR_ARG;
+  *out = nullptr;
+  rg_batch* b = new rg_batch();
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) || cudaEventCreate(&b->ev0) ||
+      cudaEventCreate(&b->ev1)) {
+    cudaGetLastError();
+    rg_batch_destroy(b);
+    return RG_ERR_CUDA;
+  }
+  for (int k = 0; k < n_systems; ++k) {
+    rg_system* s = nullptr;
+    int rc = rg_create(&cfgs[k], &s);
+    if (rc != RG_OK) {
+      rg_batch_destroy(b);
+      return rc;
+    }
+    cudaStreamDestroy(s->stream);  // members share the batch stream
+    s->stream = b->stream;
+    b->sys.push_back(s);
+    ++b->n;
+  }
+  b->coop_blocks = b->sys[0]->coop_blocks;
+  *out = b;
+  return RG_OK;
+}
+
+int rg_batch_destroy(rg_batch* b) {
+  if (!b) return RG_ERR_ARG;
+  drop_graph(b);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (rg_system* s : b->sys) {
+    s->stream = nullptr;
+    rg_destroy(s);
+  }
+  cudaFree(b->d_views); cudaFree(b->d_teams); cudaFree(b->d_members); cudaFree(b->d_bars);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return RG_OK;
+}
+
+int rg_batch_size(const rg_batch* b) { return b ? b->n : 0; }
+
+rg_system* rg_batch_member(rg_batch* b, int k) {
+  if (!b || k < 0 || k >= b->n) return nullptr;
+  return b->sys[k];
+}
+
+const char* rg_batch_last_error(const rg_batch* b) { return b ? b->err.c_str() : ""; }
+
+int rg_batch_set_bodies(rg_batch* b, int k, const double* radius, const double* half_height, const double* mass,
+                        const double* inertia, const double* restitution) {
+  if (!b || k < 0 || k >= b->n) return RG_ERR_ARG;
+  b->plan_dirty = true;
+  return rg_set_bodies(b->sys[k], radius, half_height, mass, inertia, restitution);
+}
+
+int rg_batch_set_state(rg_batch* b, int k, const double* x, const double* q, const double* v, const double* w) {
+  if (!b || k < 0 || k >= b->n) return RG_ERR_ARG;
+  return rg_set_state(b->sys[k], x, q, v, w, nullptr, nullptr);
+}
+
+int rg_batch_get_state(const rg_batch* b, int k, double* x, double* q, double* v, double* w) {
+  if (!b || k < 0 || k >= b->n) return RG_ERR_ARG;
+  return rg_get_state(b->sys[k], x, q, v, w, nullptr, nullptr);
+}
+
+int rg_batch_set_mlp(rg_batch* b, const float* params, size_t n) {
+  if (!b || !params) return RG_ERR_ARG;
+  for (rg_system* s : b->sys) {
+    if (s->cfg.model != RG_MODEL_NSC) continue;
+    int rc = rg_mlp_set_params(s, params, n);
+    if (rc != RG_OK) return rc;
+  }
+  return RG_OK;
+}
+
+int rg_batch_set_schedule(rg_batch* b, int rods_per_block, int use_graph) {
+  if (!b || rods_per_block < 0) return RG_ERR_ARG;
+  b->rods_per_block = rods_per_block;
+  b->use_graph = use_graph != 0;
+  b->plan_dirty = true;
+  drop_graph(b);
+  return RG_OK;
+}
+
+int rg_batch_get_schedule(const rg_batch* b, int* rods_per_block, int* grid, int* nteams) {
+  if (!b) return RG_ERR_ARG;
+  if (rods_per_block) *rods_per_block = b->rods_per_block;
+  if (grid) *grid = b->grid;
+  if (nteams) *nteams = (int)b->teams.size();
+  return RG_OK;
+}
+
+int rg_batch_step(rg_batch* b, int nsteps, rg_step_stats* per_system) {
+  if (!b || nsteps < 0) return RG_ERR_ARG;
+  return batch_call(b, nsteps, per_system);
+}
+
+// Times trial_steps steps for each candidate R (bodies per block; 0 = all
+// single-block teams) from the current state, puts the state back after each
+// trial and keeps the fastest R.  ms_out (optional, n_cand entries) receives
+// the trial times.
+int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand, int trial_steps, int* best_out,
+                      double* ms_out) {
+  if (!b || !candidates || n_cand <= 0 || trial_steps <= 0) return RG_ERR_ARG;
+  for (int c = 0; c < n_cand; ++c)
+    if (candidates[c] < 0) return RG_ERR_ARG;
+  int best = candidates[0];
+  double best_ms = 1e300;
+  for (int c = 0; c < n_cand; ++c) {
+    rg_batch_set_schedule(b, candidates[c], b->use_graph);
+    int rc = batch_call(b, trial_steps, nullptr, true);  // grows buffers, builds the graph
+    if (rc == RG_OK) rc = batch_call(b, trial_steps, nullptr, true);
+    if (rc != RG_OK) return rc;
+    const double ms = b->last_ms;
+    if (ms_out) ms_out[c] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = candidates[c];
+    }
+  }
+  rg_batch_set_schedule(b, best, b->use_graph);
+  if (best_out) *best_out = best;
+  return RG_OK;
+}
+
+}  // extern "C"

@@ -40,6 +40,7 @@ struct Ctl {
   long long collisions; // NSC impacts of the last step
   double jn_sum, jt_sum, pe;
   long long row_sweeps; // Σ contacts x sweeps (cumulative)
+  long long contact_steps;  // Σ velocity-solve contacts over steps
   int vel_contacts;     // NSC: contacts of the last velocity solve (lastHitCount)
   int prof_phases;      // 1: the persistent step records phase times
   long long phase_ns[12];  // persistent-step phase time accumulators
@@ -172,8 +173,8 @@ struct rg_system {
   int snap_wcap = 0;
 
   // MLP (learned warm start)
-  float* d_mlp = nullptr;
-  size_t mlp_n = 0;
+  void* mlp_host = nullptr;   // network parameters and training workspace (rg_mlp.cu)
+  double* d_ke = nullptr;     // kinetic-energy block partials
   bool mlp_ready = false;
   bool recording = false;
   int rec_cap = 0;
@@ -271,8 +272,24 @@ int nsc_team_blocks(const rg_system* s);
 size_t nsc_view_bytes();
 size_t nsc_team_bytes();
 // rg_mlp.cu
-void mlp_warm_launch(rg_system* s);
-void mlp_record_launch(rg_system* s);
+void mlp_free(rg_system* s);
+
+// rg_api.cu: one call of rg_step, in pieces the batch driver reuses.
+// Control words and the replay snapshot taken at the start of a call:
+struct Snapshot {
+  std::vector<char> ctl;
+  int hist_cur = 0;
+  int wn = 0;
+};
+int fail(rg_system* s, int code, const std::string& msg);
+int cuda_fail(rg_system* s, cudaError_t e, const char* where);
+cudaError_t take_snapshot(rg_system* s, Snapshot& sn);
+cudaError_t restore_snapshot(rg_system* s, const Snapshot& sn);
+cudaError_t reset_call_ctl(rg_system* s, const Snapshot& sn);
+int resolve_call(rg_system* s, Snapshot& sn, int err, bool* retry);
+void launch_steps(rg_system* s, int nsteps);
+void fill_stats(rg_system* s, int nsteps, rg_step_stats* stats);
+double kinetic_energy(rg_system* s);
 // launch geometry helper
 inline int grid_for(long long n, int bs, int maxb = 148 * 16) {
   long long g = (n + bs - 1) / bs;

@@ -1,0 +1,183 @@
+// rg_mlp_dev.cuh - the learned PSOR warm start on tensor cores.
+//
+// MLP 8 -> 128 -> 128 -> 128 -> 3, SiLU, BF16 weights and activations, FP32
+// accumulation.  One warp evaluates 16 contacts with mma.sync m16n8k16
+// (BF16 x BF16 -> FP32): the accumulator fragment of one layer is exactly the
+// A fragment of the next (rows g, g+8; columns 2t, 2t+1 of two adjacent
+// n-tiles), so hidden activations never leave registers.
+//
+// Features per contact (computed where the manifold row is built):
+//   0 gap φ, 1 v_n, 2 v_t1, 3 v_t2 (pre-solve relative velocity in the
+//   contact frame), 4-6 previous-step impulses (λn, λt1, λt2; 0 for a new
+//   contact), 7 contact-graph degree (other contacts on the two dynamic
+//   bodies).  Targets: converged (λn, λt1, λt2) of plain PSOR.  The network
+//   predicts the change from the previous impulse (features 4-6), so a
+//   persistent contact starts from its cached impulse plus a correction and
+//   a new one from the prediction alone; the change is scaled by the
+//   output scales (its RMS over the training records).
+#pragma once
+#include <cuda_bf16.h>
+
+#include "rg_common.cuh"
+
+namespace rg {
+
+constexpr int kMlpIn = 8, kMlpH = 128, kMlpOut = 3;
+// Float parameter vector layout (rg_mlp_param_count in include/rodgpu.h).
+constexpr int kOffW1 = 0;                          // 128 x 8
+constexpr int kOffB1 = kOffW1 + kMlpH * kMlpIn;    // 128
+constexpr int kOffW2 = kOffB1 + kMlpH;             // 128 x 128
+constexpr int kOffB2 = kOffW2 + kMlpH * kMlpH;
+constexpr int kOffW3 = kOffB2 + kMlpH;             // 128 x 128
+constexpr int kOffB3 = kOffW3 + kMlpH * kMlpH;
+constexpr int kOffW4 = kOffB3 + kMlpH;             // 3 x 128
+constexpr int kOffB4 = kOffW4 + kMlpOut * kMlpH;   // 3
+constexpr int kOffInMean = kOffB4 + kMlpOut;       // 8
+constexpr int kOffInScale = kOffInMean + kMlpIn;   // 8
+constexpr int kOffOutScale = kOffInScale + kMlpIn; // 3
+constexpr int kMlpParams = kOffOutScale + kMlpOut;
+
+// BF16 device copy used by inference: weights padded to mma tiles,
+// row-major [out][in]; W1 is 128 x 16 (inputs zero-padded), W4 is 8 x 128.
+struct MlpDev {
+  const __nv_bfloat16 *w1, *w2, *w3, *w4;
+  const float* p;  // FP32 parameter vector (biases, normalisation)
+};
+constexpr int kW1Pad = 16, kW4Pad = 8;
+
+__device__ inline unsigned pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<unsigned*>(&v);
+}
+__device__ inline float silu(float z) { return z / (1.0f + __expf(-z)); }
+
+__device__ inline void mma_bf16(float* c, unsigned a0, unsigned a1, unsigned a2, unsigned a3, unsigned b0,
+                                unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// B fragment of W (row-major [n][k], leading dimension ldk) for n-tile nt,
+// k-tile kt: (k = 2t..2t+1, n = g) and (k = 2t+8.., n = g).
+__device__ inline void load_b(const __nv_bfloat16* W, int ldk, int nt, int kt, int lane, unsigned& b0,
+                              unsigned& b1) {
+  const int g = lane >> 2, t = lane & 3;
+  const __nv_bfloat16* row = W + (size_t)(nt * 8 + g) * ldk + kt * 16 + 2 * t;
+  b0 = *reinterpret_cast<const unsigned*>(row);
+  b1 = *reinterpret_cast<const unsigned*>(row + 8);
+}
+
+// One hidden layer 128 -> 128: a[kt] (4 regs each, 8 k-tiles) -> out a.
+__device__ inline void hidden_layer(unsigned (&a)[8][4], const __nv_bfloat16* W, const float* bias, int lane) {
+  const int t = lane & 3;
+  unsigned na[8][4];
+#pragma unroll
+  for (int kk = 0; kk < 8; ++kk) {
+    float acc[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int nt = 2 * kk + h;
+      const float bl = bias[nt * 8 + 2 * t], bh = bias[nt * 8 + 2 * t + 1];
+      acc[h][0] = bl; acc[h][1] = bh; acc[h][2] = bl; acc[h][3] = bh;
+#pragma unroll
+      for (int kt = 0; kt < 8; ++kt) {
+        unsigned b0, b1;
+        load_b(W, kMlpH, nt, kt, lane, b0, b1);
+        mma_bf16(acc[h], a[kt][0], a[kt][1], a[kt][2], a[kt][3], b0, b1);
+      }
+    }
+    na[kk][0] = pack_bf16(silu(acc[0][0]), silu(acc[0][1]));
+    na[kk][1] = pack_bf16(silu(acc[0][2]), silu(acc[0][3]));
+    na[kk][2] = pack_bf16(silu(acc[1][0]), silu(acc[1][1]));
+    na[kk][3] = pack_bf16(silu(acc[1][2]), silu(acc[1][3]));
+  }
+#pragma unroll
+  for (int kk = 0; kk < 8; ++kk)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) a[kk][r] = na[kk][r];
+}
+
+// Evaluates the MLP for rows row0..row0+15 of feat (float, [8][ld]) and
+// writes the unscaled outputs times out_scale to out ([3][ld]); rows >= n
+// are ignored.  All 32 lanes of the warp must call it.
+__device__ inline void mlp_warp(const MlpDev& M, const float* feat, int ld, int row0, int n, float* out,
+                                int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const float* P = M.p;
+  // layer 1 input fragment: X (16 rows x 16 k, inputs 8..15 are zero)
+  unsigned x0, x1;
+  {
+    float v[4];
+    const int rows[2] = {row0 + g, row0 + g + 8};
+    for (int rr = 0; rr < 2; ++rr) {
+      for (int cc = 0; cc < 2; ++cc) {
+        int k = 2 * t + cc;
+        int r = rows[rr];
+        float f = r < n ? feat[(size_t)k * ld + r] : 0.0f;
+        v[rr * 2 + cc] = (f - P[kOffInMean + k]) * P[kOffInScale + k];
+      }
+    }
+    x0 = pack_bf16(v[0], v[1]);
+    x1 = pack_bf16(v[2], v[3]);
+  }
+  unsigned a[8][4];
+#pragma unroll
+  for (int kk = 0; kk < 8; ++kk) {
+    float acc[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int nt = 2 * kk + h;
+      const float bl = P[kOffB1 + nt * 8 + 2 * t], bh = P[kOffB1 + nt * 8 + 2 * t + 1];
+      acc[h][0] = bl; acc[h][1] = bh; acc[h][2] = bl; acc[h][3] = bh;
+      unsigned b0, b1;
+      load_b(M.w1, kW1Pad, nt, 0, lane, b0, b1);
+      mma_bf16(acc[h], x0, x1, 0u, 0u, b0, b1);
+    }
+    a[kk][0] = pack_bf16(silu(acc[0][0]), silu(acc[0][1]));
+    a[kk][1] = pack_bf16(silu(acc[0][2]), silu(acc[0][3]));
+    a[kk][2] = pack_bf16(silu(acc[1][0]), silu(acc[1][1]));
+    a[kk][3] = pack_bf16(silu(acc[1][2]), silu(acc[1][3]));
+  }
+  hidden_layer(a, M.w2, P + kOffB2, lane);
+  hidden_layer(a, M.w3, P + kOffB3, lane);
+  float acc[4];
+  {
+    const float bl = 2 * t < kMlpOut ? P[kOffB4 + 2 * t] : 0.0f;
+    const float bh = 2 * t + 1 < kMlpOut ? P[kOffB4 + 2 * t + 1] : 0.0f;
+    acc[0] = bl; acc[1] = bh; acc[2] = bl; acc[3] = bh;
+#pragma unroll
+    for (int kt = 0; kt < 8; ++kt) {
+      unsigned b0, b1;
+      load_b(M.w4, kMlpH, 0, kt, lane, b0, b1);
+      mma_bf16(acc, a[kt][0], a[kt][1], a[kt][2], a[kt][3], b0, b1);
+    }
+  }
+  // c0,c1: row g, outputs 2t, 2t+1; c2,c3: row g+8
+  const int rows[2] = {row0 + g, row0 + g + 8};
+  for (int rr = 0; rr < 2; ++rr) {
+    int r = rows[rr];
+    if (r >= n) continue;
+    for (int cc = 0; cc < 2; ++cc) {
+      int o = 2 * t + cc;
+      if (o < kMlpOut) out[(size_t)o * ld + r] = acc[rr * 2 + cc] * P[kOffOutScale + o];
+    }
+  }
+}
+
+// Impulse prediction projected onto the admissible set: λn >= 0 and the
+// Coulomb cone |λt| <= μ λn.
+__device__ inline void cone_clamp(double& ln, double& l1, double& l2, double mu) {
+  ln = ln > 0.0 ? ln : 0.0;
+  double lim = mu * ln;
+  double m = sqrt(l1 * l1 + l2 * l2);
+  if (m > lim) {
+    double s = m > 0.0 ? lim / m : 0.0;
+    l1 *= s;
+    l2 *= s;
+  }
+}
+
+}  // namespace rg

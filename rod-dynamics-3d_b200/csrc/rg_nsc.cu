@@ -31,15 +31,11 @@ namespace rg {
 
 GridDev* detector_grid(rg_system* s);
 unsigned long long* detector_bounds(rg_system* s);
+MlpDev mlp_dev(rg_system* s);
 
 // ---------------------------------------------------------------------------
 // Teams and team barriers.
 // ---------------------------------------------------------------------------
-struct TeamDesc {
-  int b0, nb, sys, pad;
-  unsigned int* bar;  // 4 words: full-team count/gen, subset count/gen
-};
-
 struct Team {
   int b0, nb;
   unsigned int* bar;
@@ -450,6 +446,7 @@ __device__ __noinline__ bool psor_phase(const Team& T, const NscView& V, int C, 
         ctl->sweeps_last = sweeps;
         ctl->sweeps_sum += sweeps;
         ctl->row_sweeps += (long long)C * sweeps;
+        ctl->contact_steps += C;
         if (res >= cfg.nsc_tol) ctl->not_conv += 1;
         if (res > ctl->max_residual) ctl->max_residual = res;
       }
@@ -614,6 +611,8 @@ struct SmallSmem {
   int cnt[kMaxColors + 1], coff[kMaxColors + 1], cur[kMaxColors + 1];
   int nloc, rem, ncol, act;
   double red[32];
+  float feat[kMlpIn * kSmallC];      // learned warm start features [8][kSmallC]
+  float pred[kMlpOut * kSmallC];     // predicted impulse changes [3][kSmallC]
 };
 
 __device__ inline double small_block_max(double v, SmallSmem& S) {
@@ -753,10 +752,37 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
   }
   RowIO R{S.row, S.lam, kSmallC};
   const int W = *(volatile int*)V.wn;
+  int* deg = reinterpret_cast<int*>(S.pmax);  // free after colouring
+  if (V.feat_on) {
+    for (int s = t; s < S.nloc; s += blockDim.x) deg[s] = 0;
+    __syncthreads();
+  }
   int coll = 0;
-  if (t < C) coll = build_row(V.st, V.con, cfg, S.order[t], t, R, V.wkey, V.wlam, W, V.wcap);
+  if (t < C) {
+    const int c = S.order[t];
+    coll = build_row(V.st, V.con, cfg, c, t, R, V.wkey, V.wlam, W, V.wcap, V.feat_on ? S.feat : nullptr, kSmallC);
+    if (V.feat_on) {
+      if (S.dyn[S.la[c]]) atomicAdd(&deg[S.la[c]], 1);
+      if (S.dyn[S.lb[c]]) atomicAdd(&deg[S.lb[c]], 1);
+    }
+  }
   int bcoll = __syncthreads_count(coll);
   if (t == 0 && bcoll) atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->collisions), (unsigned long long)bcoll);
+  if (V.feat_on) {
+    if (t < C) {
+      const int c = S.order[t], sa = S.la[c], sb = S.lb[c];
+      S.feat[7 * kSmallC + t] = (float)((S.dyn[sa] ? deg[sa] - 1 : 0) + (S.dyn[sb] ? deg[sb] - 1 : 0));
+    }
+    __syncthreads();
+    if (V.use_mlp) {
+      // one warp per 16 contacts on the tensor cores, then the cone
+      const int row0 = (t >> 5) * 16;
+      if (row0 < C) mlp_warp(V.mlp, S.feat, kSmallC, row0, C, S.pred, t & 31);
+      __syncthreads();
+      if (t < C) mlp_apply(R, S.pred, kSmallC, t, cfg.nsc_mu);
+      __syncthreads();
+    }
+  }
   pc.mark(3);
   Vel Vv{Vec3A{S.vel, S.vel + kSmallB, S.vel + 2 * kSmallB},
          Vec3A{S.vel + 3 * kSmallB, S.vel + 4 * kSmallB, S.vel + 5 * kSmallB}};
@@ -795,6 +821,17 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
     V.st.w.st(x, mk3(S.vel[3 * kSmallB + s], S.vel[4 * kSmallB + s], S.vel[5 * kSmallB + s]));
   }
   small_unmap(V, S);
+  if (V.rec_cap > 0 && C > 0) {
+    // records (features, converged impulses) in slot order
+    const int base = *(volatile int*)&ctl->rec_n;
+    if (p < C && base + p < V.rec_cap) {
+      const size_t r = (size_t)(base + p);
+      for (int k = 0; k < kMlpIn; ++k) V.rec_x[r * kMlpIn + k] = S.feat[k * kSmallC + p];
+      for (int k = 0; k < kMlpOut; ++k) V.rec_y[r * kMlpOut + k] = (float)S.lam[k * kSmallC + p];
+    }
+    __syncthreads();
+    if (t == 0) ctl->rec_n = base + C;
+  }
   double jn = 0, jt = 0;
   if (p < C) {
     double l0 = S.lam[p], l1 = S.lam[kSmallC + p], l2 = S.lam[2 * kSmallC + p];
@@ -820,6 +857,7 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
     if (C > 0) {
       ctl->sweeps_sum += sweeps;
       ctl->row_sweeps += (long long)C * sweeps;
+      ctl->contact_steps += C;
       if (res >= cfg.nsc_tol) ctl->not_conv += 1;
       if (res > ctl->max_residual) ctl->max_residual = res;
     }
@@ -989,13 +1027,48 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
   {
     RowIO R{V.row, V.lam, V.ccap};
     const int W = *(volatile int*)V.wn;
+    const double* im = st.inv_mass;
+    int* deg = V.owner;  // free between colouring and the next colouring
+    if (V.feat_on) {
+      for (int c = tid; c < C; c += TS) {
+        deg[V.con.a[c]] = 0;
+        deg[V.con.b[c]] = 0;
+      }
+      if (!team_sync(T)) return false;
+    }
     int coll = 0;
-    for (int p = tid; p < C; p += TS)
-      coll += build_row(st, V.con, cfg, V.order[p], p, R, V.wkey, V.wlam, W, V.wcap);
+    for (int p = tid; p < C; p += TS) {
+      const int c = V.order[p];
+      coll += build_row(st, V.con, cfg, c, p, R, V.wkey, V.wlam, W, V.wcap, V.feat_on ? V.feat : nullptr, V.ccap);
+      if (V.feat_on) {
+        if (im[V.con.a[c]] > 0.0) atomicAdd(&deg[V.con.a[c]], 1);
+        if (im[V.con.b[c]] > 0.0) atomicAdd(&deg[V.con.b[c]], 1);
+      }
+    }
     int bcoll = block_reduce_sum_i(coll, sm.red_i);
     if (threadIdx.x == 0 && bcoll)
       atomicAdd(reinterpret_cast<unsigned long long*>(&ctl->collisions), (unsigned long long)bcoll);
     if (!team_sync(T)) return false;
+    if (V.feat_on) {
+      for (int p = tid; p < C; p += TS) {
+        const int c = V.order[p], a = V.con.a[c], b = V.con.b[c];
+        V.feat[7 * (size_t)V.ccap + p] = (float)((im[a] > 0.0 ? deg[a] - 1 : 0) + (im[b] > 0.0 ? deg[b] - 1 : 0));
+      }
+      if (V.use_mlp) {
+        // each warp of the team evaluates tiles of 16 slots on the tensor
+        // cores; its own lanes then apply the tile's predictions
+        __syncthreads();
+        if (!team_sync(T)) return false;
+        const int lane = threadIdx.x & 31, gw = tid >> 5, nw = TS >> 5;
+        for (int row0 = gw * 16; row0 < C; row0 += nw * 16) {
+          mlp_warp(V.mlp, V.feat, V.ccap, row0, C, V.pred, lane);
+          __syncwarp();
+          if (lane < 16 && row0 + lane < C) mlp_apply(R, V.pred, V.ccap, row0 + lane, cfg.nsc_mu);
+          __syncwarp();
+        }
+      }
+      if (!team_sync(T)) return false;
+    }
   }
   pc.mark(3);
   // 3) PSOR
@@ -1027,6 +1100,16 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
       *V.wn = C;
       ctl->vel_contacts = C;
     }
+    int rec_base = 0;
+    if (V.rec_cap > 0 && !small && C > 0) {
+      // records (features, converged impulses) in slot order
+      rec_base = *(volatile int*)&ctl->rec_n;
+      for (int p = tid; p < C && rec_base + p < V.rec_cap; p += TS) {
+        const size_t r = (size_t)(rec_base + p);
+        for (int k = 0; k < kMlpIn; ++k) V.rec_x[r * kMlpIn + k] = V.feat[(size_t)k * V.ccap + p];
+        for (int k = 0; k < kMlpOut; ++k) V.rec_y[r * kMlpOut + k] = (float)R.lam[(size_t)k * R.ccap + p];
+      }
+    }
     int bad = 0;
     double dmax = 0.0;
     for (int i = tid; i < n; i += TS) {
@@ -1039,6 +1122,8 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     double bm = block_reduce_max(dmax, sm.red_d);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
     if (!team_sync(T)) return false;
+    // every block has read rec_n before the barrier
+    if (V.rec_cap > 0 && !small && C > 0 && tid == 0) ctl->rec_n = rec_base + C;
   }
   pc.mark(5);
   // 5) position projection (nsc_contact.cpp:659-880)
@@ -1069,23 +1154,32 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
 #endif
 constexpr int kBlock = RG_NSC_BLOCK;  // threads per block of the persistent step
 
+// Each block finds its team (teams are sorted by b0), then runs nsteps steps
+// of the team's systems, one system after the other within a step.  A
+// system whose step failed (error bits set) returns at once from its later
+// steps; the others carry on.
 __global__ void __launch_bounds__(kBlock, 1) k_nsc_run(const NscView* views, const TeamDesc* teams, int nteams,
-                                                   int nsteps) {
+                                                   const int* members, int nsteps) {
   __shared__ SmemNsc sm;
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   SmallSmem& S = *reinterpret_cast<SmallSmem*>(dyn_smem);
-  int k = -1;
-  for (int t = 0; t < nteams; ++t)
-    if ((int)blockIdx.x >= teams[t].b0 && (int)blockIdx.x < teams[t].b0 + teams[t].nb) {
-      k = t;
-      break;
+  int lo = 0, hi = nteams;  // last team with b0 <= blockIdx.x
+  while (hi - lo > 1) {
+    int m = (lo + hi) >> 1;
+    if (teams[m].b0 <= (int)blockIdx.x) lo = m;
+    else hi = m;
+  }
+  const TeamDesc td = teams[lo];
+  if ((int)blockIdx.x < td.b0 || (int)blockIdx.x >= td.b0 + td.nb) return;
+  for (int s = 0; s < nsteps; ++s) {
+    bool any = false;
+    for (int m = td.first; m < td.first + td.count; ++m) {
+      const NscView& V = views[members ? members[m] : m];
+      Team T{td.b0, td.nb, td.bar, &V.ctl->err};
+      any |= nsc_step(T, V, sm, S);
     }
-  if (k < 0) return;
-  const TeamDesc td = teams[k];
-  const NscView& V = views[td.sys];
-  Team T{td.b0, td.nb, td.bar, &V.ctl->err};
-  for (int s = 0; s < nsteps; ++s)
-    if (!nsc_step(T, V, sm, S)) break;
+    if (!any) break;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1116,6 +1210,14 @@ NscView make_view(rg_system* s) {
   V.ccap = s->ccap;
   V.blk = N.blk;
   V.slot_of = N.slot_of;
+  V.feat = s->d_feat;
+  V.pred = s->d_pred;
+  V.use_mlp = (s->cfg.nsc_warm_start == RG_WARM_MLP && s->mlp_ready) ? 1 : 0;
+  V.rec_cap = s->recording ? s->rec_cap : 0;
+  V.rec_x = s->d_rec_x;
+  V.rec_y = s->d_rec_y;
+  V.feat_on = (V.use_mlp || V.rec_cap > 0) ? 1 : 0;
+  if (V.use_mlp) V.mlp = mlp_dev(s);
   return V;
 }
 
@@ -1146,24 +1248,42 @@ static void launch_coop(const void* fn, int grid, int block, void** args, cudaSt
 void nsc_run_launch(rg_system* s, int nsteps) {
   NscView V = make_view(s);
   const int nb = nsc_team_blocks(s);
-  TeamDesc td{0, nb, 0, 0, s->nsc.bar};
+  TeamDesc td{0, nb, 0, 1, s->nsc.bar};
   cudaMemcpyAsync(s->nsc.view_dev, &V, sizeof(NscView), cudaMemcpyHostToDevice, s->stream);
   cudaMemcpyAsync(s->nsc.team_dev, &td, sizeof(TeamDesc), cudaMemcpyHostToDevice, s->stream);
   cudaMemsetAsync(s->nsc.bar, 0, 4 * sizeof(unsigned int), s->stream);
   const NscView* views = reinterpret_cast<const NscView*>(s->nsc.view_dev);
   const TeamDesc* teams = reinterpret_cast<const TeamDesc*>(s->nsc.team_dev);
   int nteams = 1;
-  void* args[] = {&views, &teams, &nteams, &nsteps};
+  const int* members = nullptr;
+  void* args[] = {&views, &teams, &nteams, &members, &nsteps};
+  nsc_set_smem();
+  ProfScope p(s, ST_OTHER);
+  launch_coop((const void*)k_nsc_run, nb, kBlock, args, s->stream, sizeof(SmallSmem));
+  s->contacts_fresh = false;
+}
+
+void nsc_set_smem() {
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute((const void*)k_nsc_run, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(SmallSmem));
     attr_set = true;
   }
-  ProfScope p(s, ST_OTHER);
-  launch_coop((const void*)k_nsc_run, nb, kBlock, args, s->stream, sizeof(SmallSmem));
-  s->contacts_fresh = false;
 }
+
+// nsteps steps of many systems as one persistent cooperative launch: teams
+// (device array, sorted by b0) cover blocks [0, grid); team k runs the
+// systems members[first_k .. first_k + count_k) of views.
+void nsc_batch_launch(const NscView* views, const TeamDesc* teams, int nteams, const int* members, int grid,
+                      int nsteps, cudaStream_t st) {
+  nsc_set_smem();
+  void* args[] = {&views, &teams, &nteams, &members, &nsteps};
+  launch_coop((const void*)k_nsc_run, grid, kBlock, args, st, sizeof(SmallSmem));
+}
+
+int nsc_block_threads() { return kBlock; }
+size_t nsc_block_smem() { return sizeof(SmallSmem) + sizeof(SmemNsc); }
 
 size_t nsc_view_bytes() { return sizeof(NscView); }
 size_t nsc_team_bytes() { return sizeof(TeamDesc); }

@@ -5,6 +5,7 @@
 // App::physicsStep (src/app/main.cpp:4397-4408, :4469-4483, :4508-4517).
 #pragma once
 #include "rg_detect_dev.cuh"
+#include "rg_mlp_dev.cuh"
 
 namespace rg {
 
@@ -58,10 +59,12 @@ __device__ inline int lower_bound_key(const unsigned long long* k, int n, unsign
 }
 
 // Manifold row of contact c into slot p; returns 1 for an impact
-// (v_n_pre < -1e-6, NscContactSolver::countImpacts).
+// (v_n_pre < -1e-6, NscContactSolver::countImpacts).  When feat is given,
+// the learned warm start's features 0-6 of slot p go to feat[k * fld + p]
+// (feature 7, the contact-graph degree, is filled by the caller).
 __device__ inline int build_row(const State& st, const Contacts& con, const rg_config& cfg, int c, int p,
                                 const RowIO& R, const unsigned long long* wkey, const double* wlam, int W,
-                                int wcap) {
+                                int wcap, float* feat = nullptr, int fld = 0) {
   const double beta = cfg.nsc_position_stabilization ? cfg.nsc_beta * 0.01 : cfg.nsc_beta;
   const int a = con.a[c], b = con.b[c];
   d3 pa{con.comp(0)[c], con.comp(1)[c], con.comp(2)[c]};
@@ -96,7 +99,7 @@ __device__ inline int build_row(const State& st, const Contacts& con, const rg_c
   R.r(R_PHI, p) = phi;
   R.r(R_VNPRE, p) = vnp;
   double l0 = 0, l1 = 0, l2 = 0;
-  if (cfg.nsc_warm_start == RG_WARM_CACHE && W > 0) {
+  if (cfg.nsc_warm_start != RG_WARM_NONE && W > 0) {
     unsigned long long k = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
     int q = lower_bound_key(wkey, W, k);
     if (q < W && wkey[q] == k) {
@@ -108,7 +111,28 @@ __device__ inline int build_row(const State& st, const Contacts& con, const rg_c
   R.lam[p] = l0;
   R.lam[R.ccap + p] = l1;
   R.lam[2 * R.ccap + p] = l2;
+  if (feat) {
+    feat[p] = (float)phi;
+    feat[fld + p] = (float)vnp;
+    feat[2 * fld + p] = (float)dot(t1, vrel);
+    feat[3 * fld + p] = (float)dot(t2, vrel);
+    feat[4 * fld + p] = (float)l0;
+    feat[5 * fld + p] = (float)l1;
+    feat[6 * fld + p] = (float)l2;
+  }
   return vnp < -1e-6 ? 1 : 0;
+}
+
+// Learned warm start of slot p: previous impulse (already in R.lam) plus the
+// network's predicted change, projected onto the friction cone.
+__device__ inline void mlp_apply(const RowIO& R, const float* pred, int pld, int p, double mu) {
+  double ln = R.lam[p] + (double)pred[p];
+  double l1 = R.lam[R.ccap + p] + (double)pred[pld + p];
+  double l2 = R.lam[2 * R.ccap + p] + (double)pred[2 * pld + p];
+  cone_clamp(ln, l1, l2, mu);
+  R.lam[p] = ln;
+  R.lam[R.ccap + p] = l1;
+  R.lam[2 * R.ccap + p] = l2;
 }
 
 struct Vel {
@@ -289,6 +313,29 @@ struct NscView {
   int ccap;
   int* blk;      // per-block scratch of the team
   int* slot_of;  // per-body local slot of the in-block solver (-1 when unused)
+  // learned warm start: features [8][ccap] and predictions [3][ccap] of the
+  // team path, the network, and the record buffers ([n][8], [n][3])
+  float *feat, *pred;
+  int feat_on;   // features needed (learned warm start or recording)
+  int use_mlp;   // warm start from the network
+  MlpDev mlp;
+  float *rec_x, *rec_y;
+  int rec_cap;   // 0: not recording
 };
+
+// A team of blocks [b0, b0 + nb) of the persistent step and the systems it
+// runs (entries first .. first + count - 1 of the member list).  A team of
+// several blocks runs exactly one system.
+struct TeamDesc {
+  int b0, nb, first, count;
+  unsigned int* bar;  // 4 words: full-team count/gen, subset count/gen
+};
+
+void nsc_set_smem();
+void nsc_batch_launch(const NscView* views, const TeamDesc* teams, int nteams, const int* members, int grid,
+                      int nsteps, cudaStream_t st);
+int nsc_block_threads();
+size_t nsc_block_smem();
+NscView make_view(rg_system* s);
 
 }  // namespace rg

@@ -56,7 +56,8 @@ class RgStepStats(ctypes.Structure):
         ("history_size", ctypes.c_int64), ("residual", _d), ("jn_sum", _d), ("jt_sum", _d),
         ("potential_energy", _d), ("kinetic_energy", _d), ("max_residual", _d),
         ("not_converged", ctypes.c_int64), ("device_ms", _d), ("psor_row_sweeps", ctypes.c_int64),
-        ("kernel_launches", ctypes.c_int64), ("reserved", ctypes.c_int64 * 3),
+        ("kernel_launches", ctypes.c_int64), ("contact_steps", ctypes.c_int64),
+        ("reserved", ctypes.c_int64 * 2),
     ]
 
     def as_dict(self):
@@ -75,7 +76,8 @@ ABI_SYMBOLS = [
     "rg_mlp_param_count", "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_record",
     "rg_mlp_records", "rg_mlp_train", "rg_mlp_infer", "rg_batch_create", "rg_batch_destroy",
     "rg_batch_set_bodies", "rg_batch_set_state", "rg_batch_get_state", "rg_batch_step",
-    "rg_batch_set_mlp",
+    "rg_batch_set_mlp", "rg_mlp_grad", "rg_batch_size", "rg_batch_member", "rg_batch_last_error",
+    "rg_batch_set_schedule", "rg_batch_get_schedule", "rg_batch_autotune",
 ]
 
 
@@ -120,6 +122,24 @@ def lib():
         L.rg_mlp_train.argtypes = [P, fp, fp, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_float, ctypes.c_uint64, fp]
         L.rg_mlp_infer.argtypes = [P, fp, fp, ctypes.c_size_t]
+        L.rg_mlp_grad.argtypes = [P, fp, fp, ctypes.c_size_t, fp, fp]
+        L.rg_batch_create.argtypes = [ctypes.POINTER(RgConfig), ctypes.c_int, ctypes.POINTER(P)]
+        L.rg_batch_destroy.argtypes = [P]
+        L.rg_batch_set_bodies.argtypes = [P, ctypes.c_int, dp, dp, dp, dp, dp]
+        L.rg_batch_set_state.argtypes = [P, ctypes.c_int, dp, dp, dp, dp]
+        L.rg_batch_get_state.argtypes = [P, ctypes.c_int, dp, dp, dp, dp]
+        L.rg_batch_step.argtypes = [P, ctypes.c_int, ctypes.POINTER(RgStepStats)]
+        L.rg_batch_set_mlp.argtypes = [P, fp, ctypes.c_size_t]
+        L.rg_batch_size.argtypes = [P]
+        L.rg_batch_member.argtypes = [P, ctypes.c_int]
+        L.rg_batch_member.restype = P
+        L.rg_batch_last_error.argtypes = [P]
+        L.rg_batch_last_error.restype = ctypes.c_char_p
+        L.rg_batch_set_schedule.argtypes = [P, ctypes.c_int, ctypes.c_int]
+        L.rg_batch_get_schedule.argtypes = [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]
+        L.rg_batch_autotune.argtypes = [P, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_int), dp]
         _lib = L
     return _lib
 
@@ -179,10 +199,14 @@ class RgError(RuntimeError):
 class System:
     """One rg_system: device state of N capsules advanced by librodgpu."""
 
-    def __init__(self, cfg):
+    def __init__(self, cfg, _borrowed=None):
         self._lib = lib()
         self.cfg = cfg
         self.n = cfg.n_bodies
+        self._owned = _borrowed is None
+        if _borrowed is not None:  # a batch member: the batch owns it
+            self._h = ctypes.c_void_p(_borrowed)
+            return
         h = ctypes.c_void_p()
         rc = self._lib.rg_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != 0:
@@ -196,7 +220,8 @@ class System:
 
     def close(self):
         if getattr(self, "_h", None):
-            self._lib.rg_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self._lib.rg_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -289,3 +314,144 @@ class System:
                                              cap, ctypes.byref(n)), "history")
         m = n.value
         return pairs[:m], val[:m], fr[:m]
+
+    # ---- learned PSOR warm start -------------------------------------------
+    MLP_IN, MLP_OUT = 8, 3
+
+    def mlp_param_count(self):
+        return int(self._lib.rg_mlp_param_count())
+
+    def mlp_set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self._lib.rg_mlp_set_params(self._h, ptr(p, ctypes.c_float), p.size), "mlp_set_params")
+
+    def mlp_get_params(self):
+        p = np.zeros(self.mlp_param_count(), np.float32)
+        self._check(self._lib.rg_mlp_get_params(self._h, ptr(p, ctypes.c_float), p.size), "mlp_get_params")
+        return p
+
+    def mlp_record(self, enable=True, cap=1 << 20):
+        self._check(self._lib.rg_mlp_record(self._h, int(enable), int(cap)), "mlp_record")
+
+    def mlp_records(self):
+        n = ctypes.c_size_t()
+        self._lib.rg_mlp_records(self._h, None, None, 0, ctypes.byref(n))
+        m = n.value
+        x = np.zeros((max(m, 1), 8), np.float32)
+        y = np.zeros((max(m, 1), 3), np.float32)
+        rc = self._lib.rg_mlp_records(self._h, ptr(x, ctypes.c_float), ptr(y, ctypes.c_float), m, ctypes.byref(n))
+        self._check(rc, "mlp_records")
+        return x[:m], y[:m]
+
+    def mlp_train(self, features, targets, epochs=20, batch=1024, lr=1e-3, seed=0):
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        y = np.ascontiguousarray(targets, dtype=np.float32)
+        loss = ctypes.c_float()
+        self._check(self._lib.rg_mlp_train(self._h, ptr(x, ctypes.c_float), ptr(y, ctypes.c_float), len(x),
+                                           int(epochs), int(batch), float(lr), int(seed), ctypes.byref(loss)),
+                    "mlp_train")
+        return float(loss.value)
+
+    def mlp_grad(self, features, targets):
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        y = np.ascontiguousarray(targets, dtype=np.float32)
+        g = np.zeros(self.mlp_param_count(), np.float32)
+        loss = ctypes.c_float()
+        self._check(self._lib.rg_mlp_grad(self._h, ptr(x, ctypes.c_float), ptr(y, ctypes.c_float), len(x),
+                                          ptr(g, ctypes.c_float), ctypes.byref(loss)), "mlp_grad")
+        return g, float(loss.value)
+
+    def mlp_infer(self, features):
+        x = np.ascontiguousarray(features, dtype=np.float32)
+        out = np.zeros((len(x), 3), np.float32)
+        self._check(self._lib.rg_mlp_infer(self._h, ptr(x, ctypes.c_float), ptr(out, ctypes.c_float), len(x)),
+                    "mlp_infer")
+        return out
+
+
+class Batch:
+    """rg_batch: independent systems of uneven size stepped by one persistent
+    launch (CUDA-graph replayed) with an autotuned team schedule."""
+
+    def __init__(self, cfgs):
+        self._lib = lib()
+        self.cfgs = list(cfgs)
+        arr = (RgConfig * len(self.cfgs))(*self.cfgs)
+        h = ctypes.c_void_p()
+        rc = self._lib.rg_batch_create(arr, len(self.cfgs), ctypes.byref(h))
+        if rc != 0:
+            raise RgError(rc, "rg_batch_create failed")
+        self._h = h
+        self._keep = {}
+
+    def __len__(self):
+        return len(self.cfgs)
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = self._lib.rg_batch_last_error(self._h)
+            raise RgError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def member(self, k):
+        """Member k as a System (owned by the batch)."""
+        h = self._lib.rg_batch_member(self._h, int(k))
+        if not h:
+            raise RgError(1, f"no member {k}")
+        return System(self.cfgs[k], _borrowed=h)
+
+    def set_bodies(self, k, radius, half_height, mass, inertia, restitution=None):
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (radius, half_height, mass, inertia)]
+        rest = None if restitution is None else np.ascontiguousarray(restitution, dtype=np.float64)
+        self._keep[k] = args + [rest]
+        self._check(self._lib.rg_batch_set_bodies(self._h, int(k), *[ptr(a) for a in args], ptr(rest)),
+                    "batch_set_bodies")
+
+    def set_state(self, k, x, q, v, w):
+        arr = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, q, v, w)]
+        self._check(self._lib.rg_batch_set_state(self._h, int(k), *[ptr(a) for a in arr]), "batch_set_state")
+
+    def get_state(self, k):
+        n = self.cfgs[k].n_bodies
+        x, v, w = (np.zeros((n, 3)) for _ in range(3))
+        q = np.zeros((n, 4))
+        self._check(self._lib.rg_batch_get_state(self._h, int(k), ptr(x), ptr(q), ptr(v), ptr(w)),
+                    "batch_get_state")
+        return {"x": x, "q": q, "v": v, "w": w}
+
+    def step(self, nsteps=1):
+        st = (RgStepStats * len(self.cfgs))()
+        self._check(self._lib.rg_batch_step(self._h, int(nsteps), st), "batch_step")
+        return [s.as_dict() for s in st]
+
+    def set_mlp(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self._lib.rg_batch_set_mlp(self._h, ptr(p, ctypes.c_float), p.size), "batch_set_mlp")
+
+    def set_schedule(self, rods_per_block=0, use_graph=True):
+        self._check(self._lib.rg_batch_set_schedule(self._h, int(rods_per_block), int(use_graph)),
+                    "batch_set_schedule")
+
+    def schedule(self):
+        r, g, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self._lib.rg_batch_get_schedule(self._h, ctypes.byref(r), ctypes.byref(g), ctypes.byref(t)),
+                    "batch_get_schedule")
+        return {"rods_per_block": r.value, "grid": g.value, "teams": t.value}
+
+    def autotune(self, candidates=(0, 1024, 2048, 4096, 8192), trial_steps=10):
+        c = (ctypes.c_int * len(candidates))(*candidates)
+        best = ctypes.c_int()
+        ms = np.zeros(len(candidates))
+        self._check(self._lib.rg_batch_autotune(self._h, c, len(candidates), int(trial_steps), ctypes.byref(best),
+                                                ptr(ms)), "batch_autotune")
+        return best.value, dict(zip(candidates, ms.tolist()))

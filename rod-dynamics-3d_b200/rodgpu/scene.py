@@ -107,3 +107,51 @@ def config_dict(cfg):
             v = list(v)
         out[k] = v
     return out
+
+
+# Isotropic RSA jams near phi * (L/d) ~ 2.4 and slows down well before;
+# batch members are capped at phi <= 1.6 / aspect ratio so every packing is
+# placed in full within seconds.
+def rsa_phi_max(ar):
+    return 1.6 / ar
+
+
+def batch_members(n_systems=256, seed=7, n_lo=500, n_hi=20000, ars=(5, 10, 20, 40), phi_lo=0.05,
+                  phi_hi=0.25, models=("hertz-mindlin", "nsc")):
+    """Member specs of the uneven-batch workload: N log-uniform in
+    [n_lo, n_hi], aspect ratio from `ars` (L=1, d=1/AR), phi ~ U[phi_lo,
+    phi_hi] capped at the RSA limit, mu ~ U[0, 1]; models alternate."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_systems):
+        n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+        ar = int(ars[rng.integers(len(ars))])
+        phi = float(min(rng.uniform(phi_lo, phi_hi), rsa_phi_max(ar)))
+        mu = float(rng.uniform(0.0, 1.0))
+        out.append(dict(n=n, ar=ar, phi=phi, mu=mu, model=models[k % len(models)], seed=seed * 1000 + k))
+    return out
+
+
+def batch_scenes(specs, threads=None, warm="cache"):
+    """(config, scene) of every member, generated on host threads (the
+    generator releases the interpreter lock)."""
+    import concurrent.futures as cf
+    import os
+    with cf.ThreadPoolExecutor(threads or os.cpu_count() or 4) as ex:
+        return list(ex.map(lambda s: batch_member_scene(s, warm), specs))
+
+
+def batch_member_scene(spec, warm="cache"):
+    """(config, scene) of one batch member: NSC dt=5e-4, tol 1e-6, 500
+    sweeps; Hertz-Mindlin E=1e5, nu=0.3, e=0.5, dt=1e-4."""
+    d = 1.0 / spec["ar"]
+    sc = make_rods(spec["n"], 1.0, d, phi=spec["phi"], seed=spec["seed"], max_attempts=20000)
+    kw = dict(gravity=(0.0, 0.0, 0.0), lin_damp=0.0, ang_damp=0.0)
+    if spec["model"] == "nsc":
+        kw.update(model="nsc", dt=5e-4, nsc_mu=spec["mu"], nsc_omega=1.0, nsc_tol=1e-6, nsc_velocity_iters=500,
+                  nsc_warm_start=warm)
+    else:
+        kw.update(model="hertz-mindlin", dt=1e-4, hm_youngs_modulus=1e5, hm_poisson_ratio=0.3,
+                  hm_restitution=0.5, hm_friction=spec["mu"])
+    kw.update(pbc_kwargs(sc))
+    return default_config(n_bodies=sc["n"], **kw), sc

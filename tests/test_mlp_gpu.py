@@ -1,0 +1,129 @@
+"""Learned PSOR warm start on the GPU: gradients of the training kernels
+against the CPU oracle, inference, training, and what the trained network
+gains over plain PSOR (tolerance 1e-6 on the residual either way)."""
+import numpy as np
+import pytest
+
+import mlp_oracle as M
+import rodgpu
+from helpers import packed_scene
+from rodgpu import scene
+
+pytestmark = pytest.mark.gpu
+
+# Device GEMMs accumulate BF16 products in FP32 in another order than the
+# oracle (FP64), which flips an occasional BF16 rounding of an activation:
+# gradient blocks agree to 2e-2 relative L2, cosine > 0.999.
+GRAD_RTOL = 2e-2
+
+
+def _system():
+    return rodgpu.System(rodgpu.default_config(n_bodies=16, model="nsc"))
+
+
+def test_mlp_gradient_matches_oracle():
+    s = _system()
+    assert s.mlp_param_count() == M.N_PARAMS
+    x, y = M.synthetic_records(512, seed=11)
+    P = M.init_params(x, y, seed=12)
+    s.mlp_set_params(P)
+    assert np.array_equal(s.mlp_get_params(), P)
+    g, loss = s.mlp_grad(x, y)
+    loss_o, g_o = M.loss_and_grad(P, x, y, emulate_bf16=True)
+    assert abs(loss - loss_o) / loss_o < 1e-2
+    for name, lo, hi in (("W1", M.OFF_W1, M.OFF_B1), ("b1", M.OFF_B1, M.OFF_W2), ("W2", M.OFF_W2, M.OFF_B2),
+                         ("b2", M.OFF_B2, M.OFF_W3), ("W3", M.OFF_W3, M.OFF_B3), ("b3", M.OFF_B3, M.OFF_W4),
+                         ("W4", M.OFF_W4, M.OFF_B4), ("b4", M.OFF_B4, M.OFF_IN_MEAN)):
+        a, b = g[lo:hi].astype(np.float64), g_o[lo:hi]
+        err = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert err < GRAD_RTOL, (name, err)
+    cos = g.astype(np.float64) @ g_o / (np.linalg.norm(g) * np.linalg.norm(g_o))
+    assert cos > 0.999
+    assert np.all(g[M.OFF_IN_MEAN:] == 0)
+
+
+def test_mlp_inference_matches_oracle():
+    s = _system()
+    x, y = M.synthetic_records(1000, seed=13)  # not a multiple of 16 rows
+    P = M.init_params(x, y, seed=14)
+    s.mlp_set_params(P)
+    out = s.mlp_infer(x)
+    ref = M.predict(P, x, emulate_bf16=True)
+    scale = np.abs(ref).max(0)
+    assert np.max(np.abs(out - ref) / scale) < 2e-2
+
+
+def test_mlp_training_reduces_loss():
+    s = _system()
+    x, y = M.synthetic_records(8192, seed=15)
+    loss0 = s.mlp_train(x, y, epochs=1, batch=512, lr=1e-3, seed=1)
+    loss = s.mlp_train(x, y, epochs=30, batch=512, lr=1e-3, seed=1)
+    assert loss < 0.25 * loss0
+    # the trained network predicts held-out records better than "no change"
+    xt, yt = M.synthetic_records(2048, seed=16)
+    pred = s.mlp_infer(xt)
+    base = np.mean((yt - xt[:, 4:7]) ** 2)
+    assert np.mean((pred - yt) ** 2) < 0.5 * base
+
+
+def _nsc_system(sc, warm, **kw):
+    cfg = dict(gravity=(0.0, 0.0, 0.0), lin_damp=0.0, ang_damp=0.0, model="nsc", dt=5e-4, nsc_mu=0.3,
+               nsc_velocity_iters=500, nsc_tol=1e-6, nsc_warm_start=warm)
+    cfg.update(scene.pbc_kwargs(sc))
+    cfg.update(kw)
+    g = rodgpu.System(rodgpu.default_config(n_bodies=sc["n"], **cfg))
+    g.set_bodies(sc["radius"], sc["half_height"], sc["mass"], sc["inertia"], sc["restitution"])
+    g.set_state(sc["x"], sc["q"], sc["v"], sc["w"])
+    return g
+
+
+@pytest.fixture(scope="module")
+def trained():
+    """Plain PSOR (cache warm start) on a dense packing, recording its
+    converged impulses; the network trained on them; the state afterwards."""
+    sc = packed_scene(3000, d=0.05, phi=0.1, seed=21, squeeze=0.9)
+    g = _nsc_system(sc, "cache")
+    g.mlp_record(True, 1 << 21)
+    g.step(120)
+    x, y = g.mlp_records()
+    assert len(x) > 1000
+    loss = g.mlp_train(x, y, epochs=40, batch=1024, lr=1e-3, seed=3)
+    return sc, g.get_state(), g.mlp_get_params(), loss, len(x)
+
+
+def test_learned_warm_start_saves_sweeps(trained):
+    sc, st, params, loss, nrec = trained
+    sc2 = dict(sc)
+    sc2.update(x=st["x"], q=st["q"], v=st["v"], w=st["w"])
+    sweeps = {}
+    first = {}
+    for warm in ("none", "cache", "mlp"):
+        g = _nsc_system(sc2, warm)
+        if warm == "mlp":
+            g.mlp_set_params(params)
+        r = g.step(1)
+        first[warm] = g.get_state()
+        tot = r["psor_sweeps"]
+        for _ in range(4):
+            r = g.step(20)
+            assert r["not_converged"] == 0 and r["max_residual"] < 1e-6
+            tot += r["psor_sweeps"]
+        sweeps[warm] = tot
+    print("sweeps per 81 steps:", sweeps, "records:", nrec, "train loss:", loss)
+    # the network beats a cold start and does not lose to the cache
+    assert sweeps["mlp"] < sweeps["none"]
+    assert sweeps["mlp"] <= 1.05 * sweeps["cache"]
+    # PSOR runs to the same residual from any start: one step from the
+    # learned start lands as close to the cache-started step as a cold
+    # start does (velocity differences ~ tol / mass)
+    dv_mlp = np.abs(first["mlp"]["v"] - first["cache"]["v"]).max()
+    dv_cold = np.abs(first["none"]["v"] - first["cache"]["v"]).max()
+    print("max |dv| after one step vs cache start: mlp", dv_mlp, "cold", dv_cold)
+    assert dv_mlp <= 10 * max(dv_cold, 1e-6)
+
+
+def test_mlp_warm_start_requires_network():
+    sc = packed_scene(500, d=0.05, phi=0.1, seed=22, squeeze=0.9)
+    g = _nsc_system(sc, "mlp")
+    with pytest.raises(rodgpu.RgError):
+        g.step(1)
