@@ -89,6 +89,7 @@ def ref_lib():
         L.ref_get_impulses.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_size_t)]
         L.ref_threads.restype = ctypes.c_int
+        L.ref_compute_forces.argtypes = [P, dp, dp]
         _ref = L
     return _ref
 
@@ -226,6 +227,12 @@ class Reference:
         r = ctypes.c_double()
         self.L.ref_step(self._h, int(nsteps), ctypes.byref(c), ctypes.byref(r))
         return {"contacts": c.value, "residual": r.value}
+
+    def compute_forces(self):
+        f = np.zeros((self.n, 3))
+        t = np.zeros((self.n, 3))
+        self.L.ref_compute_forces(self._h, _p(f), _p(t))
+        return f, t
 
     def detect(self, delta=0.0, spatial_hash=True):
         n = ctypes.c_size_t()

@@ -307,6 +307,20 @@ int ref_get_state(const ref_system* S, double* x, double* q, double* v, double* 
   return RG_OK;
 }
 
+// Contact forces and torques at the current state (one force evaluation of
+// the Verlet models; it advances the history as a step's evaluation does).
+int ref_compute_forces(ref_system* S, double* f, double* tau) {
+  for (auto& rb : S->rods) { rb.f = glm::vec3(0); rb.tau = glm::vec3(0); }
+  force_eval(*S);
+  for (size_t i = 0; i < S->rods.size(); ++i)
+    for (int k = 0; k < 3; ++k) {
+      if (f) f[3 * i + k] = S->rods[i].f[k];
+      if (tau) tau[3 * i + k] = S->rods[i].tau[k];
+    }
+  for (auto& rb : S->rods) { rb.f = glm::vec3(0); rb.tau = glm::vec3(0); }
+  return RG_OK;
+}
+
 int ref_step(ref_system* S, int nsteps, int64_t* contacts, double* residual) {
   for (int k = 0; k < nsteps; ++k) {
     if (S->cfg.model == RG_MODEL_NSC) nsc_step(*S);

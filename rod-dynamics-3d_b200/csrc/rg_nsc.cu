@@ -1222,8 +1222,8 @@ NscView make_view(rg_system* s) {
 }
 
 int nsc_team_blocks(const rg_system* s) {
-  int nb = s->team_blocks;  // explicit team size (autotuner / tests)
-  if (nb <= 0) nb = (s->n + 1023) / 1024;
+  int nb = s->team_blocks;  // explicit team size (tests, sweeps)
+  if (nb <= 0) nb = (s->n + 127) / 128;  // about one block per 128 rods, up to every SM
   if (nb < 1) nb = 1;
   if (nb > s->coop_blocks) nb = s->coop_blocks;
   return nb;
