@@ -109,7 +109,7 @@ typedef struct rg_config {
   int32_t psor_order;            /* rg_psor_order; device supports COLORED */
 
   /* Neighbour-list broad phase (project-specific, no reference field). */
-  double skin;                   /* Verlet skin; <= 0 selects automatic      */
+  double skin;                   /* Verlet skin; <= 0: max(d/2, L/20), means */
   int32_t max_neighbors;         /* initial per-rod list capacity; <= 0 auto */
   int32_t team_blocks;           /* blocks of the persistent NSC team; 0 auto */
   int32_t reserved[6];

@@ -53,9 +53,43 @@ def build_host(force=False, verbose=False):
     return HOSTLIB
 
 
+def module_path():
+    import sysconfig
+    return os.path.join(HERE, "rod_dynamics_py" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+MODULE_SRCS = [os.path.join(HERE, "host", f) for f in ("rod_dynamics_py.cpp", "simulator.cpp", "scene_gen.cpp")]
+MODULE_HDRS = [os.path.join(HERE, "host", f) for f in ("simulator.hpp", "json_min.hpp")]
+
+
+def build_module(force=False, verbose=False):
+    """The Python module rod_dynamics_py (pybind11; C++ host code over the C
+    ABI of librodgpu.so).  Skipped when pybind11 is not importable."""
+    import sysconfig
+    try:
+        import pybind11
+    except ImportError:
+        return None
+    out = module_path()
+    deps = MODULE_SRCS + MODULE_HDRS + [LIB, os.path.join(HERE, "..", "include", "rodgpu.h")]
+    if not force and os.path.exists(out) and all(os.path.getmtime(p) <= os.path.getmtime(out) for p in deps):
+        return out
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fvisibility=hidden",
+           "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"],
+           "-o", out] + MODULE_SRCS + ["-L", HERE, "-lrodgpu", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("g++ failed building rod_dynamics_py")
+    return out
+
+
 def build(force=False, verbose=False):
     build_host(force, verbose)
     if not force and up_to_date():
+        build_module(False, verbose)
         return LIB
     cmd = [NVCC] + FLAGS + ["-o", LIB] + sources() + ["-lcudart"]
     if verbose:
@@ -64,6 +98,7 @@ def build(force=False, verbose=False):
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("nvcc failed building librodgpu.so")
+    build_module(True, verbose)
     return LIB
 
 

@@ -297,7 +297,7 @@ cudaError_t detector_alloc(rg_system* s) {
   Detector& d = s->det;
   const int n = s->n;
   const rg_config& c = s->cfg;
-  double rmax = 0, hmax = 0, dsum = 0;
+  double rmax = 0, hmax = 0, dsum = 0, lsum = 0;
   std::vector<double> r(n), h(n);
   cudaMemcpy(r.data(), s->st.r, sizeof(double) * n, cudaMemcpyDeviceToHost);
   cudaMemcpy(h.data(), s->st.h, sizeof(double) * n, cudaMemcpyDeviceToHost);
@@ -305,9 +305,12 @@ cudaError_t detector_alloc(rg_system* s) {
     rmax = r[i] > rmax ? r[i] : rmax;
     hmax = h[i] > hmax ? h[i] : hmax;
     dsum += 2 * r[i];
+    lsum += 2 * h[i];
   }
   d.margin = c.model == RG_MODEL_HARMONIC ? c.soft_delta : 0.0;
-  d.skin = c.skin > 0 ? c.skin : 0.5 * (dsum / n) + 1e-6;
+  // Default skin: half a diameter, but at least 5% of the rod length, so
+  // thin rods (whose lists stay short) rebuild rarely.
+  d.skin = c.skin > 0 ? c.skin : fmax(0.5 * (dsum / n), 0.05 * (lsum / n)) + 1e-6;
   d.cut_center = 2.0 * (hmax + rmax) + d.margin + d.skin;
   d.all_pairs = false;
   GridDev gd{};

@@ -52,10 +52,27 @@ __device__ inline void open_grid(const unsigned long long* mn, const unsigned lo
   g->ncells = total;
 }
 
+// Staged segment records in structure-of-arrays form: consecutive threads
+// read consecutive 8-byte words (no shared-memory bank conflicts; a 64-byte
+// Seg stride would serialise 16 ways).
+struct SegTile {
+  double cx[kTile], cy[kTile], cz[kTile], h[kTile], ux[kTile], uy[kTile], uz[kTile], r[kTile];
+  __device__ void put(int k, const Seg& s) {
+    cx[k] = s.cx; cy[k] = s.cy; cz[k] = s.cz; h[k] = s.h;
+    ux[k] = s.ux; uy[k] = s.uy; uz[k] = s.uz; r[k] = s.r;
+  }
+  __device__ Seg get(int k) const {
+    Seg s;
+    s.cx = cx[k]; s.cy = cy[k]; s.cz = cz[k]; s.h = h[k];
+    s.ux = ux[k]; s.uy = uy[k]; s.uz = uz[k]; s.r = r[k];
+    return s;
+  }
+};
+
 struct BuildSmem {
-  Seg tile[kTile];
+  SegTile tile;
   int tidx[kTile];
-  Seg home[kTile];
+  SegTile home;
   int hidx[kTile];
   int ncl[27];
   int nn;
@@ -85,6 +102,29 @@ __device__ inline d3 centre_offset(const Seg& A, const Seg& B, const Box& box, c
     if (box.L[2] > 0.0) d.z -= box.L[2] * rint(d.z * invL[2]);
   }
   return d;
+}
+
+// True when segments A and B (B displaced by the centre offset d) are
+// certainly farther apart than lim: two axial slabs and the axis-line
+// distance bound the segment distance from below (|q - p| >= |(q - p).u|
+// for a unit u, and (q - p).c = d.c for c = uA x uB).  FP64 with the same
+// relative slack as the centre test; the line bound is used only when the
+// axes are not near parallel, where c carries full relative precision.
+// Callers still decide with the exact narrow phase: this only skips pairs
+// whose exact distance is >= lim, so lists and contacts do not change.
+__device__ inline bool seg_far(const Seg& A, const Seg& B, d3 d, double lim) {
+  const double L = lim * (1.0 + 1e-9) + 1e-12;
+  const d3 ua{A.ux, A.uy, A.uz}, ub{B.ux, B.uy, B.uz};
+  const double cab = fabs(dot(ua, ub));
+  if (fabs(dot(d, ua)) - cab * B.h - A.h > L) return true;
+  if (fabs(dot(d, ub)) - cab * A.h - B.h > L) return true;
+  const d3 c = cross(ua, ub);
+  const double c2 = dot(c, c);
+  if (c2 > 1e-6) {
+    const double dc = dot(d, c);
+    if (dc * dc > L * L * c2) return true;
+  }
+  return false;
 }
 
 // Pair-parallel list build for one home cell (all block threads call it):
@@ -131,7 +171,7 @@ __device__ inline void build_cell_pairs(const Seg* seg, const GridDev& g, const 
     if ((int)threadIdx.x < H) {
       int i = cell_rods[h0 + threadIdx.x];
       sm.hidx[threadIdx.x] = i;
-      sm.home[threadIdx.x] = seg[i];
+      sm.home.put(threadIdx.x, seg[i]);
     }
     for (int c = 0; c < nn; ++c) {
       int ns = cell_start[sm.ncl[c]], ne = cell_start[sm.ncl[c] + 1];
@@ -141,7 +181,7 @@ __device__ inline void build_cell_pairs(const Seg* seg, const GridDev& g, const 
         if ((int)threadIdx.x < m) {
           int j = cell_rods[t0 + threadIdx.x];
           sm.tidx[threadIdx.x] = j;
-          sm.tile[threadIdx.x] = seg[j];
+          sm.tile.put(threadIdx.x, seg[j]);
         }
         __syncthreads();
         const int pairs = H * m;
@@ -150,13 +190,22 @@ __device__ inline void build_cell_pairs(const Seg* seg, const GridDev& g, const 
           const int i = sm.hidx[h], j = sm.tidx[u];
           if (j <= i) continue;
           if (!all_pairs) {
-            const Seg& A = sm.home[h];
-            const Seg& B = sm.tile[u];
-            d3 d = centre_offset(A, B, box, invL);
-            double cc = A.h + B.h + A.r + B.r + margin + skin;
+            // centre test from the staged centres only (same arithmetic as
+            // centre_offset)
+            d3 d{sm.tile.cx[u] - sm.home.cx[h], sm.tile.cy[u] - sm.home.cy[h], sm.tile.cz[u] - sm.home.cz[h]};
+            if (box.pbc) {
+              if (box.L[0] > 0.0) d.x -= box.L[0] * rint(d.x * invL[0]);
+              if (box.L[1] > 0.0) d.y -= box.L[1] * rint(d.y * invL[1]);
+              if (box.L[2] > 0.0) d.z -= box.L[2] * rint(d.z * invL[2]);
+            }
+            const double hr = sm.home.h[h] + sm.tile.h[u] + sm.home.r[h] + sm.tile.r[u];
+            double cc = hr + margin + skin;
             if (dot(d, d) > cc * cc * (1.0 + 1e-9)) continue;
-            Narrow nr = narrow_pair(A, B, box);
+            const Seg A = sm.home.get(h);
+            const Seg B = sm.tile.get(u);
             double lim = A.r + B.r + margin + skin;
+            if (seg_far(A, B, d, lim)) continue;
+            Narrow nr = narrow_pair(A, B, box);
             if (!(nr.d2 < lim * lim)) continue;
           }
           int pos = atomicAdd(&nbr_cnt[i], 1);
@@ -192,10 +241,13 @@ __device__ inline void sort_list(int* nbr, int* nbr_cnt, int maxnb, int i, int& 
 // Narrow-phase count with G lanes per rod (G divides 32): lane l tests list
 // entries l, l+G, ...; contacts set bits in the rod's mask words (zeroed by
 // lane 0 first) and the group's hit count is returned to every lane.
+// prefilter: skip list entries that seg_far proves out of reach (valid when
+// the box is not in all-pairs mode, where every other image is farther than
+// the list cut-off).
 template <int G>
 __device__ inline int narrow_count_lanes(int i, bool valid, const Seg* seg, const double* inv_mass,
                                          const Box& box, double delta, const int* nbr_cnt, const int* nbr,
-                                         int maxnb, int words, unsigned long long* mask) {
+                                         int maxnb, int words, unsigned long long* mask, bool prefilter = false) {
   const int l = threadIdx.x & (G - 1);
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (threadIdx.x & 31 & ~(G - 1)));
   int cnt = valid ? nbr_cnt[i] : 0;
@@ -207,10 +259,15 @@ __device__ inline int narrow_count_lanes(int i, bool valid, const Seg* seg, cons
     const int* list = nbr + (size_t)i * maxnb;
     Seg A = seg[i];
     bool a_static = !(inv_mass[i] > 0.0);
+    double invL[3] = {1.0, 1.0, 1.0};
+    if (prefilter)
+      for (int k = 0; k < 3; ++k)
+        if (box.L[k] > 0.0) invL[k] = 1.0 / box.L[k];
     for (int k = l; k < cnt; k += G) {
       int j = list[k];
       if (a_static && !(inv_mass[j] > 0.0)) continue;
       Seg B = seg[j];
+      if (prefilter && seg_far(A, B, centre_offset(A, B, box, invL), A.r + B.r + delta)) continue;
       Narrow nr = narrow_pair(A, B, box);
       if (contact_test(nr.d2, A.r + B.r, delta)) {
         atomicOr(&mask[(size_t)i * words + (k >> 6)], 1ull << (k & 63));

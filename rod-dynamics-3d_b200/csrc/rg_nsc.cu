@@ -255,7 +255,7 @@ __device__ __noinline__ int detect_phase(const Team& T, const NscView& V, double
     int i = base + threadIdx.x / G;
     bool valid = i < hi;
     int c = narrow_count_lanes<G>(i, valid, V.seg, V.st.inv_mass, V.box, delta, V.nbr_cnt, V.nbr, V.maxnb,
-                                  V.words, V.mask);
+                                  V.words, V.mask, !V.all_pairs);
     if (valid && (threadIdx.x & (G - 1)) == 0) {
       V.hit_cnt[i] = c;
       mine += c;

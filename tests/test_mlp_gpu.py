@@ -102,7 +102,7 @@ def test_learned_warm_start_saves_sweeps(trained):
         if warm == "mlp":
             g.mlp_set_params(params)
         r = g.step(1)
-        first[warm] = g.get_state()
+        first[warm] = (g.get_state(), r)
         tot = r["psor_sweeps"]
         for _ in range(4):
             r = g.step(20)
@@ -113,13 +113,38 @@ def test_learned_warm_start_saves_sweeps(trained):
     # the network beats a cold start and does not lose to the cache
     assert sweeps["mlp"] < sweeps["none"]
     assert sweeps["mlp"] <= 1.05 * sweeps["cache"]
-    # PSOR runs to the same residual from any start: one step from the
-    # learned start lands as close to the cache-started step as a cold
-    # start does (velocity differences ~ tol / mass)
-    dv_mlp = np.abs(first["mlp"]["v"] - first["cache"]["v"]).max()
-    dv_cold = np.abs(first["none"]["v"] - first["cache"]["v"]).max()
-    print("max |dv| after one step vs cache start: mlp", dv_mlp, "cold", dv_cold)
-    assert dv_mlp <= 10 * max(dv_cold, 1e-6)
+    # PSOR ran to the same residual from either start.  Frictional contact
+    # solutions are not unique, so velocities may differ between starts;
+    # contact impulses are internal, so linear momentum is the same, and
+    # the kinetic energy agrees to the solver's tolerance.
+    m = sc2["mass"][:, None]
+    st_ref, r_ref = first["cache"]
+    p_ref = (m * st_ref["v"]).sum(0)
+    for warm in ("mlp", "none"):
+        st, r = first[warm]
+        assert r["max_residual"] < 1e-6
+        assert np.abs((m * st["v"]).sum(0) - p_ref).max() < 1e-9 * np.abs(m * st["v"]).sum()
+        assert abs(r["kinetic_energy"] - r_ref["kinetic_energy"]) < 1e-3 * r_ref["kinetic_energy"]
+
+
+def test_zero_network_reproduces_cache_start(trained):
+    """A network whose output layer is zero predicts 'no change', so the
+    learned path must follow the cache-started path (to the rounding of the
+    friction-cone projection)."""
+    sc, st, params, loss, nrec = trained
+    sc2 = dict(sc)
+    sc2.update(x=st["x"], q=st["q"], v=st["v"], w=st["w"])
+    p0 = params.copy()
+    p0[M.OFF_W4:M.OFF_IN_MEAN] = 0.0
+    a = _nsc_system(sc2, "cache")
+    b = _nsc_system(sc2, "mlp")
+    b.mlp_set_params(p0)
+    ra = a.step(10)
+    rb = b.step(10)
+    assert ra["psor_sweeps"] == rb["psor_sweeps"]
+    sa, sb = a.get_state(), b.get_state()
+    for k in ("x", "q", "v", "w"):
+        assert np.abs(sa[k] - sb[k]).max() <= 1e-12 * max(1.0, np.abs(sa[k]).max()), k
 
 
 def test_mlp_warm_start_requires_network():
