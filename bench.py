@@ -234,13 +234,13 @@ def run_ours(args, rank, world):
     single = plain_single(rodgpu, args)
 
     plain = load_batch(rodgpu, items, "cache")
-    best_plain, _ = plain.autotune(candidates=(0, 4096, 8192), trial_steps=5)
+    best_plain, _ = plain.autotune(candidates=(0, 1024, 2048, 4096, 8192, 16384), trial_steps=10)
     res_plain = time_batch(plain, n_total, args)
     plain.close()
 
     learned = load_batch(rodgpu, items, "mlp")
     learned.set_mlp(params)
-    best, tune = learned.autotune(candidates=(0, 4096, 8192), trial_steps=5)
+    best, tune = learned.autotune(candidates=(0, 1024, 2048, 4096, 8192, 16384), trial_steps=10)
     dist = world > 1
     if dist:
         import torch.distributed as tdist
@@ -306,9 +306,21 @@ def run_single(args, rank, world):
     import rodgpu
     import torch
     dev = int(os.environ.get("LOCAL_RANK", "0"))
-    kw, sc = build_scene(args.workload, args.n, args.seed + rank)
-    n = sc["n"]
-    s = load_system(rodgpu, rodgpu.default_config(n_bodies=n, **kw), sc)
+    if args.workload.startswith("member:"):
+        # one member of the batch workload, stepped by a single block (the
+        # team the batch schedule gives a member of moderate size)
+        from rodgpu import scene
+        k = int(args.workload.split(":", 1)[1])
+        specs = [x for x in scene.batch_members(256, seed=args.seed) if x["model"] == "nsc"]
+        cfg, sc = scene.batch_member_scene(specs[k])
+        cfg.team_blocks = 1
+        kw = {"model": "nsc"}
+        n = sc["n"]
+        s = load_system(rodgpu, cfg, sc)
+    else:
+        kw, sc = build_scene(args.workload, args.n, args.seed + rank)
+        n = sc["n"]
+        s = load_system(rodgpu, rodgpu.default_config(n_bodies=n, **kw), sc)
     s.step(args.warmup)
     torch.cuda.synchronize()
     with ClockSampler(dev) as clk:

@@ -187,7 +187,7 @@ cudaError_t launch_nsc(rg_batch* b, int nteams, int grid, int nsteps, bool graph
 // members that need larger buffers.  With restore_after (autotuner trials)
 // every member is put back to its state at the start of the call and its
 // neighbour lists are rebuilt at the next step.
-int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after = false) {
+int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after = false, int warm_steps = 0) {
   for (int k = 0; k < b->n; ++k) {
     rg_system* s = b->sys[k];
     if (!s->bodies_set || !s->state_set) return bfail(b, RG_ERR_STATE, "member " + std::to_string(k) + ": set bodies and state before stepping");
@@ -225,6 +225,12 @@ int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after =
       }
     }
     if (upload(b, teams, members)) return bfail(b, RG_ERR_CUDA, "upload views");
+    if (warm_steps > 0) {  // untimed lead-in (autotuner trials)
+      cudaError_t ew = launch_nsc(b, (int)teams.size(), grid, warm_steps, false);
+      if (ew) return bfail(b, RG_ERR_CUDA, std::string("persistent launch: ") + cudaGetErrorString(ew));
+      for (int k : todo)
+        if (b->sys[k]->cfg.model != RG_MODEL_NSC) launch_steps(b->sys[k], warm_steps);
+    }
     const long long l0 = g_launches;
     cudaEventRecord(b->ev0, b->stream);
     cudaError_t e = launch_nsc(b, (int)teams.size(), grid, nsteps, full);
@@ -380,9 +386,10 @@ int rg_batch_step(rg_batch* b, int nsteps, rg_step_stats* per_system) {
 }
 
 // Times trial_steps steps for each candidate R (bodies per block; 0 = all
-// single-block teams) from the current state, puts the state back after each
-// trial and keeps the fastest R.  ms_out (optional, n_cand entries) receives
-// the trial times.
+// single-block teams) after two untimed steps (the first step after the state
+// is put back rebuilds every neighbour list, which a running batch rarely
+// does), puts the state back after each trial and keeps the fastest R.
+// ms_out (optional, n_cand entries) receives the trial times.
 int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand, int trial_steps, int* best_out,
                       double* ms_out) {
   if (!b || !candidates || n_cand <= 0 || trial_steps <= 0) return RG_ERR_ARG;
@@ -392,8 +399,8 @@ int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand, int trial_
   double best_ms = 1e300;
   for (int c = 0; c < n_cand; ++c) {
     rg_batch_set_schedule(b, candidates[c], b->use_graph);
-    int rc = batch_call(b, trial_steps, nullptr, true);  // grows buffers, builds the graph
-    if (rc == RG_OK) rc = batch_call(b, trial_steps, nullptr, true);
+    int rc = batch_call(b, trial_steps, nullptr, true, 2);  // grows buffers, builds the graph
+    if (rc == RG_OK) rc = batch_call(b, trial_steps, nullptr, true, 2);
     if (rc != RG_OK) return rc;
     const double ms = b->last_ms;
     if (ms_out) ms_out[c] = ms;

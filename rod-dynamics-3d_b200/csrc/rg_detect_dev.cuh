@@ -241,13 +241,14 @@ __device__ inline void sort_list(int* nbr, int* nbr_cnt, int maxnb, int i, int& 
 // Narrow-phase count with G lanes per rod (G divides 32): lane l tests list
 // entries l, l+G, ...; contacts set bits in the rod's mask words (zeroed by
 // lane 0 first) and the group's hit count is returned to every lane.
-// prefilter: skip list entries that seg_far proves out of reach (valid when
-// the box is not in all-pairs mode, where every other image is farther than
-// the list cut-off).
+// prefilter: skip list entries that seg_far proves out of reach.  1: the
+// centre offset uses the division-free image (valid when the box is not in
+// all-pairs mode, where any other image is farther than the list cut-off);
+// 2: the exact image of the narrow phase (valid always, costs 3 divisions).
 template <int G>
 __device__ inline int narrow_count_lanes(int i, bool valid, const Seg* seg, const double* inv_mass,
                                          const Box& box, double delta, const int* nbr_cnt, const int* nbr,
-                                         int maxnb, int words, unsigned long long* mask, bool prefilter = false) {
+                                         int maxnb, int words, unsigned long long* mask, int prefilter = 0) {
   const int l = threadIdx.x & (G - 1);
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (threadIdx.x & 31 & ~(G - 1)));
   int cnt = valid ? nbr_cnt[i] : 0;
@@ -260,14 +261,18 @@ __device__ inline int narrow_count_lanes(int i, bool valid, const Seg* seg, cons
     Seg A = seg[i];
     bool a_static = !(inv_mass[i] > 0.0);
     double invL[3] = {1.0, 1.0, 1.0};
-    if (prefilter)
+    if (prefilter == 1)
       for (int k = 0; k < 3; ++k)
         if (box.L[k] > 0.0) invL[k] = 1.0 / box.L[k];
     for (int k = l; k < cnt; k += G) {
       int j = list[k];
       if (a_static && !(inv_mass[j] > 0.0)) continue;
       Seg B = seg[j];
-      if (prefilter && seg_far(A, B, centre_offset(A, B, box, invL), A.r + B.r + delta)) continue;
+      if (prefilter == 1 && seg_far(A, B, centre_offset(A, B, box, invL), A.r + B.r + delta)) continue;
+      if (prefilter == 2) {
+        d3 xa{A.cx, A.cy, A.cz}, xb{B.cx, B.cy, B.cz};
+        if (seg_far(A, B, (xb - xa) + min_image_shift(box, xa, xb), A.r + B.r + delta)) continue;
+      }
       Narrow nr = narrow_pair(A, B, box);
       if (contact_test(nr.d2, A.r + B.r, delta)) {
         atomicOr(&mask[(size_t)i * words + (k >> 6)], 1ull << (k & 63));

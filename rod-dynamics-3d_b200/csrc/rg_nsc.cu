@@ -249,13 +249,16 @@ __device__ __noinline__ int detect_phase(const Team& T, const NscView& V, double
   const int seg = (n + T.nb - 1) / T.nb;
   const int lo = rank * seg < n ? rank * seg : n;
   const int hi = lo + seg < n ? lo + seg : n;
-  constexpr int G = 4;  // lanes per rod
+#ifndef RG_NARROW_LANES
+#define RG_NARROW_LANES 2
+#endif
+  constexpr int G = RG_NARROW_LANES;  // lanes per rod
   int mine = 0;
   for (int base = lo; base < hi; base += blockDim.x / G) {
     int i = base + threadIdx.x / G;
     bool valid = i < hi;
     int c = narrow_count_lanes<G>(i, valid, V.seg, V.st.inv_mass, V.box, delta, V.nbr_cnt, V.nbr, V.maxnb,
-                                  V.words, V.mask, !V.all_pairs);
+                                  V.words, V.mask, V.all_pairs ? 2 : 1);
     if (valid && (threadIdx.x & (G - 1)) == 0) {
       V.hit_cnt[i] = c;
       mine += c;
