@@ -310,16 +310,19 @@ int rg_batch_size(const rg_batch* b);
  * the batch's stream and is destroyed with the batch). */
 rg_system* rg_batch_member(rg_batch* b, int k);
 const char* rg_batch_last_error(const rg_batch* b);
-/* Schedule of the persistent launch: NSC members of at least 1.5 R bodies
- * get a team of round(n/R) blocks, the rest share single-block teams
- * (R = rods_per_block; 0 = all single-block).  use_graph: replay the launch
- * from a CUDA graph. */
+/* Schedule of the persistent launch: NSC members of at least 1.5 R work
+ * units get a team of round(work/R) blocks, the rest share single-block
+ * teams (R = rods_per_block; 0 = all single-block).  A member's work is its
+ * rod count until a call has timed its steps on the device, then that
+ * measured cost converted to rods at the batch's mean cost per rod.
+ * use_graph: replay the launch from a CUDA graph. */
 int rg_batch_set_schedule(rg_batch* b, int rods_per_block, int use_graph);
 int rg_batch_get_schedule(const rg_batch* b, int* rods_per_block, int* grid,
                           int* nteams);
-/* Autotuner: times trial_steps steps per candidate R from the current state
- * (state put back after each trial), selects the fastest; ms_out
- * (optional) gets n_cand times. */
+/* Autotuner: measures every member's step cost (all single-block), then
+ * times trial_steps steps per candidate R after two untimed steps, from the
+ * current state (state put back after each trial), and selects the fastest;
+ * ms_out (optional) gets n_cand times. */
 int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand,
                       int trial_steps, int* best, double* ms_out);
 

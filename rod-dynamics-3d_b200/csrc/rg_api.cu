@@ -526,6 +526,7 @@ cudaError_t reset_call_ctl(rg_system* s, const Snapshot& sn) {
   h->max_residual = 0;
   h->row_sweeps = 0;
   h->contact_steps = 0;
+  h->member_ns = 0;
   h->bar_count = 0;
   return cudaMemcpyAsync(s->d_ctl, h, s->ctl_bytes, cudaMemcpyHostToDevice, s->stream);
 }

@@ -11,12 +11,15 @@
 // CUDA graph and replayed.  Members with the Verlet models run their
 // multi-kernel step on the same stream after it.
 //
-// Schedule: members of at least 1.5 R bodies (R = bodies per block) get a
-// team of round(n/R) blocks to themselves; the rest share single-block teams,
-// assigned longest-first to the least-loaded block.  rg_batch_autotune times
-// a few R on the live systems (from a snapshot, restored afterwards) and
-// keeps the fastest.  The schedule changes time only: every member's
-// results are the same for any schedule.
+// Schedule: each member's work is its rod count until the device has timed
+// its steps (every call records each member's own step time), then that
+// measured cost in rod units.  Members of at least 1.5 R work units (R =
+// rods per block) get a team of round(work/R) blocks to themselves; the rest
+// share single-block teams, assigned longest-first to the least-loaded
+// block.  rg_batch_autotune first measures the costs, then times a few R on
+// the live systems (from a snapshot, restored afterwards) and keeps the
+// fastest.  The schedule changes time only: every member's results are the
+// same for any schedule.
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -51,6 +54,9 @@ struct rg_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
   std::string err;
+  // measured cost per member: block-milliseconds per step (0: not measured)
+  std::vector<double> cost;
+  std::vector<int> team_nb;  // blocks of the member's team in the last plan
 };
 
 namespace {
@@ -60,29 +66,42 @@ int bfail(rg_batch* b, int code, const std::string& msg) {
   return code;
 }
 
-// Team plan for the NSC members in `which` with R bodies per block.
+// Work of member k in rod units: its rod count, or, once measured, its
+// device cost converted to rods at the batch's average cost per rod (so a
+// system of thin rods or a tiny all-pairs box weighs what it costs).
+std::vector<double> work_of(const rg_batch* b, const std::vector<int>& which) {
+  double cn = 0, cc = 0;
+  for (int k : which)
+    if (b->cost[k] > 0) { cn += b->sys[k]->n; cc += b->cost[k]; }
+  std::vector<double> w(b->n, 0.0);
+  for (int k : which) w[k] = (cc > 0 && b->cost[k] > 0) ? b->cost[k] * (cn / cc) : (double)b->sys[k]->n;
+  return w;
+}
+
+// Team plan for the NSC members in `which` with R (work in rod units) per
+// block: members of at least 1.5 R get round(work / R) blocks, the rest are
+// packed longest-first onto the least-loaded single blocks.
 void plan(rg_batch* b, const std::vector<int>& which, int R, std::vector<TeamDesc>& teams,
           std::vector<int>& members, int& grid) {
   teams.clear();
   members.clear();
   const int budget = b->coop_blocks;
+  const std::vector<double> W = work_of(b, which);
   std::vector<int> big, small;
   for (int k : which) {
-    if (R > 0 && b->sys[k]->n >= (3 * R) / 2) big.push_back(k);
+    if (R > 0 && W[k] >= 1.5 * R) big.push_back(k);
     else small.push_back(k);
   }
   if ((int)big.size() > budget / 2) {  // too many large members: pack everything
     small.insert(small.end(), big.begin(), big.end());
     big.clear();
   }
-  std::sort(big.begin(), big.end(), [&](int x, int y) { return b->sys[x]->n > b->sys[y]->n; });
-  std::sort(small.begin(), small.end(), [&](int x, int y) {
-    return b->sys[x]->n != b->sys[y]->n ? b->sys[x]->n > b->sys[y]->n : x < y;
-  });
+  std::sort(big.begin(), big.end(), [&](int x, int y) { return W[x] != W[y] ? W[x] > W[y] : x < y; });
+  std::sort(small.begin(), small.end(), [&](int x, int y) { return W[x] != W[y] ? W[x] > W[y] : x < y; });
   std::vector<int> nb(big.size());
   long long want = 0;
   for (size_t i = 0; i < big.size(); ++i) {
-    nb[i] = std::max(1, (int)((b->sys[big[i]]->n + R / 2) / R));
+    nb[i] = std::max(1, (int)(W[big[i]] / R + 0.5));
     want += nb[i];
   }
   const int reserve = small.empty() ? 0 : std::min<int>((int)small.size(), std::max(1, budget / 8));
@@ -102,11 +121,11 @@ void plan(rg_batch* b, const std::vector<int>& which, int R, std::vector<TeamDes
   const int nsb = std::min<int>((int)small.size(), std::max(1, budget - b0));
   if (!small.empty()) {
     std::vector<std::vector<int>> bins(nsb);
-    std::vector<long long> load(nsb, 0);
+    std::vector<double> load(nsb, 0.0);
     for (int k : small) {
       int m = (int)(std::min_element(load.begin(), load.end()) - load.begin());
       bins[m].push_back(k);
-      load[m] += b->sys[k]->n;
+      load[m] += W[k];
     }
     for (int i = 0; i < nsb; ++i) {
       teams.push_back(TeamDesc{b0, 1, (int)members.size(), (int)bins[i].size(), nullptr});
@@ -115,6 +134,8 @@ void plan(rg_batch* b, const std::vector<int>& which, int R, std::vector<TeamDes
     }
   }
   grid = b0;
+  for (const TeamDesc& t : teams)
+    for (int m = t.first; m < t.first + t.count; ++m) b->team_nb[members[m]] = t.nb;
 }
 
 cudaError_t ensure_dev(rg_batch* b, size_t nteams, size_t nmembers) {
@@ -252,6 +273,8 @@ int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after =
       s->last_call_ms = ms;
       s->last_call_launches = launches;
       const int err = s->h_ctl->err;
+      if (!err && full && s->cfg.model == RG_MODEL_NSC && nsteps > 0 && s->h_ctl->member_ns > 0)
+        b->cost[k] = 1e-6 * (double)s->h_ctl->member_ns / nsteps * b->team_nb[k];
       if (!err) continue;
       bool retry = false;
       int rc = resolve_call(s, sn[k], err, &retry);
@@ -307,6 +330,8 @@ int rg_batch_create(const rg_config* cfgs, int n_systems, rg_batch** out) {
     ++b->n;
   }
   b->coop_blocks = b->sys[0]->coop_blocks;
+  b->cost.assign(b->n, 0.0);
+  b->team_nb.assign(b->n, 1);
   *out = b;
   return RG_OK;
 }
@@ -395,6 +420,11 @@ int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand, int trial_
   if (!b || !candidates || n_cand <= 0 || trial_steps <= 0) return RG_ERR_ARG;
   for (int c = 0; c < n_cand; ++c)
     if (candidates[c] < 0) return RG_ERR_ARG;
+  // cost model first: every member's own step time on the device, measured
+  // with all members in single-block teams
+  rg_batch_set_schedule(b, 0, b->use_graph);
+  const int rc0 = batch_call(b, trial_steps, nullptr, true, 2);
+  if (rc0 != RG_OK) return rc0;
   int best = candidates[0];
   double best_ms = 1e300;
   for (int c = 0; c < n_cand; ++c) {

@@ -40,6 +40,7 @@ struct Ctl {
   long long collisions; // NSC impacts of the last step
   double jn_sum, jt_sum, pe;
   long long row_sweeps; // Σ contacts x sweeps (cumulative)
+  long long member_ns;  // device time of this system's steps in the call (batch cost model)
   long long contact_steps;  // Σ velocity-solve contacts over steps
   int vel_contacts;     // NSC: contacts of the last velocity solve (lastHitCount)
   int prof_phases;      // 1: the persistent step records phase times

@@ -1179,7 +1179,10 @@ __global__ void __launch_bounds__(kBlock, 1) k_nsc_run(const NscView* views, con
     for (int m = td.first; m < td.first + td.count; ++m) {
       const NscView& V = views[members ? members[m] : m];
       Team T{td.b0, td.nb, td.bar, &V.ctl->err};
+      const bool timer = threadIdx.x == 0 && (int)blockIdx.x == td.b0;
+      const unsigned long long t0 = timer ? gtimer() : 0ull;
       any |= nsc_step(T, V, sm, S);
+      if (timer) V.ctl->member_ns += (long long)(gtimer() - t0);  // one writer per system
     }
     if (!any) break;
   }
