@@ -354,6 +354,11 @@ cudaError_t detector_alloc(rg_system* s) {
   if ((e = cudaMalloc(&d.hit_off, sizeof(int) * (n + 1)))) return e;
   if ((e = cudaMalloc(&d.hit_mask, sizeof(unsigned long long) * (size_t)n * d.mask_words))) return e;
   if ((e = cudaMemset(d.nbr_cnt, 0, sizeof(int) * n))) return e;
+  if (c.model == RG_MODEL_NSC) {
+    d.near_skin = 0.2 * d.skin;
+    if ((e = cudaMalloc(&d.near, sizeof(int2) * (size_t)n * d.maxnb))) return e;
+    if ((e = cudaMalloc(&d.ref2, sizeof(double) * 6 * (size_t)n))) return e;
+  }
   DetDev hd{};
   hd.grid = gd;
   hd.n = n;
@@ -366,6 +371,7 @@ void detector_free(rg_system* s) {
   cudaFree(d.nbr_cnt); cudaFree(d.nbr); cudaFree(d.ref); cudaFree(d.seg);
   cudaFree(d.cell_of); cudaFree(d.cell_cnt); cudaFree(d.cell_start); cudaFree(d.cell_fill);
   cudaFree(d.cell_rods); cudaFree(d.hit_cnt); cudaFree(d.hit_off); cudaFree(d.hit_mask);
+  cudaFree(d.near); cudaFree(d.ref2);
   d = Detector();
 }
 

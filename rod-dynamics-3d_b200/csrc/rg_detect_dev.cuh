@@ -320,6 +320,70 @@ __device__ inline int narrow_count_rod(int i, const Seg* seg, const double* inv_
   return hits;
 }
 
+// Centre offset B - A for seg_far: division-free image (mode 1, valid when
+// the box is not in all-pairs mode) or the narrow phase's exact image (2).
+__device__ inline d3 prefilter_offset(const Seg& A, const Seg& B, const Box& box, const double* invL, int mode) {
+  if (mode == 1) return centre_offset(A, B, box, invL);
+  d3 xa{A.cx, A.cy, A.cz}, xb{B.cx, B.cy, B.cz};
+  return (xb - xa) + min_image_shift(box, xa, xb);
+}
+
+// Near-list count with G lanes per rod: list entries that seg_far cannot
+// place beyond r_a + r_b + extra set their bit in the rod's mask words; the
+// group's count is returned to every lane.
+template <int G>
+__device__ inline int near_count_lanes(int i, bool valid, const Seg* seg, const double* inv_mass, const Box& box,
+                                       const double* invL, int mode, double extra, const int* nbr_cnt,
+                                       const int* nbr, int maxnb, int words, unsigned long long* mask) {
+  const int l = threadIdx.x & (G - 1);
+  int cnt = valid ? nbr_cnt[i] : 0;
+  if (valid && l == 0)
+    for (int w = 0; w < words && w * 64 < cnt; ++w) mask[(size_t)i * words + w] = 0ull;
+  __syncwarp();
+  int hits = 0;
+  if (valid) {
+    const int* list = nbr + (size_t)i * maxnb;
+    const Seg A = seg[i];
+    const bool a_static = !(inv_mass[i] > 0.0);
+    for (int k = l; k < cnt; k += G) {
+      const int j = list[k];
+      if (a_static && !(inv_mass[j] > 0.0)) continue;
+      const Seg B = seg[j];
+      if (seg_far(A, B, prefilter_offset(A, B, box, invL, mode), A.r + B.r + extra)) continue;
+      atomicOr(&mask[(size_t)i * words + (k >> 6)], 1ull << (k & 63));
+      ++hits;
+    }
+  }
+#pragma unroll
+  for (int o = 1; o < G; o <<= 1) hits += __shfl_xor_sync(0xffffffffu, hits, o);
+  return hits;
+}
+
+// Writes rod i's marked list entries as (i, j) pairs from slot o on.
+__device__ inline void near_write_rod(int i, int o, const int* nbr_cnt, const int* nbr, int maxnb, int words,
+                                      const unsigned long long* mask, int2* out) {
+  const int cnt = nbr_cnt[i];
+  const int* list = nbr + (size_t)i * maxnb;
+  for (int k = 0; k < cnt; ++k)
+    if ((mask[(size_t)i * words + (k >> 6)] >> (k & 63)) & 1ull) out[o++] = make_int2(i, list[k]);
+}
+
+// Contact record o of pair (i, j) from its narrow-phase result.
+__device__ inline void write_contact(const Contacts& con, int o, int i, int j, double rsum, const Narrow& nr) {
+  double dist = sqrt(nr.d2);
+  d3 diff = nr.pb - nr.pa;
+  d3 nv = dist > 1e-10 ? diff / dist : mk3(1, 0, 0);
+  con.a[o] = i;
+  con.b[o] = j;
+  con.type[o] = contact_type(nr.s, nr.t);
+  con.comp(0)[o] = nr.pa.x; con.comp(1)[o] = nr.pa.y; con.comp(2)[o] = nr.pa.z;
+  con.comp(3)[o] = nr.pb.x; con.comp(4)[o] = nr.pb.y; con.comp(5)[o] = nr.pb.z;
+  con.comp(6)[o] = nv.x; con.comp(7)[o] = nv.y; con.comp(8)[o] = nv.z;
+  con.comp(9)[o] = nr.sh.x; con.comp(10)[o] = nr.sh.y; con.comp(11)[o] = nr.sh.z;
+  con.comp(12)[o] = dist;
+  con.comp(13)[o] = rsum;
+}
+
 // Writes the contacts of rod i (in list order: ascending b) from slot o on.
 __device__ inline void narrow_write_rod(int i, int o, const Seg* seg, const Box& box, const int* nbr_cnt,
                                         const int* nbr, int maxnb, int words,

@@ -31,6 +31,9 @@ struct Ctl {
   int proj_active;      // projection rows active in the current pass
   int sweeps_last;      // PSOR sweeps of the last solve
   double maxdisp;       // max displacement since the last list build
+  double near_disp;     // max displacement since the last near-list build
+  int near_valid;       // 1: the near list matches the current lists
+  int near_n;           // pairs in the near list
   double residual;      // last PSOR residual
   long long frame;      // force-evaluation counter (HM / Cundall frames)
   long long rebuilds;   // list rebuilds (cumulative)
@@ -71,6 +74,11 @@ struct Detector {
   double cell[3] = {1, 1, 1};
   int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr,
       *cell_rods = nullptr;
+  // near list (persistent NSC step): the list entries within the contact
+  // reach plus near_skin, as sorted (i, j) pairs, and the segments at its build
+  int2* near = nullptr;           // n * maxnb
+  double* ref2 = nullptr;         // 6n
+  double near_skin = 0;
   int* hit_cnt = nullptr;         // n+1
   int* hit_off = nullptr;         // n+1
   unsigned long long* hit_mask = nullptr;  // n * words

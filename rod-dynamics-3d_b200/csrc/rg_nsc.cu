@@ -29,6 +29,10 @@
 
 namespace rg {
 
+#ifndef RG_NARROW_LANES
+#define RG_NARROW_LANES 2  // lanes per rod in the narrow phase over the lists
+#endif
+
 GridDev* detector_grid(rg_system* s);
 unsigned long long* detector_bounds(rg_system* s);
 MlpDev mlp_dev(rg_system* s);
@@ -239,6 +243,116 @@ __device__ __noinline__ bool rebuild_phase(const Team& T, const NscView& V, Smem
 // Contacts at the current segment records (V.seg current, ctl->maxdisp
 // accumulated by the caller, all blocks past a team barrier).  Returns the
 // contact count, or -1 on error.
+// Two-level lists: the near list holds the list entries within the contact
+// reach (r_a + r_b + margin) plus near_skin, rebuilt from the lists when a
+// rod has moved near_skin/2 since its build (or the lists were rebuilt).  A
+// pair outside it was at least near_skin beyond contact at the build, and
+// each rod has since moved less than near_skin/2 (|dx| + h|du| bounds every
+// point of a segment), so it cannot touch: the contact set found from the
+// near list is the exact one.  Contacts come out in near-list order, which
+// is (a, b) order.
+__device__ __noinline__ int detect_near(const Team& T, const NscView& V, double delta, SmemNsc& sm,
+                                        bool lists_rebuilt) {
+  Ctl* ctl = V.ctl;
+  const int n = V.st.n;
+  const int rank = T.rank();
+  const int mode = V.all_pairs ? 2 : 1;
+  double invL[3] = {1.0, 1.0, 1.0};
+  for (int k = 0; k < 3; ++k)
+    if (V.box.L[k] > 0.0) invL[k] = 1.0 / V.box.L[k];
+  const bool rebuild_near = lists_rebuilt || !*(volatile int*)&ctl->near_valid ||
+                            *(volatile double*)&ctl->near_disp >= 0.5 * V.near_skin * (1.0 - 1e-9);
+  int prefix, total;
+  if (rebuild_near) {
+    const int seg = (n + T.nb - 1) / T.nb;
+    const int lo = rank * seg < n ? rank * seg : n;
+    const int hi = lo + seg < n ? lo + seg : n;
+    constexpr int G = RG_NARROW_LANES;
+    int mine = 0;
+    for (int base = lo; base < hi; base += blockDim.x / G) {
+      const int i = base + threadIdx.x / G;
+      const bool valid = i < hi;
+      const int c = near_count_lanes<G>(i, valid, V.seg, V.st.inv_mass, V.box, invL, mode, V.margin + V.near_skin,
+                                        V.nbr_cnt, V.nbr, V.maxnb, V.words, V.mask);
+      if (valid && (threadIdx.x & (G - 1)) == 0) {
+        V.hit_cnt[i] = c;
+        mine += c;
+      }
+    }
+    const int bsum = block_reduce_sum_i(mine, sm.red_i);
+    if (threadIdx.x == 0) V.blk[rank] = bsum;
+    if (!team_sync(T)) return -1;
+    if (rank == 0 && threadIdx.x == 0) ctl->near_disp = 0.0;  // every block has read it
+    block_prefix(V.blk, T.nb, rank, prefix, total, sm);
+    int run = prefix;
+    for (int base = lo; base < hi; base += blockDim.x) {
+      const int i = base + threadIdx.x;
+      const int c = i < hi ? V.hit_cnt[i] : 0;
+      int tot;
+      const int ex = block_excl_scan(c, sm.scan_w, tot);
+      if (i < hi) {
+        if (c) near_write_rod(i, run + ex, V.nbr_cnt, V.nbr, V.maxnb, V.words, V.mask, V.near);
+        const Seg s = V.seg[i];
+        V.ref2[i] = s.cx; V.ref2[n + i] = s.cy; V.ref2[2 * n + i] = s.cz;
+        V.ref2[3 * n + i] = s.ux; V.ref2[4 * n + i] = s.uy; V.ref2[5 * n + i] = s.uz;
+      }
+      run += tot;
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+      ctl->near_n = total;
+      ctl->near_valid = 1;
+    }
+    if (!team_sync(T)) return -1;
+  }
+  // exact narrow phase over the near list: each block a 64-aligned range
+  const int P = *(volatile int*)&ctl->near_n;
+  const int segp = (((P + T.nb - 1) / T.nb) + 63) & ~63;
+  const int plo = rank * segp < P ? rank * segp : P;
+  const int phi = plo + segp < P ? plo + segp : P;
+  unsigned long long* bits = V.mask;  // one bit per near pair
+  for (int w = (plo >> 6) + threadIdx.x; w < ((phi + 63) >> 6); w += blockDim.x) bits[w] = 0ull;
+  __syncthreads();
+  const double* im = V.st.inv_mass;
+  int mine = 0;
+  for (int p = plo + threadIdx.x; p < phi; p += blockDim.x) {
+    const int2 pr = V.near[p];
+    if (!(im[pr.x] > 0.0) && !(im[pr.y] > 0.0)) continue;
+    const Seg A = V.seg[pr.x], B = V.seg[pr.y];
+    if (seg_far(A, B, prefilter_offset(A, B, V.box, invL, mode), A.r + B.r + delta)) continue;
+    const Narrow nr = narrow_pair(A, B, V.box);
+    if (contact_test(nr.d2, A.r + B.r, delta)) {
+      atomicOr(&bits[p >> 6], 1ull << (p & 63));
+      ++mine;
+    }
+  }
+  const int bsum = block_reduce_sum_i(mine, sm.red_i);
+  if (threadIdx.x == 0) V.blk[rank] = bsum;
+  if (!team_sync(T)) return -1;
+  if (rank == 0 && threadIdx.x == 0) ctl->maxdisp = 0.0;  // every block has read it
+  block_prefix(V.blk, T.nb, rank, prefix, total, sm);
+  if (total > V.ccap) {
+    if (rank == 0 && threadIdx.x == 0) atomicOr(&ctl->err, ERR_CONTACT_CAP);
+    return -1;
+  }
+  int run = prefix;
+  for (int base = plo; base < phi; base += blockDim.x) {
+    const int p = base + threadIdx.x;
+    const int f = (p < phi && ((bits[p >> 6] >> (p & 63)) & 1ull)) ? 1 : 0;
+    int tot;
+    const int ex = block_excl_scan(f, sm.scan_w, tot);
+    if (f) {
+      const int2 pr = V.near[p];
+      const Seg A = V.seg[pr.x], B = V.seg[pr.y];
+      const Narrow nr = narrow_pair(A, B, V.box);
+      write_contact(V.con, run + ex, pr.x, pr.y, A.r + B.r, nr);
+    }
+    run += tot;
+  }
+  if (rank == 0 && threadIdx.x == 0) ctl->contacts = total;
+  if (!team_sync(T)) return -1;
+  return total;
+}
+
 __device__ __noinline__ int detect_phase(const Team& T, const NscView& V, double delta, SmemNsc& sm) {
   Ctl* ctl = V.ctl;
   const int n = V.st.n;
@@ -246,12 +360,10 @@ __device__ __noinline__ int detect_phase(const Team& T, const NscView& V, double
   const bool need = *(volatile int*)&ctl->rebuild ||
                     (!V.all_pairs && *(volatile double*)&ctl->maxdisp >= 0.5 * V.skin * (1.0 - 1e-9));
   if (need && !rebuild_phase(T, V, sm)) return -1;
+  if (V.near) return detect_near(T, V, delta, sm, need);
   const int seg = (n + T.nb - 1) / T.nb;
   const int lo = rank * seg < n ? rank * seg : n;
   const int hi = lo + seg < n ? lo + seg : n;
-#ifndef RG_NARROW_LANES
-#define RG_NARROW_LANES 2
-#endif
   constexpr int G = RG_NARROW_LANES;  // lanes per rod
   int mine = 0;
   for (int base = lo; base < hi; base += blockDim.x / G) {
@@ -999,15 +1111,20 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
   // 1) free flight (main.cpp:4397-4408) + segment records + displacement
   {
     const d3 g{cfg.gravity[0], cfg.gravity[1], cfg.gravity[2]};
-    double dmax = 0.0;
+    double dmax = 0.0, dnear = 0.0;
     for (int i = tid; i < n; i += TS) {
       nsc_free_flight_body(st, i, g, cfg.dt);
       Seg s = make_seg(st, i);
       V.seg[i] = s;
       dmax = fmax(dmax, seg_disp(s, V.ref, n, i, V.box));
+      if (V.near) dnear = fmax(dnear, seg_disp(s, V.ref2, n, i, V.box));
     }
     double bm = block_reduce_max(dmax, sm.red_d);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
+    if (V.near) {
+      double bn = block_reduce_max(dnear, sm.red_d);
+      if (threadIdx.x == 0) atomic_max_nonneg(&ctl->near_disp, bn);
+    }
     if (!team_sync(T)) return false;
   }
   pc.mark(0);
@@ -1114,16 +1231,21 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
       }
     }
     int bad = 0;
-    double dmax = 0.0;
+    double dmax = 0.0, dnear = 0.0;
     for (int i = tid; i < n; i += TS) {
       bad |= nsc_position_update_body(st, i, cfg);
       Seg s = make_seg(st, i);
       V.seg[i] = s;
       dmax = fmax(dmax, seg_disp(s, V.ref, n, i, V.box));
+      if (V.near) dnear = fmax(dnear, seg_disp(s, V.ref2, n, i, V.box));
     }
     if (bad) atomicOr(&ctl->err, ERR_NONFINITE);
     double bm = block_reduce_max(dmax, sm.red_d);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
+    if (V.near) {
+      double bn = block_reduce_max(dnear, sm.red_d);
+      if (threadIdx.x == 0) atomic_max_nonneg(&ctl->near_disp, bn);
+    }
     if (!team_sync(T)) return false;
     // every block has read rec_n before the barrier
     if (V.rec_cap > 0 && !small && C > 0 && tid == 0) ctl->rec_n = rec_base + C;
@@ -1216,6 +1338,9 @@ NscView make_view(rg_system* s) {
   V.ccap = s->ccap;
   V.blk = N.blk;
   V.slot_of = N.slot_of;
+  V.near = d.near;
+  V.ref2 = d.ref2;
+  V.near_skin = d.near_skin;
   V.feat = s->d_feat;
   V.pred = s->d_pred;
   V.use_mlp = (s->cfg.nsc_warm_start == RG_WARM_MLP && s->mlp_ready) ? 1 : 0;

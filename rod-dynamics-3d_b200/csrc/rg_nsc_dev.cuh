@@ -313,6 +313,9 @@ struct NscView {
   int ccap;
   int* blk;      // per-block scratch of the team
   int* slot_of;  // per-body local slot of the in-block solver (-1 when unused)
+  int2* near;    // near list (see Detector); null: test the whole lists
+  double* ref2;
+  double near_skin;
   // learned warm start: features [8][ccap] and predictions [3][ccap] of the
   // team path, the network, and the record buffers ([n][8], [n][3])
   float *feat, *pred;
