@@ -75,7 +75,9 @@ typedef enum rg_psor_order {
 typedef enum rg_warm_start {
   RG_WARM_CACHE = 0,     /* previous-step impulses by pair (nsc_contact.cpp:305-317) */
   RG_WARM_NONE = 1,      /* cold start                                       */
-  RG_WARM_MLP = 2        /* learned warm start from rg_mlp weights           */
+  RG_WARM_MLP = 2        /* learned warm start from rg_mlp weights (for the
+                            contacts nsc_mlp_scope selects; the others start
+                            from the cache)                                  */
 } rg_warm_start;
 
 /* Configuration.  Field meanings and defaults follow AppCfg
@@ -112,7 +114,14 @@ typedef struct rg_config {
   double skin;                   /* Verlet skin; <= 0: max(d/2, L/20), means */
   int32_t max_neighbors;         /* initial per-rod list capacity; <= 0 auto */
   int32_t team_blocks;           /* blocks of the persistent NSC team; 0 auto */
-  int32_t reserved[6];
+  int32_t nsc_mlp_scope;         /* learned start for: 0 contacts new since
+                                    the last step (not in the warm cache),
+                                    1 every contact                          */
+  int32_t nsc_mlp_min_sweeps;    /* ... in a step only when the previous one
+                                    needed more PSOR sweeps than this, or the
+                                    warm cache is empty (default 3; -1: in
+                                    every step)                              */
+  int32_t reserved[4];
 } rg_config;
 
 /* Per-call statistics (the profile-CSV columns of main.cpp:3276-3355). */

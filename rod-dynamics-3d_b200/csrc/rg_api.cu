@@ -265,6 +265,7 @@ void rg_config_default(rg_config* c) {
   c->nsc_mu = 0.3; c->nsc_beta = 0.2; c->nsc_cfm = 0.0; c->nsc_omega = 1.0; c->nsc_slop = 1e-4;
   c->nsc_tol = 1e-6; c->nsc_velocity_iters = 40; c->nsc_position_stabilization = 1;
   c->nsc_position_iters = 5; c->nsc_position_psor_iters = 50; c->nsc_warm_start = RG_WARM_CACHE;
+  c->nsc_mlp_scope = 0; c->nsc_mlp_min_sweeps = 3;
   c->psor_order = RG_ORDER_COLORED;
   c->skin = 0.0; c->max_neighbors = 0;
 }

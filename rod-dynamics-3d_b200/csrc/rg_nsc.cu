@@ -728,6 +728,7 @@ struct SmallSmem {
   double red[32];
   float feat[kMlpIn * kSmallC];      // learned warm start features [8][kSmallC]
   float pred[kMlpOut * kSmallC];     // predicted impulse changes [3][kSmallC]
+  int mtile[kSmallC / 16];           // 16-contact tiles that need the network
 };
 
 __device__ inline double small_block_max(double v, SmallSmem& S) {
@@ -738,6 +739,15 @@ __device__ inline double small_block_max(double v, SmallSmem& S) {
   double r = 0.0;
   for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, S.red[w]);
   return r;  // every thread
+}
+
+// True when contact c has an entry in the warm cache of the previous step
+// (W entries): the learned start by default serves only the others.
+__device__ inline bool warm_cached(const NscView& V, int c, int W) {
+  if (W <= 0) return false;
+  const unsigned long long k = ((unsigned long long)(unsigned)V.con.a[c] << 32) | (unsigned)V.con.b[c];
+  const int q = lower_bound_key(V.wkey, W, k);
+  return q < W && V.wkey[q] == k;
 }
 
 // Local slots for the bodies of contacts 0..C-1 (C <= blockDim).
@@ -889,13 +899,21 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
       S.feat[7 * kSmallC + t] = (float)((S.dyn[sa] ? deg[sa] - 1 : 0) + (S.dyn[sb] ? deg[sb] - 1 : 0));
     }
     __syncthreads();
-    if (V.use_mlp) {
-      // one warp per 16 contacts on the tensor cores, then the cone
-      const int row0 = (t >> 5) * 16;
-      if (row0 < C) mlp_warp(V.mlp, S.feat, kSmallC, row0, C, S.pred, t & 31);
+    if (V.use_mlp && (W == 0 || *(volatile int*)&ctl->sweeps_last > V.mlp_min_sweeps)) {
+      // the contacts the learned start is for (every contact, or those new
+      // since the last step); the network runs only on tiles that hold one
+      const bool want = t < C && (V.mlp_all || !warm_cached(V, S.order[t], W));
+      if (t < kSmallC / 16) S.mtile[t] = 0;
       __syncthreads();
-      if (t < C) mlp_apply(R, S.pred, kSmallC, t, cfg.nsc_mu);
-      __syncthreads();
+      if (want) S.mtile[t >> 4] = 1;
+      if (__syncthreads_or(want)) {
+        // one warp per 16 contacts on the tensor cores, then the cone
+        const int row0 = (t >> 5) * 16;
+        if (row0 < C && S.mtile[t >> 5]) mlp_warp(V.mlp, S.feat, kSmallC, row0, C, S.pred, t & 31);
+        __syncthreads();
+        if (want) mlp_apply(R, S.pred, kSmallC, t, cfg.nsc_mu);
+        __syncthreads();
+      }
     }
   }
   pc.mark(3);
@@ -1112,13 +1130,12 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
   {
     const d3 g{cfg.gravity[0], cfg.gravity[1], cfg.gravity[2]};
     double dmax = 0.0, dnear = 0.0;
-    for (int i = tid; i < n; i += TS) {
-      nsc_free_flight_body(st, i, g, cfg.dt);
-      Seg s = make_seg(st, i);
-      V.seg[i] = s;
-      dmax = fmax(dmax, seg_disp(s, V.ref, n, i, V.box));
-      if (V.near) dnear = fmax(dnear, seg_disp(s, V.ref2, n, i, V.box));
-    }
+    const double* ref2 = V.near ? V.ref2 : nullptr;
+    double invL[3] = {1.0, 1.0, 1.0};
+    for (int k = 0; k < 3; ++k)
+      if (V.box.L[k] > 0.0) invL[k] = 1.0 / V.box.L[k];
+    for (int i = tid; i < n; i += TS)
+      free_flight_fused(st, i, g, cfg.dt, V.ref, ref2, n, V.box, invL, V.seg, dmax, dnear);
     double bm = block_reduce_max(dmax, sm.red_d);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
     if (V.near) {
@@ -1174,16 +1191,19 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
         const int c = V.order[p], a = V.con.a[c], b = V.con.b[c];
         V.feat[7 * (size_t)V.ccap + p] = (float)((im[a] > 0.0 ? deg[a] - 1 : 0) + (im[b] > 0.0 ? deg[b] - 1 : 0));
       }
-      if (V.use_mlp) {
+      if (V.use_mlp && (W == 0 || *(volatile int*)&ctl->sweeps_last > V.mlp_min_sweeps)) {
         // each warp of the team evaluates tiles of 16 slots on the tensor
         // cores; its own lanes then apply the tile's predictions
         __syncthreads();
         if (!team_sync(T)) return false;
         const int lane = threadIdx.x & 31, gw = tid >> 5, nw = TS >> 5;
         for (int row0 = gw * 16; row0 < C; row0 += nw * 16) {
+          const int p = row0 + (lane & 15);
+          const bool want = lane < 16 && p < C && (V.mlp_all || !warm_cached(V, V.order[p], W));
+          if (!__ballot_sync(0xffffffffu, want)) continue;  // no row of this tile needs the network
           mlp_warp(V.mlp, V.feat, V.ccap, row0, C, V.pred, lane);
           __syncwarp();
-          if (lane < 16 && row0 + lane < C) mlp_apply(R, V.pred, V.ccap, row0 + lane, cfg.nsc_mu);
+          if (want) mlp_apply(R, V.pred, V.ccap, p, cfg.nsc_mu);
           __syncwarp();
         }
       }
@@ -1232,13 +1252,12 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     }
     int bad = 0;
     double dmax = 0.0, dnear = 0.0;
-    for (int i = tid; i < n; i += TS) {
-      bad |= nsc_position_update_body(st, i, cfg);
-      Seg s = make_seg(st, i);
-      V.seg[i] = s;
-      dmax = fmax(dmax, seg_disp(s, V.ref, n, i, V.box));
-      if (V.near) dnear = fmax(dnear, seg_disp(s, V.ref2, n, i, V.box));
-    }
+    const double* ref2 = V.near ? V.ref2 : nullptr;
+    double invL[3] = {1.0, 1.0, 1.0};
+    for (int k = 0; k < 3; ++k)
+      if (V.box.L[k] > 0.0) invL[k] = 1.0 / V.box.L[k];
+    for (int i = tid; i < n; i += TS)
+      bad |= position_update_fused(st, i, cfg, V.ref, ref2, n, V.box, invL, V.seg, dmax, dnear);
     if (bad) atomicOr(&ctl->err, ERR_NONFINITE);
     double bm = block_reduce_max(dmax, sm.red_d);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
@@ -1344,6 +1363,8 @@ NscView make_view(rg_system* s) {
   V.feat = s->d_feat;
   V.pred = s->d_pred;
   V.use_mlp = (s->cfg.nsc_warm_start == RG_WARM_MLP && s->mlp_ready) ? 1 : 0;
+  V.mlp_all = s->cfg.nsc_mlp_scope == 1 ? 1 : 0;
+  V.mlp_min_sweeps = s->cfg.nsc_mlp_min_sweeps;
   V.rec_cap = s->recording ? s->rec_cap : 0;
   V.rec_x = s->d_rec_x;
   V.rec_y = s->d_rec_y;

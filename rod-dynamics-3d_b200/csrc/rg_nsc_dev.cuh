@@ -256,6 +256,98 @@ __device__ inline int nsc_position_update_body(const State& st, int i, const rg_
   return (x.x == x.x && x.y == x.y && x.z == x.z && v.x == v.x) ? 0 : 1;
 }
 
+// |dx| + h|du| of a segment against reference centre/axis values already in
+// registers.  The periodic image is taken with a multiplication by 1/L: it
+// can differ from the division-based image only when |dx| is within rounding
+// of L/2, where either image's displacement is far beyond any skin and
+// triggers the rebuild all the same.
+__device__ inline double disp_from(const Seg& s, const double* rf, const Box& box, const double* invL) {
+  d3 dx{s.cx - rf[0], s.cy - rf[1], s.cz - rf[2]};
+  if (box.pbc) {
+    if (box.L[0] > 0.0) dx.x -= box.L[0] * rint(dx.x * invL[0]);
+    if (box.L[1] > 0.0) dx.y -= box.L[1] * rint(dx.y * invL[1]);
+    if (box.L[2] > 0.0) dx.z -= box.L[2] * rint(dx.z * invL[2]);
+  }
+  d3 du{s.ux - rf[3], s.uy - rf[4], s.uz - rf[5]};
+  double d = len(dx) + s.h * len(du);
+  return (d == d) ? d : 1e300;
+}
+
+__device__ inline Seg seg_of(d3 x, dq q, double h, double r) {
+  d3 u = axis_y(q);
+  Seg s;
+  s.cx = x.x; s.cy = x.y; s.cz = x.z; s.h = h;
+  s.ux = u.x; s.uy = u.y; s.uz = u.z; s.r = r;
+  return s;
+}
+
+// Free flight of rod i (nsc_free_flight_body), its segment record and the
+// displacement bounds against ref (and ref2 when given), with every input
+// loaded before the first store: one round trip to memory per rod instead
+// of three.  Same arithmetic as the separate functions.
+__device__ inline void free_flight_fused(const State& st, int i, d3 g, double dt, const double* ref,
+                                         const double* ref2, int n, const Box& box, const double* invL,
+                                         Seg* seg_out, double& dmax, double& dnear) {
+  const double im = st.inv_mass[i];
+  const dq q = st.q.ld(i);
+  d3 w = st.w.ld(i);
+  d3 v = st.v.ld(i);
+  const d3 f = st.f.ld(i), tau = st.tau.ld(i), I = st.I.ld(i), Iinv = st.Iinv.ld(i);
+  const d3 x = st.x.ld(i);
+  const double h = st.h[i], r = st.r[i];
+  double rf[6], rf2[6];
+  for (int k = 0; k < 6; ++k) rf[k] = ref[(size_t)k * n + i];
+  if (ref2)
+    for (int k = 0; k < 6; ++k) rf2[k] = ref2[(size_t)k * n + i];
+  if (im > 0) {
+    v = v + (f * im + g) * dt;
+    d3 Iw_w = rot_diag_apply(q, I, w);
+    d3 gyro = cross(w, Iw_w);
+    w = w + rot_diag_apply(q, Iinv, tau - gyro) * dt;
+    st.v.st(i, v);
+    st.w.st(i, w);
+  }
+  const Seg s = seg_of(x, q, h, r);
+  seg_out[i] = s;
+  dmax = fmax(dmax, disp_from(s, rf, box, invL));
+  if (ref2) dnear = fmax(dnear, disp_from(s, rf2, box, invL));
+}
+
+// Position update of rod i (nsc_position_update_body) fused the same way;
+// returns 1 when the new state is not finite.
+__device__ inline int position_update_fused(const State& st, int i, const rg_config& cfg, const double* ref,
+                                            const double* ref2, int n, const Box& box, const double* invL,
+                                            Seg* seg_out, double& dmax, double& dnear) {
+  const double dt = cfg.dt;
+  const double ld = 1.0 - cfg.lin_damp * dt, ad = 1.0 - cfg.ang_damp * dt;
+  d3 v = st.v.ld(i), w = st.w.ld(i);
+  d3 x = st.x.ld(i);
+  dq q = st.q.ld(i);
+  const double h = st.h[i], r = st.r[i];
+  double rf[6], rf2[6];
+  for (int k = 0; k < 6; ++k) rf[k] = ref[(size_t)k * n + i];
+  if (ref2)
+    for (int k = 0; k < 6; ++k) rf2[k] = ref2[(size_t)k * n + i];
+  x = x + v * dt;
+  d3 hw = w * (0.5 * dt);
+  dq wq{0.0, hw.x, hw.y, hw.z};
+  dq d = qmul(wq, q);
+  q = qnormalize(dq{q.w + d.w, q.x + d.x, q.y + d.y, q.z + d.z});
+  v = v * ld;
+  w = w * ad;
+  double wl = len(w);
+  if (wl > cfg.w_max) w = w * (cfg.w_max / wl);
+  st.x.st(i, x);
+  st.q.st(i, q);
+  st.v.st(i, v);
+  st.w.st(i, w);
+  const Seg s = seg_of(x, q, h, r);
+  seg_out[i] = s;
+  dmax = fmax(dmax, disp_from(s, rf, box, invL));
+  if (ref2) dnear = fmax(dnear, disp_from(s, rf2, box, invL));
+  return (x.x == x.x && x.y == x.y && x.z == x.z && v.x == v.x) ? 0 : 1;
+}
+
 __device__ inline void wrap_pos(const Box& box, d3& p) {
   if (!box.pbc) return;
   double* c[3] = {&p.x, &p.y, &p.z};
@@ -321,6 +413,8 @@ struct NscView {
   float *feat, *pred;
   int feat_on;   // features needed (learned warm start or recording)
   int use_mlp;   // warm start from the network
+  int mlp_min_sweeps;  // ... in steps after one that needed more sweeps than this
+  int mlp_all;   // ... for every contact (else only where the cache gives zero)
   MlpDev mlp;
   float *rec_x, *rec_y;
   int rec_cap;   // 0: not recording

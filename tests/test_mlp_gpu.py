@@ -67,8 +67,9 @@ def test_mlp_training_reduces_loss():
 
 
 def _nsc_system(sc, warm, **kw):
+    # the network is consulted in every step (-1), to measure it alone
     cfg = dict(gravity=(0.0, 0.0, 0.0), lin_damp=0.0, ang_damp=0.0, model="nsc", dt=5e-4, nsc_mu=0.3,
-               nsc_velocity_iters=500, nsc_tol=1e-6, nsc_warm_start=warm)
+               nsc_velocity_iters=500, nsc_tol=1e-6, nsc_warm_start=warm, nsc_mlp_min_sweeps=-1)
     cfg.update(scene.pbc_kwargs(sc))
     cfg.update(kw)
     g = rodgpu.System(rodgpu.default_config(n_bodies=sc["n"], **cfg))
@@ -97,9 +98,9 @@ def test_learned_warm_start_saves_sweeps(trained):
     sc2.update(x=st["x"], q=st["q"], v=st["v"], w=st["w"])
     sweeps = {}
     first = {}
-    for warm in ("none", "cache", "mlp"):
-        g = _nsc_system(sc2, warm)
-        if warm == "mlp":
+    for warm in ("none", "cache", "mlp", "mlp_all"):
+        g = _nsc_system(sc2, "mlp" if warm == "mlp_all" else warm, nsc_mlp_scope=1 if warm == "mlp_all" else 0)
+        if warm.startswith("mlp"):
             g.mlp_set_params(params)
         r = g.step(1)
         first[warm] = (g.get_state(), r)
@@ -120,24 +121,27 @@ def test_learned_warm_start_saves_sweeps(trained):
     m = sc2["mass"][:, None]
     st_ref, r_ref = first["cache"]
     p_ref = (m * st_ref["v"]).sum(0)
-    for warm in ("mlp", "none"):
+    assert sweeps["mlp_all"] < sweeps["none"]
+    for warm in ("mlp", "mlp_all", "none"):
         st, r = first[warm]
         assert r["max_residual"] < 1e-6
         assert np.abs((m * st["v"]).sum(0) - p_ref).max() < 1e-9 * np.abs(m * st["v"]).sum()
         assert abs(r["kinetic_energy"] - r_ref["kinetic_energy"]) < 1e-3 * r_ref["kinetic_energy"]
 
 
-def test_zero_network_reproduces_cache_start(trained):
+@pytest.mark.parametrize("scope", [0, 1])
+def test_zero_network_reproduces_cache_start(trained, scope):
     """A network whose output layer is zero predicts 'no change', so the
     learned path must follow the cache-started path (to the rounding of the
-    friction-cone projection)."""
+    friction-cone projection), whether it is consulted for new contacts only
+    (scope 0) or for every contact (scope 1)."""
     sc, st, params, loss, nrec = trained
     sc2 = dict(sc)
     sc2.update(x=st["x"], q=st["q"], v=st["v"], w=st["w"])
     p0 = params.copy()
     p0[M.OFF_W4:M.OFF_IN_MEAN] = 0.0
     a = _nsc_system(sc2, "cache")
-    b = _nsc_system(sc2, "mlp")
+    b = _nsc_system(sc2, "mlp", nsc_mlp_scope=scope)
     b.mlp_set_params(p0)
     ra = a.step(10)
     rb = b.step(10)
@@ -145,6 +149,19 @@ def test_zero_network_reproduces_cache_start(trained):
     sa, sb = a.get_state(), b.get_state()
     for k in ("x", "q", "v", "w"):
         assert np.abs(sa[k] - sb[k]).max() <= 1e-12 * max(1.0, np.abs(sa[k]).max()), k
+
+
+def test_sweep_gated_learned_start(trained):
+    """With the default gate the network serves only steps after a hard one
+    (more than 3 sweeps) and the first step; PSOR still meets the tolerance
+    and needs no more sweeps than with the network in every step."""
+    sc, st, params, loss, nrec = trained
+    sc2 = dict(sc)
+    sc2.update(x=st["x"], q=st["q"], v=st["v"], w=st["w"])
+    g = _nsc_system(sc2, "mlp", nsc_mlp_min_sweeps=3)
+    g.mlp_set_params(params)
+    r = g.step(40)
+    assert r["not_converged"] == 0 and r["max_residual"] < 1e-6
 
 
 def test_mlp_warm_start_requires_network():
