@@ -234,13 +234,13 @@ def run_ours(args, rank, world):
     single = plain_single(rodgpu, args)
 
     plain = load_batch(rodgpu, items, "cache")
-    best_plain, _ = plain.autotune(candidates=(0, 1024, 2048, 4096, 8192, 16384), trial_steps=10)
+    best_plain, _ = plain.autotune(candidates=(0, 1024, 2048, 4096, 8192, 16384), trial_steps=20)
     res_plain = time_batch(plain, n_total, args)
     plain.close()
 
     learned = load_batch(rodgpu, items, "mlp")
     learned.set_mlp(params)
-    best, tune = learned.autotune(candidates=(0, 1024, 2048, 4096, 8192, 16384), trial_steps=10)
+    best, tune = learned.autotune(candidates=(0, 1024, 2048, 4096, 8192, 16384), trial_steps=20)
     dist = world > 1
     if dist:
         import torch.distributed as tdist
@@ -256,17 +256,20 @@ def run_ours(args, rank, world):
         ms = float(t.item())
     value = n_total * args.steps * world / (ms / 1000.0)
 
-    # end to end through the C ABI: every step uploads every member's state
-    # from host arrays, steps, and reads every state back
-    states = [learned.get_state(k) for k in range(len(items))]
-    k_e2e = max(3, min(args.steps, 10))
+    # end to end through the C ABI: every step uploads all members' states
+    # from page-locked host arrays (one bulk transfer per array), steps, and
+    # reads all states back
+    def pinned(cols):
+        return torch.empty((n_total, cols), dtype=torch.float64, pin_memory=True).numpy()
+    host = (pinned(3), pinned(4), pinned(3), pinned(3))
+    learned.get_state_all(out=host)
+    k_e2e = max(3, min(args.steps, 20))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(k_e2e):
-        for k, st in enumerate(states):
-            learned.set_state(k, st["x"], st["q"], st["v"], st["w"])
-        learned.step(1)
-        states = [learned.get_state(k) for k in range(len(items))]
+        learned.set_state_all(*host)
+        learned.step(1, stats=False)
+        learned.get_state_all(out=host)
     t1 = time.perf_counter()
     e2e = n_total * k_e2e / (t1 - t0)
     sched = learned.schedule()
@@ -293,7 +296,8 @@ def run_ours(args, rank, world):
                        "autotuned_rods_per_block": {"plain": best_plain, "learned": best},
                        "training": train},
         "e2e": {"value": round(e2e, 1), "unit": "rod-steps/s", "h2d_bytes_per_step": n_total * 13 * 8,
-                "d2h_bytes_per_step": n_total * 19 * 8, "steps": k_e2e},
+                "d2h_bytes_per_step": n_total * 13 * 8, "steps": k_e2e,
+                "path": "rg_batch_set_state_all + rg_batch_step(1) + rg_batch_get_state_all, pinned host arrays"},
         "gpu_launches": res["kernel_launches"],
         "roofline": roof,
         "clocks": clk.summary(),

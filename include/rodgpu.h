@@ -312,6 +312,14 @@ int rg_batch_get_state(const rg_batch* b, int k, double* x, double* q,
 /* nsteps steps of every member; per_system (optional) gets n_systems stats,
  * each with device_ms = the whole batch call. */
 int rg_batch_step(rg_batch* b, int nsteps, rg_step_stats* per_system);
+/* States of all members at once: x[3T], q[4T], v[3T], w[3T] (host arrays,
+ * member k's rods after those of members 0..k-1, T = total rods); forces
+ * and torques are cleared as rg_set_state does.  One transfer per array:
+ * page-locked arrays move at full host-link speed. */
+int rg_batch_set_state_all(rg_batch* b, const double* x, const double* q,
+                           const double* v, const double* w);
+int rg_batch_get_state_all(rg_batch* b, double* x, double* q, double* v,
+                           double* w);
 /* Loads the same network into every NSC member. */
 int rg_batch_set_mlp(rg_batch* b, const float* params, size_t n);
 int rg_batch_size(const rg_batch* b);

@@ -166,23 +166,32 @@ __global__ void k_ke(State st, Ctl* ctl, double* out) {
   (void)ctl;
 }
 
-double kinetic_energy(rg_system* s) {
-  const int g = 64;
-  if (!s->d_ke && cudaMalloc(&s->d_ke, sizeof(double) * g) != cudaSuccess) return NAN;
-  RGL k_ke<<<g, 256, 0, s->stream>>>(s->st, s->d_ctl, s->d_ke);
-  double hp[g];
-  cudaMemcpyAsync(hp, s->d_ke, sizeof(double) * g, cudaMemcpyDeviceToHost, s->stream);
-  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return NAN;
+constexpr int kKeBlocks = 64;
+
+void ke_launch(rg_system* s) {
+  if (!s->d_ke && cudaMalloc(&s->d_ke, sizeof(double) * kKeBlocks) != cudaSuccess) return;
+  RGL k_ke<<<kKeBlocks, 256, 0, s->stream>>>(s->st, s->d_ctl, s->d_ke);
+  cudaMemcpyAsync(s->h_ke, s->d_ke, sizeof(double) * kKeBlocks, cudaMemcpyDeviceToHost, s->stream);
+}
+
+double ke_sum(const rg_system* s) {
+  if (!s->d_ke) return NAN;
   double ke = 0;
-  for (int i = 0; i < g; ++i) ke += hp[i];
+  for (int i = 0; i < kKeBlocks; ++i) ke += s->h_ke[i];
   return ke;
+}
+
+double kinetic_energy(rg_system* s) {
+  ke_launch(s);
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return NAN;
+  return ke_sum(s);
 }
 
 // Device snapshot of everything a step mutates: state, control words,
 // current history table and the NSC warm cache.
-cudaError_t take_snapshot(rg_system* s, Snapshot& sn) {
+cudaError_t snapshot_alloc(rg_system* s) {
   const int n = s->n;
-  cudaError_t e;
+  cudaError_t e = cudaSuccess;
   size_t need = sizeof(double) * 19 * (size_t)n;
   if (!s->d_snap && (e = cudaMalloc(&s->d_snap, need))) return e;
   const History& H = s->hist;
@@ -201,6 +210,72 @@ cudaError_t take_snapshot(rg_system* s, Snapshot& sn) {
     if ((e = cudaMalloc(&s->snap_wlam, wl_bytes))) return e;
     s->snap_wcap = N.wcap;
   }
+  return e;
+}
+
+void snapshot_segments(rg_system* s, std::vector<CopySeg>& out) {
+  const History& H = s->hist;
+  const Nsc& N = s->nsc;
+  const size_t wl_bytes = sizeof(double) * 3 * (size_t)N.wcap + sizeof(int) * (size_t)N.wcap;
+  out.push_back({s->d_state, s->d_snap, sizeof(double) * 19 * (size_t)s->n});
+  out.push_back({H.key[H.cur], s->snap_hkey, sizeof(unsigned long long) * H.cap});
+  out.push_back({H.val[H.cur], s->snap_hval, sizeof(double) * 3 * (size_t)H.cap});
+  out.push_back({H.frame[H.cur], s->snap_hframe, sizeof(long long) * H.cap});
+  out.push_back({N.wkey, s->snap_wkey, sizeof(unsigned long long) * N.wcap});
+  out.push_back({N.wlam, s->snap_wlam, wl_bytes});
+}
+
+// One block per segment (strided): 16-byte words when both ends allow it,
+// else 4-byte words (every buffer here is 4-byte aligned and sized).
+__global__ void k_copy_segments(const CopySeg* segs, int n) {
+  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+    const CopySeg g = segs[k];
+    const unsigned long long a = (unsigned long long)g.src | (unsigned long long)g.dst | g.bytes;
+    if ((a & 15ull) == 0) {
+      const uint4* src = static_cast<const uint4*>(g.src);
+      uint4* dst = static_cast<uint4*>(g.dst);
+      for (unsigned long long i = threadIdx.x; i < g.bytes / 16; i += blockDim.x) dst[i] = src[i];
+    } else {
+      const unsigned* src = static_cast<const unsigned*>(g.src);
+      unsigned* dst = static_cast<unsigned*>(g.dst);
+      for (unsigned long long i = threadIdx.x; i < g.bytes / 4; i += blockDim.x) dst[i] = src[i];
+    }
+  }
+}
+
+void copy_segments_launch(const CopySeg* d_segs, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  RGL k_copy_segments<<<n < 2048 ? n : 2048, 256, 0, st>>>(d_segs, n);
+}
+
+__global__ void k_ctl_reset(Ctl* const* ctls, int n) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    Ctl* c = ctls[k];
+    c->err = 0;
+    c->rebuilds = 0;
+    c->sweeps_sum = 0;
+    c->not_conv = 0;
+    c->max_residual = 0;
+    c->row_sweeps = 0;
+    c->contact_steps = 0;
+    c->member_ns = 0;
+    c->bar_count = 0;
+  }
+}
+
+void ctl_reset_launch(Ctl* const* d_ctls, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  RGL k_ctl_reset<<<(n + 127) / 128, 128, 0, st>>>(d_ctls, n);
+}
+
+cudaError_t take_snapshot(rg_system* s, Snapshot& sn, bool sync) {
+  cudaError_t e = snapshot_alloc(s);
+  if (e) return e;
+  const int n = s->n;
+  const size_t need = sizeof(double) * 19 * (size_t)n;
+  const History& H = s->hist;
+  const Nsc& N = s->nsc;
+  const size_t wl_bytes = sizeof(double) * 3 * (size_t)N.wcap + sizeof(int) * (size_t)N.wcap;
   cudaStream_t st = s->stream;
   cudaMemcpyAsync(s->d_snap, s->d_state, need, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(s->snap_hkey, H.key[H.cur], sizeof(unsigned long long) * H.cap, cudaMemcpyDeviceToDevice, st);
@@ -208,11 +283,19 @@ cudaError_t take_snapshot(rg_system* s, Snapshot& sn) {
   cudaMemcpyAsync(s->snap_hframe, H.frame[H.cur], sizeof(long long) * H.cap, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(s->snap_wkey, N.wkey, sizeof(unsigned long long) * N.wcap, cudaMemcpyDeviceToDevice, st);
   cudaMemcpyAsync(s->snap_wlam, N.wlam, wl_bytes, cudaMemcpyDeviceToDevice, st);
-  sn.ctl.resize(s->ctl_bytes);
-  cudaMemcpyAsync(sn.ctl.data(), s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(&sn.wn, N.wn, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(s->h_snapctl, s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(s->h_wn, N.wn, sizeof(int), cudaMemcpyDeviceToHost, st);
   sn.hist_cur = H.cur;
-  return cudaStreamSynchronize(st);
+  if (!sync) return cudaGetLastError();
+  e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) finish_snapshot(s, sn);
+  return e;
+}
+
+void finish_snapshot(rg_system* s, Snapshot& sn) {
+  sn.ctl.resize(s->ctl_bytes);
+  std::memcpy(sn.ctl.data(), s->h_snapctl, s->ctl_bytes);
+  sn.wn = *s->h_wn;
 }
 
 // Puts the snapshot back into the live buffers (same capacities).
@@ -309,7 +392,8 @@ int rg_create(const rg_config* cfg, rg_system** out) {
   }
   s->ctl_bytes = ctl_size(*cfg);
   if ((e = cudaMalloc(&s->d_ctl, s->ctl_bytes)) || (e = cudaMemset(s->d_ctl, 0, s->ctl_bytes)) ||
-      (e = cudaMallocHost(&s->h_ctl, s->ctl_bytes))) {
+      (e = cudaMallocHost(&s->h_ctl, s->ctl_bytes)) || (e = cudaMallocHost(&s->h_snapctl, s->ctl_bytes)) ||
+      (e = cudaMallocHost(&s->h_wn, sizeof(int))) || (e = cudaMallocHost(&s->h_ke, sizeof(double) * 64))) {
     rg_destroy(s);
     return RG_ERR_CUDA;
   }
@@ -336,6 +420,9 @@ int rg_destroy(rg_system* s) {
   mlp_free(s);
   cudaFree(s->d_rec_x); cudaFree(s->d_rec_y); cudaFree(s->d_ke);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
+  if (s->h_snapctl) cudaFreeHost(s->h_snapctl);
+  if (s->h_wn) cudaFreeHost(s->h_wn);
+  if (s->h_ke) cudaFreeHost(s->h_ke);
   if (s->h_stage) cudaFreeHost(s->h_stage);
   for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -552,7 +639,7 @@ int resolve_call(rg_system* s, Snapshot& sn, int err, bool* retry) {
   return RG_OK;
 }
 
-void fill_stats(rg_system* s, int nsteps, rg_step_stats* stats) {
+void fill_stats(rg_system* s, int nsteps, rg_step_stats* stats, bool ke_launched) {
   Ctl* h = s->h_ctl;
   std::memset(stats, 0, sizeof(*stats));
   stats->steps = nsteps;
@@ -573,7 +660,7 @@ void fill_stats(rg_system* s, int nsteps, rg_step_stats* stats) {
   stats->psor_row_sweeps = h->row_sweeps;
   stats->kernel_launches = s->last_call_launches;
   stats->contact_steps = h->contact_steps;
-  stats->kinetic_energy = kinetic_energy(s);
+  stats->kinetic_energy = ke_launched ? ke_sum(s) : kinetic_energy(s);
 }
 
 }  // namespace rg

@@ -57,7 +57,75 @@ struct rg_batch {
   // measured cost per member: block-milliseconds per step (0: not measured)
   std::vector<double> cost;
   std::vector<int> team_nb;  // blocks of the member's team in the last plan
+  // control plane: copy segments, member control blocks gathered into one
+  // device buffer and one page-locked host buffer (control words + wn)
+  CopySeg* d_segs = nullptr;
+  int cap_segs = 0;
+  Ctl** d_ctls = nullptr;
+  unsigned char* d_ctlbuf = nullptr;
+  unsigned char* h_ctlbuf = nullptr;
+  std::vector<size_t> ctl_off;
+  size_t ctlbuf_bytes = 0;
+  // bulk state transfer: member table and device staging (x, q, v, w)
+  void* d_bulk = nullptr;
+  double* d_stage = nullptr;
+  long long total = 0;
 };
+
+namespace {
+struct BulkMember {
+  double* state;  // 19 n component arrays of the member
+  int n;
+  long long off;  // first rod in the concatenated arrays
+};
+
+__device__ inline int bulk_find(const BulkMember* m, int nm, long long g) {
+  int lo = 0, hi = nm;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (m[mid].off <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Concatenated host-layout arrays (x[3T], q[4T], v[3T], w[3T]) into every
+// member's component arrays; forces and torques are cleared, as
+// rg_set_state does without them.
+__global__ void k_bulk_scatter(const BulkMember* m, int nm, long long T, const double* x, const double* q,
+                               const double* v, const double* w) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < T;
+       g += (long long)gridDim.x * blockDim.x) {
+    const BulkMember M = m[bulk_find(m, nm, g)];
+    const size_t n = (size_t)M.n, i = (size_t)(g - M.off);
+    double* b = M.state;
+    for (int k = 0; k < 3; ++k) {
+      b[k * n + i] = x[3 * g + k];
+      b[(7 + k) * n + i] = v[3 * g + k];
+      b[(10 + k) * n + i] = w[3 * g + k];
+      b[(13 + k) * n + i] = 0.0;
+      b[(16 + k) * n + i] = 0.0;
+    }
+    for (int k = 0; k < 4; ++k) b[(3 + k) * n + i] = q[4 * g + k];
+  }
+}
+
+__global__ void k_bulk_gather(const BulkMember* m, int nm, long long T, double* x, double* q, double* v,
+                              double* w) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < T;
+       g += (long long)gridDim.x * blockDim.x) {
+    const BulkMember M = m[bulk_find(m, nm, g)];
+    const size_t n = (size_t)M.n, i = (size_t)(g - M.off);
+    const double* b = M.state;
+    for (int k = 0; k < 3; ++k) {
+      x[3 * g + k] = b[k * n + i];
+      v[3 * g + k] = b[(7 + k) * n + i];
+      w[3 * g + k] = b[(10 + k) * n + i];
+    }
+    for (int k = 0; k < 4; ++k) q[4 * g + k] = b[(3 + k) * n + i];
+  }
+}
+}  // namespace
 
 namespace {
 
@@ -204,6 +272,83 @@ cudaError_t launch_nsc(rg_batch* b, int nteams, int grid, int nsteps, bool graph
   return cudaGetLastError();
 }
 
+// Gathered control-plane buffers (allocated on first use).
+int ctl_setup(rg_batch* b) {
+  if (b->d_ctlbuf) return RG_OK;
+  b->ctl_off.resize(b->n + 1);
+  size_t off = 0;
+  for (int k = 0; k < b->n; ++k) {
+    b->ctl_off[k] = off;
+    off += (b->sys[k]->ctl_bytes + sizeof(int) + 15) & ~(size_t)15;  // control words, then wn
+  }
+  b->ctl_off[b->n] = off;
+  b->ctlbuf_bytes = off;
+  std::vector<Ctl*> ctls(b->n);
+  for (int k = 0; k < b->n; ++k) ctls[k] = b->sys[k]->d_ctl;
+  if (cudaMalloc(&b->d_ctlbuf, off) || cudaMallocHost(&b->h_ctlbuf, off) ||
+      cudaMalloc(&b->d_ctls, sizeof(Ctl*) * b->n)) {
+    cudaGetLastError();
+    return bfail(b, RG_ERR_CUDA, "control-plane buffers");
+  }
+  cudaMemcpy(b->d_ctls, ctls.data(), sizeof(Ctl*) * b->n, cudaMemcpyHostToDevice);
+  return RG_OK;
+}
+
+// Runs the copy segments on the device (one upload, one kernel).
+int run_segments(rg_batch* b, const std::vector<CopySeg>& segs) {
+  if ((int)segs.size() > b->cap_segs) {
+    cudaFree(b->d_segs);
+    b->cap_segs = (int)segs.size() * 2;
+    if (cudaMalloc(&b->d_segs, sizeof(CopySeg) * b->cap_segs)) {
+      cudaGetLastError();
+      b->cap_segs = 0;
+      return bfail(b, RG_ERR_CUDA, "copy segments");
+    }
+  }
+  cudaMemcpyAsync(b->d_segs, segs.data(), sizeof(CopySeg) * segs.size(), cudaMemcpyHostToDevice, b->stream);
+  copy_segments_launch(b->d_segs, (int)segs.size(), b->stream);
+  return RG_OK;
+}
+
+// Snapshots of all members with one copy kernel and one host read.
+int snapshot_all(rg_batch* b, std::vector<Snapshot>& sn) {
+  int rc = ctl_setup(b);
+  if (rc != RG_OK) return rc;
+  std::vector<CopySeg> segs;
+  segs.reserve(8 * b->n);
+  for (int k = 0; k < b->n; ++k) {
+    rg_system* s = b->sys[k];
+    if (snapshot_alloc(s)) return bfail(b, RG_ERR_CUDA, "snapshot buffers");
+    snapshot_segments(s, segs);
+    segs.push_back({s->d_ctl, b->d_ctlbuf + b->ctl_off[k], s->ctl_bytes});
+    segs.push_back({s->nsc.wn, b->d_ctlbuf + b->ctl_off[k] + s->ctl_bytes, sizeof(int)});
+    sn[k].hist_cur = s->hist.cur;
+  }
+  if ((rc = run_segments(b, segs)) != RG_OK) return rc;
+  cudaMemcpyAsync(b->h_ctlbuf, b->d_ctlbuf, b->ctlbuf_bytes, cudaMemcpyDeviceToHost, b->stream);
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e) return bfail(b, RG_ERR_CUDA, std::string("snapshot: ") + cudaGetErrorString(e));
+  for (int k = 0; k < b->n; ++k) {
+    rg_system* s = b->sys[k];
+    sn[k].ctl.assign(b->h_ctlbuf + b->ctl_off[k], b->h_ctlbuf + b->ctl_off[k] + s->ctl_bytes);
+    std::memcpy(&sn[k].wn, b->h_ctlbuf + b->ctl_off[k] + s->ctl_bytes, sizeof(int));
+  }
+  return RG_OK;
+}
+
+// Control blocks of the members in `which` into their host mirrors: one
+// copy kernel and one read (the caller synchronises the stream).
+int read_ctls(rg_batch* b, const std::vector<int>& which) {
+  std::vector<CopySeg> segs;
+  segs.reserve(which.size());
+  for (int k : which) segs.push_back({b->sys[k]->d_ctl, b->d_ctlbuf + b->ctl_off[k], b->sys[k]->ctl_bytes});
+  int rc = run_segments(b, segs);
+  if (rc != RG_OK) return rc;
+  cudaMemcpyAsync(b->h_ctlbuf, b->d_ctlbuf, b->ctlbuf_bytes, cudaMemcpyDeviceToHost, b->stream);
+  return RG_OK;
+}
+
 // One batch call: snapshot, launch, error resolution with replay of the
 // members that need larger buffers.  With restore_after (autotuner trials)
 // every member is put back to its state at the start of the call and its
@@ -216,14 +361,20 @@ int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after =
       return bfail(b, RG_ERR_STATE, "member " + std::to_string(k) + ": learned warm start without a network");
   }
   std::vector<Snapshot> sn(b->n);
-  for (int k = 0; k < b->n; ++k)
-    if (take_snapshot(b->sys[k], sn[k])) return bfail(b, RG_ERR_CUDA, "snapshot");
+  int rc0 = snapshot_all(b, sn);
+  if (rc0 != RG_OK) return rc0;
   std::vector<int> todo(b->n);
   std::iota(todo.begin(), todo.end(), 0);
   double total_ms = 0;
   for (int attempt = 0; attempt < 8 && !todo.empty(); ++attempt) {
-    for (int k : todo)
-      if (reset_call_ctl(b->sys[k], sn[k])) return bfail(b, RG_ERR_CUDA, "ctl upload");
+    if (attempt == 0) {
+      // the device control blocks equal the snapshots: zero the per-call
+      // counters in place
+      ctl_reset_launch(b->d_ctls, b->n, b->stream);
+    } else {
+      for (int k : todo)  // replays start from the (edited) snapshot words
+        if (reset_call_ctl(b->sys[k], sn[k])) return bfail(b, RG_ERR_CUDA, "ctl upload");
+    }
     std::vector<int> nsc;
     for (int k : todo)
       if (b->sys[k]->cfg.model == RG_MODEL_NSC) nsc.push_back(k);
@@ -260,9 +411,9 @@ int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after =
       if (b->sys[k]->cfg.model != RG_MODEL_NSC) launch_steps(b->sys[k], nsteps);
     cudaEventRecord(b->ev1, b->stream);
     if ((e = cudaGetLastError())) return bfail(b, RG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
-    for (int k : todo)
-      cudaMemcpyAsync(b->sys[k]->h_ctl, b->sys[k]->d_ctl, b->sys[k]->ctl_bytes, cudaMemcpyDeviceToHost, b->stream);
+    if (read_ctls(b, todo) != RG_OK) return RG_ERR_CUDA;
     if ((e = cudaStreamSynchronize(b->stream))) return bfail(b, RG_ERR_CUDA, std::string("step: ") + cudaGetErrorString(e));
+    for (int k : todo) std::memcpy(b->sys[k]->h_ctl, b->h_ctlbuf + b->ctl_off[k], b->sys[k]->ctl_bytes);
     float ms = 0;
     cudaEventElapsedTime(&ms, b->ev0, b->ev1);
     total_ms += ms;
@@ -295,11 +446,14 @@ int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after =
     }
     return RG_OK;
   }
-  if (per)
+  if (per) {
+    for (int k = 0; k < b->n; ++k) ke_launch(b->sys[k]);
+    if (cudaStreamSynchronize(b->stream)) return bfail(b, RG_ERR_CUDA, "statistics");
     for (int k = 0; k < b->n; ++k) {
-      fill_stats(b->sys[k], nsteps, &per[k]);
+      fill_stats(b->sys[k], nsteps, &per[k], true);
       per[k].device_ms = total_ms;
     }
+  }
   return RG_OK;
 }
 
@@ -345,6 +499,9 @@ int rg_batch_destroy(rg_batch* b) {
     rg_destroy(s);
   }
   cudaFree(b->d_views); cudaFree(b->d_teams); cudaFree(b->d_members); cudaFree(b->d_bars);
+  cudaFree(b->d_bulk); cudaFree(b->d_stage);
+  cudaFree(b->d_segs); cudaFree(b->d_ctls); cudaFree(b->d_ctlbuf);
+  if (b->h_ctlbuf) cudaFreeHost(b->h_ctlbuf);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -376,6 +533,75 @@ int rg_batch_set_state(rg_batch* b, int k, const double* x, const double* q, con
 int rg_batch_get_state(const rg_batch* b, int k, double* x, double* q, double* v, double* w) {
   if (!b || k < 0 || k >= b->n) return RG_ERR_ARG;
   return rg_get_state(b->sys[k], x, q, v, w, nullptr, nullptr);
+}
+
+namespace {
+// Member table and staging for the bulk transfers (allocated on first use).
+int bulk_setup(rg_batch* b) {
+  if (b->d_bulk) return RG_OK;
+  std::vector<BulkMember> t(b->n);
+  long long off = 0;
+  for (int k = 0; k < b->n; ++k) {
+    t[k] = BulkMember{b->sys[k]->d_state, b->sys[k]->n, off};
+    off += b->sys[k]->n;
+  }
+  b->total = off;
+  if (cudaMalloc(&b->d_bulk, sizeof(BulkMember) * b->n) ||
+      cudaMalloc(&b->d_stage, sizeof(double) * 13 * (size_t)off)) {
+    cudaGetLastError();
+    return bfail(b, RG_ERR_CUDA, "bulk staging allocation");
+  }
+  cudaMemcpy(b->d_bulk, t.data(), sizeof(BulkMember) * b->n, cudaMemcpyHostToDevice);
+  return RG_OK;
+}
+}  // namespace
+
+// States of all members at once: x[3T], q[4T], v[3T], w[3T] with the
+// members' rods concatenated in member order (T = total rods).  One copy per
+// array and one device kernel, instead of per-member host staging; page-
+// locked host arrays transfer at full link speed.
+int rg_batch_set_state_all(rg_batch* b, const double* x, const double* q, const double* v, const double* w) {
+  if (!b || !x || !q || !v || !w) return RG_ERR_ARG;
+  int rc = bulk_setup(b);
+  if (rc != RG_OK) return rc;
+  const long long T = b->total;
+  double* sx = b->d_stage;
+  double* sq = sx + 3 * T;
+  double* sv = sq + 4 * T;
+  double* sw = sv + 3 * T;
+  cudaMemcpyAsync(sx, x, sizeof(double) * 3 * T, cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync(sq, q, sizeof(double) * 4 * T, cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync(sv, v, sizeof(double) * 3 * T, cudaMemcpyHostToDevice, b->stream);
+  cudaMemcpyAsync(sw, w, sizeof(double) * 3 * T, cudaMemcpyHostToDevice, b->stream);
+  RGL k_bulk_scatter<<<592, 256, 0, b->stream>>>(static_cast<const BulkMember*>(b->d_bulk), b->n, T, sx, sq, sv, sw);
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e) return bfail(b, RG_ERR_CUDA, std::string("bulk set_state: ") + cudaGetErrorString(e));
+  for (rg_system* s : b->sys) {
+    s->state_set = true;
+    s->contacts_fresh = false;
+  }
+  return RG_OK;
+}
+
+int rg_batch_get_state_all(rg_batch* b, double* x, double* q, double* v, double* w) {
+  if (!b || !x || !q || !v || !w) return RG_ERR_ARG;
+  int rc = bulk_setup(b);
+  if (rc != RG_OK) return rc;
+  const long long T = b->total;
+  double* sx = b->d_stage;
+  double* sq = sx + 3 * T;
+  double* sv = sq + 4 * T;
+  double* sw = sv + 3 * T;
+  RGL k_bulk_gather<<<592, 256, 0, b->stream>>>(static_cast<const BulkMember*>(b->d_bulk), b->n, T, sx, sq, sv, sw);
+  cudaMemcpyAsync(x, sx, sizeof(double) * 3 * T, cudaMemcpyDeviceToHost, b->stream);
+  cudaMemcpyAsync(q, sq, sizeof(double) * 4 * T, cudaMemcpyDeviceToHost, b->stream);
+  cudaMemcpyAsync(v, sv, sizeof(double) * 3 * T, cudaMemcpyDeviceToHost, b->stream);
+  cudaMemcpyAsync(w, sw, sizeof(double) * 3 * T, cudaMemcpyDeviceToHost, b->stream);
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e) return bfail(b, RG_ERR_CUDA, std::string("bulk get_state: ") + cudaGetErrorString(e));
+  return RG_OK;
 }
 
 int rg_batch_set_mlp(rg_batch* b, const float* params, size_t n) {

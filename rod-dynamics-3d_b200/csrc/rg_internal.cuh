@@ -184,6 +184,10 @@ struct rg_system {
   // MLP (learned warm start)
   void* mlp_host = nullptr;   // network parameters and training workspace (rg_mlp.cu)
   double* d_ke = nullptr;     // kinetic-energy block partials
+  // page-locked host words for asynchronous snapshots and statistics
+  rg::Ctl* h_snapctl = nullptr;  // ctl_bytes
+  int* h_wn = nullptr;
+  double* h_ke = nullptr;        // 64 partial sums
   bool mlp_ready = false;
   bool recording = false;
   int rec_cap = 0;
@@ -292,13 +296,30 @@ struct Snapshot {
 };
 int fail(rg_system* s, int code, const std::string& msg);
 int cuda_fail(rg_system* s, cudaError_t e, const char* where);
-cudaError_t take_snapshot(rg_system* s, Snapshot& sn);
+cudaError_t take_snapshot(rg_system* s, Snapshot& sn, bool sync = true);
+// Pieces of a snapshot for callers that gather many systems' copies into one
+// device copy kernel (rg_batch): buffer set-up and the device-to-device
+// copies a snapshot makes.
+struct CopySeg {
+  const void* src;
+  void* dst;
+  unsigned long long bytes;
+};
+cudaError_t snapshot_alloc(rg_system* s);
+void snapshot_segments(rg_system* s, std::vector<CopySeg>& out);
+void copy_segments_launch(const CopySeg* d_segs, int n, cudaStream_t st);
+// Zeroes the per-call counters (as reset_call_ctl does from a snapshot)
+// of n systems' control blocks on the device.
+void ctl_reset_launch(rg::Ctl* const* d_ctls, int n, cudaStream_t st);
+void finish_snapshot(rg_system* s, Snapshot& sn);  // after the stream synchronised
 cudaError_t restore_snapshot(rg_system* s, const Snapshot& sn);
 cudaError_t reset_call_ctl(rg_system* s, const Snapshot& sn);
 int resolve_call(rg_system* s, Snapshot& sn, int err, bool* retry);
 void launch_steps(rg_system* s, int nsteps);
-void fill_stats(rg_system* s, int nsteps, rg_step_stats* stats);
+void fill_stats(rg_system* s, int nsteps, rg_step_stats* stats, bool ke_launched = false);
 double kinetic_energy(rg_system* s);
+void ke_launch(rg_system* s);  // partials to h_ke; read them with ke_sum after a stream sync
+double ke_sum(const rg_system* s);
 // launch geometry helper
 inline int grid_for(long long n, int bs, int maxb = 148 * 16) {
   long long g = (n + bs - 1) / bs;

@@ -78,6 +78,7 @@ ABI_SYMBOLS = [
     "rg_batch_set_bodies", "rg_batch_set_state", "rg_batch_get_state", "rg_batch_step",
     "rg_batch_set_mlp", "rg_mlp_grad", "rg_batch_size", "rg_batch_member", "rg_batch_last_error",
     "rg_batch_set_schedule", "rg_batch_get_schedule", "rg_batch_autotune",
+    "rg_batch_set_state_all", "rg_batch_get_state_all",
 ]
 
 
@@ -140,6 +141,8 @@ def lib():
                                             ctypes.POINTER(ctypes.c_int)]
         L.rg_batch_autotune.argtypes = [P, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_int), dp]
+        L.rg_batch_set_state_all.argtypes = [P, dp, dp, dp, dp]
+        L.rg_batch_get_state_all.argtypes = [P, dp, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -429,7 +432,28 @@ class Batch:
                     "batch_get_state")
         return {"x": x, "q": q, "v": v, "w": w}
 
-    def step(self, nsteps=1):
+    def total_rods(self):
+        return sum(c.n_bodies for c in self.cfgs)
+
+    def set_state_all(self, x, q, v, w):
+        """All members' states, rods concatenated in member order (pass
+        page-locked arrays for full transfer speed)."""
+        arr = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, q, v, w)]
+        self._check(self._lib.rg_batch_set_state_all(self._h, *[ptr(a) for a in arr]), "batch_set_state_all")
+
+    def get_state_all(self, out=None):
+        """All members' states as (x[T,3], q[T,4], v[T,3], w[T,3]); out, when
+        given, is a tuple of such contiguous float64 arrays to fill."""
+        T = self.total_rods()
+        if out is None:
+            out = (np.zeros((T, 3)), np.zeros((T, 4)), np.zeros((T, 3)), np.zeros((T, 3)))
+        self._check(self._lib.rg_batch_get_state_all(self._h, *[ptr(a) for a in out]), "batch_get_state_all")
+        return out
+
+    def step(self, nsteps=1, stats=True):
+        if not stats:
+            self._check(self._lib.rg_batch_step(self._h, int(nsteps), None), "batch_step")
+            return None
         st = (RgStepStats * len(self.cfgs))()
         self._check(self._lib.rg_batch_step(self._h, int(nsteps), st), "batch_step")
         return [s.as_dict() for s in st]

@@ -113,3 +113,26 @@ def test_batch_member_handle_and_learned_warm_start(specs):
     mu = specs[1][1].nsc_mu
     assert np.all(lam[:, 0] >= 0)
     assert np.all(np.hypot(lam[:, 1], lam[:, 2]) <= mu * lam[:, 0] * (1 + 1e-9) + 1e-15)
+
+
+def test_bulk_state_transfer_matches_members(specs):
+    b = _batch(specs)
+    b.step(3)
+    x, q, v, w = b.get_state_all()
+    off = 0
+    for k, (sc, _) in enumerate(specs):
+        n = sc["n"]
+        st = b.get_state(k)
+        assert np.array_equal(x[off:off + n], st["x"]) and np.array_equal(q[off:off + n], st["q"])
+        assert np.array_equal(v[off:off + n], st["v"]) and np.array_equal(w[off:off + n], st["w"])
+        off += n
+    # writing the same states back and stepping equals stepping on
+    c = _batch(specs)
+    c.step(3)
+    c.set_state_all(x, q, v, w)
+    b.step(4)
+    c.step(4)
+    for k in range(len(specs)):
+        sb, sc_ = b.get_state(k), c.get_state(k)
+        for key in ("x", "q", "v", "w"):
+            assert np.array_equal(sb[key], sc_[key]), (k, key)
