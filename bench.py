@@ -120,13 +120,15 @@ def roofline(bytes_, ms, kernel, traffic=None):
             "algorithmic_bytes_per_launch": round(bytes_, 1)}
 
 
-def profile_traffic(name):
-    """DRAM bytes per launch recorded by the committed ncu summary, if any."""
+def profile_traffic(name, rod_steps):
+    """DRAM bytes of a launch of rod_steps rod-steps, from the DRAM bytes per
+    rod-step that the committed ncu summary records (a capture of a smaller
+    launch of the same kernel, scaled by the rods and steps processed)."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
+            if line.startswith("traffic_bytes_per_rod_step:"):
+                return round(float(line.split(":", 1)[1].split()[0]) * rod_steps, 1)
     except OSError:
         pass
     return None
@@ -166,8 +168,7 @@ def plain_single(rodgpu, args):
             "sweeps_per_step": round(st["psor_sweeps"] / args.steps, 2),
             "contacts_per_step": round(st["contact_steps"] / args.steps, 1),
             "not_converged_steps": st["not_converged"], "max_residual": st["max_residual"],
-            "roofline": roofline(b, ms, "k_nsc_run (single system)",
-                                 profile_traffic("k_nsc_run_nsc_dense.md"))}
+            "roofline": roofline(b, ms, "k_nsc_run (single system)", None)}
 
 
 def train_network(rodgpu, args):
@@ -225,6 +226,8 @@ def run_ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     import torch
     torch.cuda.set_device(dev)  # the C library uses the current device
+    if args.workload == "batch_only":
+        return run_batch_only(args, rank, world)
     if args.workload != "batch":
         return run_single(args, rank, world)
     specs = [s for s in scene.batch_members(256, seed=args.seed + rank) if s["model"] == "nsc"]
@@ -276,7 +279,7 @@ def run_ours(args, rank, world):
     learned.close()
 
     roof = roofline(res["bytes"], res["ms"], "k_nsc_run (batched, learned warm start)",
-                    profile_traffic("k_nsc_run_batch.md"))
+                    profile_traffic("k_nsc_run_batch.md", n_total * args.steps))
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "rod-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
@@ -303,6 +306,40 @@ def run_ours(args, rank, world):
         "clocks": clk.summary(),
     }
     return out
+
+
+def run_batch_only(args, rank, world):
+    """The first --systems members of the batch workload, plain PSOR, fixed
+    schedule (4096 rods per block): one warm-up launch, then one timed
+    launch of --steps steps (the launch that profiles capture)."""
+    import rodgpu
+    from rodgpu import scene
+    import torch
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    specs = [x for x in scene.batch_members(256, seed=args.seed + rank) if x["model"] == "nsc"][:args.systems]
+    items = scene.batch_scenes(specs)
+    n_total = sum(sc["n"] for _, sc in items)
+    b = load_batch(rodgpu, items, "cache")
+    b.set_schedule(4096, True)
+    b.step(args.warmup, stats=False)
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        res = time_batch_once(b, n_total, args.steps)
+    return {"metric": METRIC, "value": res["value"], "unit": "rod-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded RSA packings)",
+            "config": {"workload": f"batch_only: {len(items)} NSC systems, {n_total} rods, plain PSOR"},
+            "gpu_launches": res["kernel_launches"], "clocks": clk.summary(),
+            "roofline": roofline(res["bytes"], res["ms"], "k_nsc_run (batched)", None)}
+
+
+def time_batch_once(b, n_total, steps):
+    st = b.step(steps)
+    ms = st[0]["device_ms"]
+    rs = sum(x["psor_row_sweeps"] for x in st)
+    cs = sum(x["contact_steps"] for x in st)
+    return {"value": round(n_total * steps / (ms / 1000.0), 1), "ms": ms, "ms_per_step": round(ms / steps, 4),
+            "kernel_launches": int(st[0]["kernel_launches"]), "bytes": nsc_bytes(n_total * steps, cs, rs)}
 
 
 def run_single(args, rank, world):
@@ -380,6 +417,7 @@ def main():
     ap.add_argument("--train-systems", type=int, default=32)
     ap.add_argument("--train-steps", type=int, default=40)
     ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--systems", type=int, default=128, help="batch_only: number of batch members")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batch")
     ap.add_argument("--n", type=int, default=None)
