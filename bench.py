@@ -236,14 +236,17 @@ def run_ours(args, rank, world):
     params, train = train_network(rodgpu, args)
     single = plain_single(rodgpu, args)
 
+    # schedule candidates: multiples of the rods per block of an even split
+    r0 = n_total / 148.0
+    cands = (0,) + tuple(int(r0 * f) for f in (0.5, 0.75, 1.0, 1.5, 2.0, 3.0))
     plain = load_batch(rodgpu, items, "cache")
-    best_plain, _ = plain.autotune(candidates=(0, 1024, 2048, 4096, 8192, 16384), trial_steps=20)
+    best_plain, _ = plain.autotune(candidates=cands, trial_steps=20)
     res_plain = time_batch(plain, n_total, args)
     plain.close()
 
     learned = load_batch(rodgpu, items, "mlp")
     learned.set_mlp(params)
-    best, tune = learned.autotune(candidates=(0, 1024, 2048, 4096, 8192, 16384), trial_steps=20)
+    best, tune = learned.autotune(candidates=cands, trial_steps=20)
     dist = world > 1
     if dist:
         import torch.distributed as tdist

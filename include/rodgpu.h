@@ -111,7 +111,7 @@ typedef struct rg_config {
   int32_t psor_order;            /* rg_psor_order; device supports COLORED */
 
   /* Neighbour-list broad phase (project-specific, no reference field). */
-  double skin;                   /* Verlet skin; <= 0: max(d/2, L/20), means */
+  double skin;                   /* Verlet skin; <= 0: max(d/2, L/10), means */
   int32_t max_neighbors;         /* initial per-rod list capacity; <= 0 auto */
   int32_t team_blocks;           /* blocks of the persistent NSC team; 0 auto */
   int32_t nsc_mlp_scope;         /* learned start for: 0 contacts new since
@@ -121,7 +121,9 @@ typedef struct rg_config {
                                     needed more PSOR sweeps than this, or the
                                     warm cache is empty (default 3; -1: in
                                     every step)                              */
-  int32_t reserved[4];
+  int32_t near_skin_pct;         /* near-list skin, % of the Verlet skin (0:
+                                    automatic, 5 %)                          */
+  int32_t reserved[3];
 } rg_config;
 
 /* Per-call statistics (the profile-CSV columns of main.cpp:3276-3355). */
@@ -336,6 +338,10 @@ const char* rg_batch_last_error(const rg_batch* b);
 int rg_batch_set_schedule(rg_batch* b, int rods_per_block, int use_graph);
 int rg_batch_get_schedule(const rg_batch* b, int* rods_per_block, int* grid,
                           int* nteams);
+/* The cost model: each member's measured device cost (block-milliseconds
+ * per step, 0 before its first timed call) and its team's block count in
+ * the current plan. */
+int rg_batch_get_costs(const rg_batch* b, double* cost_ms, int* team_blocks);
 /* Autotuner: measures every member's step cost (all single-block), then
  * times trial_steps steps per candidate R after two untimed steps, from the
  * current state (state put back after each trial), and selects the fastest;

@@ -21,6 +21,7 @@
 // fastest.  The schedule changes time only: every member's results are the
 // same for any schedule.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -57,6 +58,7 @@ struct rg_batch {
   // measured cost per member: block-milliseconds per step (0: not measured)
   std::vector<double> cost;
   std::vector<int> team_nb;  // blocks of the member's team in the last plan
+  bool cost_frozen = false;  // autotuner trials compare schedules on one cost model
   // control plane: copy segments, member control blocks gathered into one
   // device buffer and one page-locked host buffer (control words + wn)
   CopySeg* d_segs = nullptr;
@@ -172,7 +174,12 @@ void plan(rg_batch* b, const std::vector<int>& which, int R, std::vector<TeamDes
     nb[i] = std::max(1, (int)(W[big[i]] / R + 0.5));
     want += nb[i];
   }
-  const int reserve = small.empty() ? 0 : std::min<int>((int)small.size(), std::max(1, budget / 8));
+  // blocks for the packed members: their work at R per block
+  double small_work = 0.0;
+  for (int k : small) small_work += W[k];
+  const int reserve = small.empty() ? 0
+                                    : std::min<int>((int)small.size(),
+                                                    std::max(1, (int)std::ceil(small_work / std::max(1, R))));
   const int avail = std::max<int>((int)big.size(), budget - reserve);
   if (want > avail) {  // scale the large teams down to fit
     for (size_t i = 0; i < big.size(); ++i) nb[i] = std::max(1, (int)((long long)nb[i] * avail / want));
@@ -424,8 +431,13 @@ int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after =
       s->last_call_ms = ms;
       s->last_call_launches = launches;
       const int err = s->h_ctl->err;
-      if (!err && full && s->cfg.model == RG_MODEL_NSC && nsteps > 0 && s->h_ctl->member_ns > 0)
-        b->cost[k] = 1e-6 * (double)s->h_ctl->member_ns / nsteps * b->team_nb[k];
+      if (!err && full && !b->cost_frozen && s->cfg.model == RG_MODEL_NSC && nsteps > 0 && s->h_ctl->member_ns > 0) {
+        // block-ms per step, averaged with the previous estimate: list
+        // rebuilds and steps that run to the sweep limit make single calls
+        // noisy
+        const double c = 1e-6 * (double)s->h_ctl->member_ns / nsteps * b->team_nb[k];
+        b->cost[k] = b->cost[k] > 0 ? 0.5 * (b->cost[k] + c) : c;
+      }
       if (!err) continue;
       bool retry = false;
       int rc = resolve_call(s, sn[k], err, &retry);
@@ -631,6 +643,15 @@ int rg_batch_get_schedule(const rg_batch* b, int* rods_per_block, int* grid, int
   return RG_OK;
 }
 
+int rg_batch_get_costs(const rg_batch* b, double* cost_ms, int* team_blocks) {
+  if (!b) return RG_ERR_ARG;
+  for (int k = 0; k < b->n; ++k) {
+    if (cost_ms) cost_ms[k] = b->cost[k];
+    if (team_blocks) team_blocks[k] = b->team_nb[k];
+  }
+  return RG_OK;
+}
+
 int rg_batch_step(rg_batch* b, int nsteps, rg_step_stats* per_system) {
   if (!b || nsteps < 0) return RG_ERR_ARG;
   return batch_call(b, nsteps, per_system);
@@ -649,15 +670,19 @@ int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand, int trial_
   // cost model first: every member's own step time on the device, measured
   // with all members in single-block teams
   rg_batch_set_schedule(b, 0, b->use_graph);
-  const int rc0 = batch_call(b, trial_steps, nullptr, true, 2);
+  const int rc0 = batch_call(b, 2 * trial_steps, nullptr, true, 2);
   if (rc0 != RG_OK) return rc0;
   int best = candidates[0];
   double best_ms = 1e300;
+  b->cost_frozen = true;
   for (int c = 0; c < n_cand; ++c) {
     rg_batch_set_schedule(b, candidates[c], b->use_graph);
     int rc = batch_call(b, trial_steps, nullptr, true, 2);  // grows buffers, builds the graph
     if (rc == RG_OK) rc = batch_call(b, trial_steps, nullptr, true, 2);
-    if (rc != RG_OK) return rc;
+    if (rc != RG_OK) {
+      b->cost_frozen = false;
+      return rc;
+    }
     const double ms = b->last_ms;
     if (ms_out) ms_out[c] = ms;
     if (ms < best_ms) {
@@ -665,6 +690,7 @@ int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand, int trial_
       best = candidates[c];
     }
   }
+  b->cost_frozen = false;
   rg_batch_set_schedule(b, best, b->use_graph);
   if (best_out) *best_out = best;
   return RG_OK;

@@ -308,9 +308,10 @@ cudaError_t detector_alloc(rg_system* s) {
     lsum += 2 * h[i];
   }
   d.margin = c.model == RG_MODEL_HARMONIC ? c.soft_delta : 0.0;
-  // Default skin: half a diameter, but at least 5% of the rod length, so
-  // thin rods (whose lists stay short) rebuild rarely.
-  d.skin = c.skin > 0 ? c.skin : fmax(0.5 * (dsum / n), 0.05 * (lsum / n)) + 1e-6;
+  // Default skin: half a diameter, but at least a tenth of the rod length,
+  // so thin rods (whose lists stay short, and whose per-step narrow phase
+  // runs over the near list only) rebuild rarely.
+  d.skin = c.skin > 0 ? c.skin : fmax(0.5 * (dsum / n), 0.1 * (lsum / n)) + 1e-6;
   d.cut_center = 2.0 * (hmax + rmax) + d.margin + d.skin;
   d.all_pairs = false;
   GridDev gd{};
@@ -355,7 +356,7 @@ cudaError_t detector_alloc(rg_system* s) {
   if ((e = cudaMalloc(&d.hit_mask, sizeof(unsigned long long) * (size_t)n * d.mask_words))) return e;
   if ((e = cudaMemset(d.nbr_cnt, 0, sizeof(int) * n))) return e;
   if (c.model == RG_MODEL_NSC) {
-    d.near_skin = 0.2 * d.skin;
+    d.near_skin = (c.near_skin_pct > 0 ? 0.01 * c.near_skin_pct : 0.05) * d.skin;
     if ((e = cudaMalloc(&d.near, sizeof(int2) * (size_t)n * d.maxnb))) return e;
     if ((e = cudaMalloc(&d.ref2, sizeof(double) * 6 * (size_t)n))) return e;
   }

@@ -218,6 +218,60 @@ __device__ inline void build_cell_pairs(const Seg* seg, const GridDev& g, const 
   __syncthreads();
 }
 
+// Rod-parallel list build (one thread per home rod, no block barriers):
+// the candidates of rod i are the rods of its cell's neighbourhood, read
+// from the cell arrays; accepted j > i are appended to i's own list (sorted
+// afterwards by sort_list).  Same acceptance as build_cell_pairs.  Suits
+// sparse cells, where staging a tile per neighbouring cell costs a memory
+// round trip and a barrier for a handful of pairs.
+__device__ inline void build_rod_list(int i, const Seg* seg, const GridDev& g, const Box& box, const double* invL,
+                                      const int* cell_of, const int* cell_start, const int* cell_rods, double margin,
+                                      double skin, int all_pairs, int* nbr_cnt, int* nbr, int maxnb, int& overflow) {
+  const int cell = cell_of[i];
+  const int c3[3] = {cell % g.n[0], (cell / g.n[0]) % g.n[1], cell / (g.n[0] * g.n[1])};
+  int lo[3], hi[3];
+  for (int k = 0; k < 3; ++k) {
+    if (box.pbc && (g.n[k] < 3 || all_pairs)) {
+      lo[k] = 0; hi[k] = g.n[k] - 1;
+    } else {
+      lo[k] = c3[k] - 1; hi[k] = c3[k] + 1;
+    }
+  }
+  const Seg A = seg[i];
+  int* L = nbr + (size_t)i * maxnb;
+  int cnt = 0;
+  for (int z = lo[2]; z <= hi[2]; ++z)
+    for (int y = lo[1]; y <= hi[1]; ++y)
+      for (int x = lo[0]; x <= hi[0]; ++x) {
+        int X = x, Y = y, Z = z;
+        if (box.pbc) {
+          X = (X + g.n[0]) % g.n[0]; Y = (Y + g.n[1]) % g.n[1]; Z = (Z + g.n[2]) % g.n[2];
+        } else if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) {
+          continue;
+        }
+        const int c = (Z * g.n[1] + Y) * g.n[0] + X;
+        const int e = cell_start[c + 1];
+        for (int q = cell_start[c]; q < e; ++q) {
+          const int j = cell_rods[q];
+          if (j <= i) continue;
+          const Seg B = seg[j];
+          if (!all_pairs) {
+            const d3 d = centre_offset(A, B, box, invL);
+            const double cc = A.h + B.h + A.r + B.r + margin + skin;
+            if (dot(d, d) > cc * cc * (1.0 + 1e-9)) continue;
+            const double lim = A.r + B.r + margin + skin;
+            if (seg_far(A, B, d, lim)) continue;
+            const Narrow nr = narrow_pair(A, B, box);
+            if (!(nr.d2 < lim * lim)) continue;
+          }
+          if (cnt < maxnb) L[cnt] = j;
+          else overflow = 1;
+          ++cnt;
+        }
+      }
+  nbr_cnt[i] = cnt;
+}
+
 // Sorts rod i's neighbour list ascending (insertion sort; lists are short).
 __device__ inline void sort_list(int* nbr, int* nbr_cnt, int maxnb, int i, int& overflow) {
   int cnt = nbr_cnt[i];

@@ -219,9 +219,17 @@ __device__ __noinline__ bool rebuild_phase(const Team& T, const NscView& V, Smem
   double invL[3] = {1.0, 1.0, 1.0};
   for (int k = 0; k < 3; ++k)
     if (V.box.L[k] > 0.0) invL[k] = 1.0 / V.box.L[k];
-  for (int cell = rank; cell < g.ncells; cell += T.nb)
-    build_cell_pairs(V.seg, g, V.box, invL, V.cell_start, V.cell_rods, V.margin, V.skin, V.all_pairs,
-                     V.nbr_cnt, V.nbr, V.maxnb, cell, sm.build, overflow);
+  if (n < 48 * g.ncells) {
+    // sparse cells: one thread per home rod
+    for (int i = tid; i < n; i += TS)
+      build_rod_list(i, V.seg, g, V.box, invL, V.cell_of, V.cell_start, V.cell_rods, V.margin, V.skin,
+                     V.all_pairs, V.nbr_cnt, V.nbr, V.maxnb, overflow);
+  } else {
+    // crowded cells: the block splits the pairs of one home cell at a time
+    for (int cell = rank; cell < g.ncells; cell += T.nb)
+      build_cell_pairs(V.seg, g, V.box, invL, V.cell_start, V.cell_rods, V.margin, V.skin, V.all_pairs,
+                       V.nbr_cnt, V.nbr, V.maxnb, cell, sm.build, overflow);
+  }
   if (!team_sync(T)) return false;
   for (int i = tid; i < n; i += TS) {
     sort_list(V.nbr, V.nbr_cnt, V.maxnb, i, overflow);

@@ -44,7 +44,7 @@ class RgConfig(ctypes.Structure):
         ("nsc_tol", _d), ("nsc_velocity_iters", _i), ("nsc_position_stabilization", _i),
         ("nsc_position_iters", _i), ("nsc_position_psor_iters", _i), ("nsc_warm_start", _i),
         ("psor_order", _i), ("skin", _d), ("max_neighbors", _i), ("team_blocks", _i),
-        ("nsc_mlp_scope", _i), ("nsc_mlp_min_sweeps", _i), ("reserved", _i * 4),
+        ("nsc_mlp_scope", _i), ("nsc_mlp_min_sweeps", _i), ("near_skin_pct", _i), ("reserved", _i * 3),
     ]
 
 
@@ -78,7 +78,7 @@ ABI_SYMBOLS = [
     "rg_batch_set_bodies", "rg_batch_set_state", "rg_batch_get_state", "rg_batch_step",
     "rg_batch_set_mlp", "rg_mlp_grad", "rg_batch_size", "rg_batch_member", "rg_batch_last_error",
     "rg_batch_set_schedule", "rg_batch_get_schedule", "rg_batch_autotune",
-    "rg_batch_set_state_all", "rg_batch_get_state_all",
+    "rg_batch_set_state_all", "rg_batch_get_state_all", "rg_batch_get_costs",
 ]
 
 
@@ -142,6 +142,7 @@ def lib():
         L.rg_batch_autotune.argtypes = [P, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_int), dp]
         L.rg_batch_set_state_all.argtypes = [P, dp, dp, dp, dp]
+        L.rg_batch_get_costs.argtypes = [P, dp, ctypes.POINTER(ctypes.c_int)]
         L.rg_batch_get_state_all.argtypes = [P, dp, dp, dp, dp]
         _lib = L
     return _lib
@@ -471,6 +472,13 @@ class Batch:
         self._check(self._lib.rg_batch_get_schedule(self._h, ctypes.byref(r), ctypes.byref(g), ctypes.byref(t)),
                     "batch_get_schedule")
         return {"rods_per_block": r.value, "grid": g.value, "teams": t.value}
+
+    def costs(self):
+        """(measured block-ms per step of each member, its team's blocks)."""
+        c = np.zeros(len(self.cfgs))
+        t = np.zeros(len(self.cfgs), np.int32)
+        self._check(self._lib.rg_batch_get_costs(self._h, ptr(c), ptr(t, ctypes.c_int)), "batch_get_costs")
+        return c, t
 
     def autotune(self, candidates=(0, 1024, 2048, 4096, 8192), trial_steps=10):
         c = (ctypes.c_int * len(candidates))(*candidates)
