@@ -122,7 +122,7 @@ typedef struct rg_config {
                                     warm cache is empty (default 3; -1: in
                                     every step)                              */
   int32_t near_skin_pct;         /* near-list skin, % of the Verlet skin (0:
-                                    automatic, 5 %)                          */
+                                    automatic: 5 %, 50 % in all-pairs boxes) */
   int32_t reserved[3];
 } rg_config;
 
@@ -342,6 +342,10 @@ int rg_batch_get_schedule(const rg_batch* b, int* rods_per_block, int* grid,
  * per step, 0 before its first timed call) and its team's block count in
  * the current plan. */
 int rg_batch_get_costs(const rg_batch* b, double* cost_ms, int* team_blocks);
+/* Device time of each team of the last full plan's launch (ms), its block
+ * count and member count; at most cap teams, *nteams gets the number. */
+int rg_batch_get_team_times(const rg_batch* b, double* ms, int* blocks, int* members, int cap,
+                            int* nteams);
 /* Autotuner: measures every member's step cost (all single-block), then
  * times trial_steps steps per candidate R after two untimed steps, from the
  * current state (state put back after each trial), and selects the fastest;

@@ -263,6 +263,15 @@ __global__ void k_ctl_reset(Ctl* const* ctls, int n) {
   }
 }
 
+__global__ void k_ctl_zero_time(Ctl* const* ctls, int n) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) ctls[k]->member_ns = 0;
+}
+
+void ctl_zero_time_launch(Ctl* const* d_ctls, int n, cudaStream_t st) {
+  if (n <= 0) return;
+  RGL k_ctl_zero_time<<<(n + 127) / 128, 128, 0, st>>>(d_ctls, n);
+}
+
 void ctl_reset_launch(Ctl* const* d_ctls, int n, cudaStream_t st) {
   if (n <= 0) return;
   RGL k_ctl_reset<<<(n + 127) / 128, 128, 0, st>>>(d_ctls, n);

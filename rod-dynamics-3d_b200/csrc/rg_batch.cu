@@ -48,6 +48,7 @@ struct rg_batch {
   TeamDesc* d_teams = nullptr;
   int* d_members = nullptr;
   unsigned int* d_bars = nullptr;
+  long long* d_team_ns = nullptr;
   int cap_members = 0, cap_teams = 0;
   // graph of (barrier reset + persistent launch) for graph_steps steps
   cudaGraphExec_t graph = nullptr;
@@ -228,6 +229,8 @@ cudaError_t ensure_dev(rg_batch* b, size_t nteams, size_t nmembers) {
     b->cap_teams = (int)std::max<size_t>(nteams, (size_t)b->coop_blocks);
     if ((e = cudaMalloc(&b->d_teams, sizeof(TeamDesc) * b->cap_teams))) return e;
     if ((e = cudaMalloc(&b->d_bars, sizeof(unsigned int) * 4 * b->cap_teams))) return e;
+    cudaFree(b->d_team_ns);
+    if ((e = cudaMalloc(&b->d_team_ns, sizeof(long long) * b->cap_teams))) return e;
   }
   return e;
 }
@@ -240,7 +243,10 @@ cudaError_t upload(rg_batch* b, std::vector<TeamDesc>& teams, const std::vector<
   std::vector<NscView> views(b->n);
   for (int k = 0; k < b->n; ++k)
     if (b->sys[k]->cfg.model == RG_MODEL_NSC) views[k] = make_view(b->sys[k]);
-  for (size_t t = 0; t < teams.size(); ++t) teams[t].bar = b->d_bars + 4 * t;
+  for (size_t t = 0; t < teams.size(); ++t) {
+    teams[t].bar = b->d_bars + 4 * t;
+    teams[t].t_ns = b->d_team_ns + t;
+  }
   cudaMemcpyAsync(b->d_views, views.data(), sizeof(NscView) * b->n, cudaMemcpyHostToDevice, b->stream);
   cudaMemcpyAsync(b->d_teams, teams.data(), sizeof(TeamDesc) * teams.size(), cudaMemcpyHostToDevice, b->stream);
   cudaMemcpyAsync(b->d_members, members.data(), sizeof(int) * members.size(), cudaMemcpyHostToDevice, b->stream);
@@ -409,6 +415,7 @@ int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after =
       if (ew) return bfail(b, RG_ERR_CUDA, std::string("persistent launch: ") + cudaGetErrorString(ew));
       for (int k : todo)
         if (b->sys[k]->cfg.model != RG_MODEL_NSC) launch_steps(b->sys[k], warm_steps);
+      ctl_zero_time_launch(b->d_ctls, b->n, b->stream);  // costs count the timed steps only
     }
     const long long l0 = g_launches;
     cudaEventRecord(b->ev0, b->stream);
@@ -510,7 +517,7 @@ int rg_batch_destroy(rg_batch* b) {
     s->stream = nullptr;
     rg_destroy(s);
   }
-  cudaFree(b->d_views); cudaFree(b->d_teams); cudaFree(b->d_members); cudaFree(b->d_bars);
+  cudaFree(b->d_views); cudaFree(b->d_teams); cudaFree(b->d_members); cudaFree(b->d_bars); cudaFree(b->d_team_ns);
   cudaFree(b->d_bulk); cudaFree(b->d_stage);
   cudaFree(b->d_segs); cudaFree(b->d_ctls); cudaFree(b->d_ctlbuf);
   if (b->h_ctlbuf) cudaFreeHost(b->h_ctlbuf);
@@ -640,6 +647,21 @@ int rg_batch_get_schedule(const rg_batch* b, int* rods_per_block, int* grid, int
   if (rods_per_block) *rods_per_block = b->rods_per_block;
   if (grid) *grid = b->grid;
   if (nteams) *nteams = (int)b->teams.size();
+  return RG_OK;
+}
+
+int rg_batch_get_team_times(const rg_batch* b, double* ms, int* blocks, int* members, int cap, int* nteams) {
+  if (!b || !nteams) return RG_ERR_ARG;
+  const int nt = (int)b->teams.size();
+  *nteams = nt;
+  if (nt == 0 || !b->d_team_ns) return RG_OK;
+  std::vector<long long> ns(nt);
+  cudaMemcpy(ns.data(), b->d_team_ns, sizeof(long long) * nt, cudaMemcpyDeviceToHost);
+  for (int t = 0; t < nt && t < cap; ++t) {
+    if (ms) ms[t] = 1e-6 * (double)ns[t];
+    if (blocks) blocks[t] = b->teams[t].nb;
+    if (members) members[t] = b->teams[t].count;
+  }
   return RG_OK;
 }
 

@@ -356,7 +356,9 @@ cudaError_t detector_alloc(rg_system* s) {
   if ((e = cudaMalloc(&d.hit_mask, sizeof(unsigned long long) * (size_t)n * d.mask_words))) return e;
   if ((e = cudaMemset(d.nbr_cnt, 0, sizeof(int) * n))) return e;
   if (c.model == RG_MODEL_NSC) {
-    d.near_skin = (c.near_skin_pct > 0 ? 0.01 * c.near_skin_pct : 0.05) * d.skin;
+    // all-pairs boxes rebuild the near list from every pair: a wider near
+    // skin makes those rebuilds rare
+    d.near_skin = (c.near_skin_pct > 0 ? 0.01 * c.near_skin_pct : (d.all_pairs ? 0.5 : 0.05)) * d.skin;
     if ((e = cudaMalloc(&d.near, sizeof(int2) * (size_t)n * d.maxnb))) return e;
     if ((e = cudaMalloc(&d.ref2, sizeof(double) * 6 * (size_t)n))) return e;
   }

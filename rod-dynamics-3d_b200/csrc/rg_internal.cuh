@@ -311,6 +311,7 @@ void copy_segments_launch(const CopySeg* d_segs, int n, cudaStream_t st);
 // Zeroes the per-call counters (as reset_call_ctl does from a snapshot)
 // of n systems' control blocks on the device.
 void ctl_reset_launch(rg::Ctl* const* d_ctls, int n, cudaStream_t st);
+void ctl_zero_time_launch(rg::Ctl* const* d_ctls, int n, cudaStream_t st);  // member_ns only
 void finish_snapshot(rg_system* s, Snapshot& sn);  // after the stream synchronised
 cudaError_t restore_snapshot(rg_system* s, const Snapshot& sn);
 cudaError_t reset_call_ctl(rg_system* s, const Snapshot& sn);

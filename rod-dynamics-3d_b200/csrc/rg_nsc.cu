@@ -1323,6 +1323,8 @@ __global__ void __launch_bounds__(kBlock, 1) k_nsc_run(const NscView* views, con
   }
   const TeamDesc td = teams[lo];
   if ((int)blockIdx.x < td.b0 || (int)blockIdx.x >= td.b0 + td.nb) return;
+  const bool team_timer = td.t_ns && threadIdx.x == 0 && (int)blockIdx.x == td.b0;
+  const unsigned long long t_start = team_timer ? gtimer() : 0ull;
   for (int s = 0; s < nsteps; ++s) {
     bool any = false;
     for (int m = td.first; m < td.first + td.count; ++m) {
@@ -1335,6 +1337,7 @@ __global__ void __launch_bounds__(kBlock, 1) k_nsc_run(const NscView* views, con
     }
     if (!any) break;
   }
+  if (team_timer) *td.t_ns = (long long)(gtimer() - t_start);
 }
 
 // ---------------------------------------------------------------------------

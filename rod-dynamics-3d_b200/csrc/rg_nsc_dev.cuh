@@ -34,7 +34,7 @@ struct RowIO {
 };
 enum { R_N = 0, R_T1 = 3, R_T2 = 6, R_RA = 9, R_RB = 12, R_IAN = 15, R_IAT1 = 18, R_IAT2 = 21,
        R_IBN = 24, R_IBT1 = 27, R_IBT2 = 30, R_IMA = 33, R_IMB = 34, R_GN = 35, R_GT1 = 36,
-       R_GT2 = 37, R_BN = 38, R_BREST = 39, R_PHI = 40, R_VNPRE = 41 };
+       R_GT2 = 37, R_BN = 38, R_BREST = 39, R_PHI = 40, R_VNPRE = 41 };  // R_G*: omega / g
 enum { P_N = 0, P_RA = 3, P_RB = 6, P_PHI = 9, P_G = 10, P_L = 11 };
 
 __device__ inline d3 iinv_apply(const State& st, int i, d3 v) {
@@ -80,9 +80,11 @@ __device__ inline int build_row(const State& st, const Contacts& con, const rg_c
   d3 rb = pb - (st.x.ld(b) + sh);
   R.w3(R_N, p, n); R.w3(R_T1, p, t1); R.w3(R_T2, p, t2);
   R.w3(R_RA, p, ra); R.w3(R_RB, p, rb);
-  R.r(R_GN, p) = diag_of(st, a, b, ra, rb, n, cfg.nsc_cfm);
-  R.r(R_GT1, p) = diag_of(st, a, b, ra, rb, t1, cfg.nsc_cfm);
-  R.r(R_GT2, p) = diag_of(st, a, b, ra, rb, t2, cfg.nsc_cfm);
+  // omega / g per direction, computed once here instead of in every sweep
+  // (the same quotient the sweep would form, so results are unchanged)
+  R.r(R_GN, p) = cfg.nsc_omega / diag_of(st, a, b, ra, rb, n, cfg.nsc_cfm);
+  R.r(R_GT1, p) = cfg.nsc_omega / diag_of(st, a, b, ra, rb, t1, cfg.nsc_cfm);
+  R.r(R_GT2, p) = cfg.nsc_omega / diag_of(st, a, b, ra, rb, t2, cfg.nsc_cfm);
   R.r(R_IMA, p) = st.inv_mass[a];
   R.r(R_IMB, p) = st.inv_mass[b];
   R.w3(R_IAN, p, iinv_apply(st, a, cross(ra, n)));
@@ -160,6 +162,7 @@ __device__ inline void warm_apply(const RowIO& R, const Vel& V, int p, int a, in
 // |dλn| + |dλt1| + |dλt2|.
 __device__ inline double psor_row(const RowIO& R, const Vel& V, int p, int a, int b, double omega, double cfm,
                                   double mu) {
+  (void)omega;  // folded into the row (R_GN, R_GT1, R_GT2 hold omega / g)
   d3 n = R.r3(R_N, p), t1 = R.r3(R_T1, p), t2 = R.r3(R_T2, p);
   d3 ra = R.r3(R_RA, p), rb = R.r3(R_RB, p);
   d3 IAn = R.r3(R_IAN, p), IAt1 = R.r3(R_IAT1, p), IAt2 = R.r3(R_IAT2, p);
@@ -169,7 +172,7 @@ __device__ inline double psor_row(const RowIO& R, const Vel& V, int p, int a, in
   d3 vA = V.v.ld(a), wA = V.w.ld(a), vB = V.v.ld(b), wB = V.w.ld(b);
   d3 vrel = (vB + cross(wB, rb)) - (vA + cross(wA, ra));
   double wn = dot(n, vrel) + R.r(R_BN, p) + R.r(R_BREST, p) + cfm * ln;
-  double dn_ = -(omega / R.r(R_GN, p)) * wn;
+  double dn_ = -R.r(R_GN, p) * wn;
   double old = ln;
   ln = smax(0.0, old + dn_);
   double dn = ln - old;
@@ -186,7 +189,7 @@ __device__ inline double psor_row(const RowIO& R, const Vel& V, int p, int a, in
   double mf = mu * ln;
   double lim1 = sqrt(smax(0.0, mf * mf - lt2 * lt2));
   double w1 = dot(t1, vrel) + cfm * lt1;
-  double d1_ = -(omega / R.r(R_GT1, p)) * w1;
+  double d1_ = -R.r(R_GT1, p) * w1;
   double o1 = lt1;
   lt1 = smin(smax(o1 + d1_, -lim1), lim1);
   double d1 = lt1 - o1;
@@ -202,7 +205,7 @@ __device__ inline double psor_row(const RowIO& R, const Vel& V, int p, int a, in
   }
   double lim2 = sqrt(smax(0.0, mf * mf - lt1 * lt1));
   double w2 = dot(t2, vrel) + cfm * lt2;
-  double d2_ = -(omega / R.r(R_GT2, p)) * w2;
+  double d2_ = -R.r(R_GT2, p) * w2;
   double o2 = lt2;
   lt2 = smin(smax(o2 + d2_, -lim2), lim2);
   double d2 = lt2 - o2;
@@ -426,6 +429,7 @@ struct NscView {
 struct TeamDesc {
   int b0, nb, first, count;
   unsigned int* bar;  // 4 words: full-team count/gen, subset count/gen
+  long long* t_ns;    // optional: the team's device time for the launch
 };
 
 void nsc_set_smem();

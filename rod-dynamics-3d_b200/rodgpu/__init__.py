@@ -78,7 +78,7 @@ ABI_SYMBOLS = [
     "rg_batch_set_bodies", "rg_batch_set_state", "rg_batch_get_state", "rg_batch_step",
     "rg_batch_set_mlp", "rg_mlp_grad", "rg_batch_size", "rg_batch_member", "rg_batch_last_error",
     "rg_batch_set_schedule", "rg_batch_get_schedule", "rg_batch_autotune",
-    "rg_batch_set_state_all", "rg_batch_get_state_all", "rg_batch_get_costs",
+    "rg_batch_set_state_all", "rg_batch_get_state_all", "rg_batch_get_costs", "rg_batch_get_team_times",
 ]
 
 
@@ -143,6 +143,8 @@ def lib():
                                         ctypes.POINTER(ctypes.c_int), dp]
         L.rg_batch_set_state_all.argtypes = [P, dp, dp, dp, dp]
         L.rg_batch_get_costs.argtypes = [P, dp, ctypes.POINTER(ctypes.c_int)]
+        L.rg_batch_get_team_times.argtypes = [P, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                              ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.rg_batch_get_state_all.argtypes = [P, dp, dp, dp, dp]
         _lib = L
     return _lib
@@ -479,6 +481,18 @@ class Batch:
         t = np.zeros(len(self.cfgs), np.int32)
         self._check(self._lib.rg_batch_get_costs(self._h, ptr(c), ptr(t, ctypes.c_int)), "batch_get_costs")
         return c, t
+
+    def team_times(self):
+        """Per team of the last launch: (device ms, blocks, members)."""
+        cap = 4096
+        ms = np.zeros(cap)
+        nb = np.zeros(cap, np.int32)
+        nm = np.zeros(cap, np.int32)
+        nt = ctypes.c_int()
+        self._check(self._lib.rg_batch_get_team_times(self._h, ptr(ms), ptr(nb, ctypes.c_int), ptr(nm, ctypes.c_int),
+                                                      cap, ctypes.byref(nt)), "batch_get_team_times")
+        k = min(nt.value, cap)
+        return ms[:k], nb[:k], nm[:k]
 
     def autotune(self, candidates=(0, 1024, 2048, 4096, 8192), trial_steps=10):
         c = (ctypes.c_int * len(candidates))(*candidates)
