@@ -3,7 +3,7 @@ plain GPU PSOR.
 
 Headline (default workload 'batch'): the NSC half of the uneven-batch
 workload - 128 independent periodic systems, N log-uniform in [500, 20000]
-(610,790 rods in total), aspect ratio 5/10/20/40 (L=1, d=1/AR), phi ~
+(662,433 rods in total for seed 1), aspect ratio 5/10/20/40 (L=1, d=1/AR), phi ~
 U[0.05, 0.25] capped at 1.6/AR (isotropic RSA limit), mu ~ U[0, 1], PSOR
 omega=1, tol 1e-6, max 500 sweeps, dt=5e-4, no gravity, no damping - run as
 ONE persistent CUDA-graph launch per call with the learned warm start
@@ -236,9 +236,10 @@ def run_ours(args, rank, world):
     params, train = train_network(rodgpu, args)
     single = plain_single(rodgpu, args)
 
-    # schedule candidates: multiples of the rods per block of an even split
+    # schedule candidates: the balanced plan, and multiples of the rods per
+    # block of an even split
     r0 = n_total / 148.0
-    cands = (0,) + tuple(int(r0 * f) for f in (0.5, 0.75, 1.0, 1.5, 2.0, 3.0))
+    cands = (-1, 0) + tuple(int(r0 * f) for f in (0.5, 0.75, 1.0, 1.5, 2.0, 3.0))
     plain = load_batch(rodgpu, items, "cache")
     best_plain, _ = plain.autotune(candidates=cands, trial_steps=20)
     res_plain = time_batch(plain, n_total, args)

@@ -334,6 +334,11 @@ const char* rg_batch_last_error(const rg_batch* b);
  * teams (R = rods_per_block; 0 = all single-block).  A member's work is its
  * rod count until a call has timed its steps on the device, then that
  * measured cost converted to rods at the batch's mean cost per rod.
+ * R = -1: balanced plan - each member's step on nb blocks is modelled as
+ * s + p / nb (+ a measured team overhead for nb > 1) from its timed
+ * single-block solves (s) and the rest of its single-block step (p), and
+ * the smallest makespan that fits the blocks is chosen (all single-block
+ * until every member has been timed on one block).
  * use_graph: replay the launch from a CUDA graph. */
 int rg_batch_set_schedule(rg_batch* b, int rods_per_block, int use_graph);
 int rg_batch_get_schedule(const rg_batch* b, int* rods_per_block, int* grid,
@@ -347,9 +352,9 @@ int rg_batch_get_costs(const rg_batch* b, double* cost_ms, int* team_blocks);
 int rg_batch_get_team_times(const rg_batch* b, double* ms, int* blocks, int* members, int cap,
                             int* nteams);
 /* Autotuner: measures every member's step cost (all single-block), then
- * times trial_steps steps per candidate R after two untimed steps, from the
- * current state (state put back after each trial), and selects the fastest;
- * ms_out (optional) gets n_cand times. */
+ * times trial_steps steps per candidate R (-1: balanced) after two untimed
+ * steps, from the current state (state put back after each trial), and
+ * selects the fastest; ms_out (optional) gets n_cand times. */
 int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand,
                       int trial_steps, int* best, double* ms_out);
 

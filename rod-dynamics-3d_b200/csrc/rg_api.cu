@@ -259,12 +259,17 @@ __global__ void k_ctl_reset(Ctl* const* ctls, int n) {
     c->row_sweeps = 0;
     c->contact_steps = 0;
     c->member_ns = 0;
+    c->serial_ns = 0;
+    c->det_valid = 0;
     c->bar_count = 0;
   }
 }
 
 __global__ void k_ctl_zero_time(Ctl* const* ctls, int n) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) ctls[k]->member_ns = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    ctls[k]->member_ns = 0;
+    ctls[k]->serial_ns = 0;
+  }
 }
 
 void ctl_zero_time_launch(Ctl* const* d_ctls, int n, cudaStream_t st) {
@@ -624,6 +629,8 @@ cudaError_t reset_call_ctl(rg_system* s, const Snapshot& sn) {
   h->row_sweeps = 0;
   h->contact_steps = 0;
   h->member_ns = 0;
+  h->serial_ns = 0;
+  h->det_valid = 0;
   h->bar_count = 0;
   return cudaMemcpyAsync(s->d_ctl, h, s->ctl_bytes, cudaMemcpyHostToDevice, s->stream);
 }

@@ -16,7 +16,11 @@
 // measured cost in rod units.  Members of at least 1.5 R work units (R =
 // rods per block) get a team of round(work/R) blocks to themselves; the rest
 // share single-block teams, assigned longest-first to the least-loaded
-// block.  rg_batch_autotune first measures the costs, then times a few R on
+// block.  The balanced plan (R = -1) models each member's step on a team of
+// nb blocks as s + p / nb (+ a team overhead when nb > 1), from its measured
+// time in the single-block solves (s) and the rest of its single-block step
+// (p), and finds the smallest makespan that fits the blocks.
+// rg_batch_autotune first measures the costs, then times a few schedules on
 // the live systems (from a snapshot, restored afterwards) and keeps the
 // fastest.  The schedule changes time only: every member's results are the
 // same for any schedule.
@@ -38,7 +42,7 @@ struct rg_batch {
   cudaStream_t stream = nullptr;
   int coop_blocks = 0;
   // schedule
-  int rods_per_block = 0;  // 0: every NSC member in single-block teams
+  int rods_per_block = 0;  // 0: every NSC member in single-block teams; -1: balanced
   bool use_graph = true;
   bool plan_dirty = true;
   std::vector<TeamDesc> teams;
@@ -59,6 +63,10 @@ struct rg_batch {
   // measured cost per member: block-milliseconds per step (0: not measured)
   std::vector<double> cost;
   std::vector<int> team_nb;  // blocks of the member's team in the last plan
+  // balanced-plan model per member (ms per step): single-block solves and
+  // the rest of a single-block step; team overhead of a multi-block team
+  std::vector<double> ser, par;
+  double team_ms = 0.05;
   bool cost_frozen = false;  // autotuner trials compare schedules on one cost model
   // control plane: copy segments, member control blocks gathered into one
   // device buffer and one page-locked host buffer (control words + wn)
@@ -149,11 +157,122 @@ std::vector<double> work_of(const rg_batch* b, const std::vector<int>& which) {
   return w;
 }
 
+// Packs `small` (sorted by decreasing w) longest-first onto nbins blocks.
+void pack_lpt(const std::vector<int>& small, const std::vector<double>& w, int nbins,
+              std::vector<std::vector<int>>& bins) {
+  bins.assign(nbins, {});
+  std::vector<double> load(nbins, 0.0);
+  for (int k : small) {
+    int m = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    bins[m].push_back(k);
+    load[m] += w[k];
+  }
+}
+
+// Blocks needed for makespan M (member k on nb blocks: ser + par / nb, plus
+// team_ms when nb > 1; single-block members first-fit into blocks of
+// capacity M); nb_out gets each large member's team size.  Returns a count
+// above the budget when M is not reachable.
+long long balanced_blocks(const rg_batch* b, const std::vector<int>& order, double M, int budget,
+                          std::vector<int>* nb_out) {
+  long long blocks = 0;
+  std::vector<double> bins;
+  for (int k : order) {
+    const double w1 = b->ser[k] + b->par[k];
+    if (w1 <= M) {
+      bool placed = false;
+      for (double& l : bins)
+        if (l + w1 <= M) {
+          l += w1;
+          placed = true;
+          break;
+        }
+      if (!placed) bins.push_back(w1);
+      if (nb_out) (*nb_out)[k] = 1;
+      continue;
+    }
+    const double room = M - b->ser[k] - b->team_ms;
+    if (room <= 0.0) return (long long)budget + 1;
+    const long long nb = std::max<long long>(2, (long long)std::ceil(b->par[k] / room));
+    if (nb > budget) return (long long)budget + 1;
+    blocks += nb;
+    if (nb_out) (*nb_out)[k] = (int)nb;
+  }
+  return blocks + (long long)bins.size();
+}
+
+// Balanced plan: the smallest makespan whose teams fit the blocks (bisection
+// on M), then the single-block members packed over all remaining blocks.
+// Returns false when a member has no measured cost yet.
+bool plan_balanced(rg_batch* b, const std::vector<int>& which, std::vector<TeamDesc>& teams,
+                   std::vector<int>& members, int& grid) {
+  const int budget = b->coop_blocks;
+  double sum = 0.0, lo = 0.0, hi = 0.0;
+  for (int k : which) {
+    if (!(b->par[k] > 0.0)) return false;
+    sum += b->ser[k] + b->par[k];
+    lo = std::max(lo, b->ser[k]);
+    hi = std::max(hi, b->ser[k] + b->par[k]);
+  }
+  std::vector<int> order(which);
+  std::sort(order.begin(), order.end(), [&](int x, int y) {
+    const double wx = b->ser[x] + b->par[x], wy = b->ser[y] + b->par[y];
+    return wx != wy ? wx > wy : x < y;
+  });
+  lo = std::max(lo, sum / budget);
+  hi = std::max(hi, sum);  // one block holds everything
+  if (balanced_blocks(b, order, lo, budget, nullptr) > budget) {
+    for (int it = 0; it < 48 && hi - lo > 1e-6 * hi; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      if (balanced_blocks(b, order, mid, budget, nullptr) <= budget) hi = mid;
+      else lo = mid;
+    }
+  } else {
+    hi = lo;
+  }
+  std::vector<int> nb(b->n, 1);
+  balanced_blocks(b, order, hi, budget, &nb);
+  teams.clear();
+  members.clear();
+  int b0 = 0;
+  std::vector<int> small;
+  for (int k : order) {
+    if (nb[k] > 1) {
+      teams.push_back(TeamDesc{b0, nb[k], (int)members.size(), 1, nullptr});
+      members.push_back(k);
+      b0 += nb[k];
+    } else {
+      small.push_back(k);
+    }
+  }
+  if (!small.empty()) {
+    std::vector<double> w(b->n, 0.0);
+    for (int k : small) w[k] = b->ser[k] + b->par[k];
+    std::vector<std::vector<int>> bins;
+    pack_lpt(small, w, std::min<int>((int)small.size(), std::max(1, budget - b0)), bins);
+    for (auto& bin : bins) {
+      teams.push_back(TeamDesc{b0, 1, (int)members.size(), (int)bin.size(), nullptr});
+      for (int k : bin) members.push_back(k);
+      ++b0;
+    }
+  }
+  grid = b0;
+  for (const TeamDesc& t : teams)
+    for (int m = t.first; m < t.first + t.count; ++m) b->team_nb[members[m]] = t.nb;
+  return true;
+}
+
 // Team plan for the NSC members in `which` with R (work in rod units) per
 // block: members of at least 1.5 R get round(work / R) blocks, the rest are
-// packed longest-first onto the least-loaded single blocks.
+// packed longest-first onto the least-loaded single blocks.  R = -1: the
+// balanced plan once every member has been timed on one block (all
+// single-block before, which times them).
 void plan(rg_batch* b, const std::vector<int>& which, int R, std::vector<TeamDesc>& teams,
           std::vector<int>& members, int& grid) {
+  if (R < 0) {
+    if (plan_balanced(b, which, teams, members, grid)) return;
+    R = 0;
+  }
   teams.clear();
   members.clear();
   const int budget = b->coop_blocks;
@@ -433,6 +552,7 @@ int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after =
     total_ms += ms;
     const long long launches = g_launches - l0;
     std::vector<int> again;
+    std::vector<double> over;  // team overhead samples of multi-block members
     for (int k : todo) {
       rg_system* s = b->sys[k];
       s->last_call_ms = ms;
@@ -442,14 +562,29 @@ int batch_call(rg_batch* b, int nsteps, rg_step_stats* per, bool restore_after =
         // block-ms per step, averaged with the previous estimate: list
         // rebuilds and steps that run to the sweep limit make single calls
         // noisy
-        const double c = 1e-6 * (double)s->h_ctl->member_ns / nsteps * b->team_nb[k];
+        const int nb = b->team_nb[k];
+        const double t = 1e-6 * (double)s->h_ctl->member_ns / nsteps;
+        const double sv = std::min(t, 1e-6 * (double)s->h_ctl->serial_ns / nsteps);
+        const double c = t * nb;
         b->cost[k] = b->cost[k] > 0 ? 0.5 * (b->cost[k] + c) : c;
+        b->ser[k] = b->ser[k] > 0 ? 0.5 * (b->ser[k] + sv) : sv;
+        if (nb == 1) {
+          const double p = std::max(1e-6, t - sv);
+          b->par[k] = b->par[k] > 0 ? 0.5 * (b->par[k] + p) : p;
+        } else if (b->par[k] > 0) {
+          over.push_back(t - sv - b->par[k] / nb);
+        }
       }
       if (!err) continue;
       bool retry = false;
       int rc = resolve_call(s, sn[k], err, &retry);
       if (rc != RG_OK) return bfail(b, rc, "member " + std::to_string(k) + ": " + s->err_text);
       again.push_back(k);
+    }
+    if (!over.empty()) {
+      std::nth_element(over.begin(), over.begin() + over.size() / 2, over.end());
+      const double m = std::min(1.0, std::max(0.0, over[over.size() / 2]));
+      b->team_ms = 0.5 * (b->team_ms + m);
     }
     todo.swap(again);
   }
@@ -504,6 +639,8 @@ int rg_batch_create(const rg_config* cfgs, int n_systems, rg_batch** out) {
   }
   b->coop_blocks = b->sys[0]->coop_blocks;
   b->cost.assign(b->n, 0.0);
+  b->ser.assign(b->n, 0.0);
+  b->par.assign(b->n, 0.0);
   b->team_nb.assign(b->n, 1);
   *out = b;
   return RG_OK;
@@ -634,7 +771,7 @@ int rg_batch_set_mlp(rg_batch* b, const float* params, size_t n) {
 }
 
 int rg_batch_set_schedule(rg_batch* b, int rods_per_block, int use_graph) {
-  if (!b || rods_per_block < 0) return RG_ERR_ARG;
+  if (!b || rods_per_block < -1) return RG_ERR_ARG;
   b->rods_per_block = rods_per_block;
   b->use_graph = use_graph != 0;
   b->plan_dirty = true;
@@ -688,7 +825,7 @@ int rg_batch_autotune(rg_batch* b, const int* candidates, int n_cand, int trial_
                       double* ms_out) {
   if (!b || !candidates || n_cand <= 0 || trial_steps <= 0) return RG_ERR_ARG;
   for (int c = 0; c < n_cand; ++c)
-    if (candidates[c] < 0) return RG_ERR_ARG;
+    if (candidates[c] < -1) return RG_ERR_ARG;
   // cost model first: every member's own step time on the device, measured
   // with all members in single-block teams
   rg_batch_set_schedule(b, 0, b->use_graph);

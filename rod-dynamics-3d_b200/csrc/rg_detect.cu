@@ -361,6 +361,8 @@ cudaError_t detector_alloc(rg_system* s) {
     d.near_skin = (c.near_skin_pct > 0 ? 0.01 * c.near_skin_pct : (d.all_pairs ? 0.5 : 0.05)) * d.skin;
     if ((e = cudaMalloc(&d.near, sizeof(int2) * (size_t)n * d.maxnb))) return e;
     if ((e = cudaMalloc(&d.ref2, sizeof(double) * 6 * (size_t)n))) return e;
+    if ((e = cudaMalloc(&d.moved, (size_t)n))) return e;
+    if ((e = cudaMemset(d.moved, 1, (size_t)n))) return e;
   }
   DetDev hd{};
   hd.grid = gd;
@@ -374,7 +376,7 @@ void detector_free(rg_system* s) {
   cudaFree(d.nbr_cnt); cudaFree(d.nbr); cudaFree(d.ref); cudaFree(d.seg);
   cudaFree(d.cell_of); cudaFree(d.cell_cnt); cudaFree(d.cell_start); cudaFree(d.cell_fill);
   cudaFree(d.cell_rods); cudaFree(d.hit_cnt); cudaFree(d.hit_off); cudaFree(d.hit_mask);
-  cudaFree(d.near); cudaFree(d.ref2);
+  cudaFree(d.near); cudaFree(d.ref2); cudaFree(d.moved);
   d = Detector();
 }
 

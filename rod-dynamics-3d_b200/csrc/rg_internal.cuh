@@ -44,12 +44,14 @@ struct Ctl {
   double jn_sum, jt_sum, pe;
   long long row_sweeps; // Σ contacts x sweeps (cumulative)
   long long member_ns;  // device time of this system's steps in the call (batch cost model)
+  long long serial_ns;  // of which in the single-block solves (no team speed-up)
   long long contact_steps;  // Σ velocity-solve contacts over steps
   int vel_contacts;     // NSC: contacts of the last velocity solve (lastHitCount)
   int prof_phases;      // 1: the persistent step records phase times
   long long phase_ns[12];  // persistent-step phase time accumulators
   int rec_n;            // MLP records stored
-  int pad;
+  int det_valid;        // 1: the near-pair hit bits hold the position-level
+                        // detection of this call's last step
   unsigned int bar_count, bar_gen;  // grid barrier
   double res_sweep[1];  // per-sweep residual slots follow (velocity_iters)
 };
@@ -79,6 +81,9 @@ struct Detector {
   int2* near = nullptr;           // n * maxnb
   double* ref2 = nullptr;         // 6n
   double near_skin = 0;
+  // 1: rod moved (position projection or periodic wrap) since the
+  // position-level detection of the step; cleared by the position update
+  unsigned char* moved = nullptr;  // n
   int* hit_cnt = nullptr;         // n+1
   int* hit_off = nullptr;         // n+1
   unsigned long long* hit_mask = nullptr;  // n * words
@@ -311,7 +316,7 @@ void copy_segments_launch(const CopySeg* d_segs, int n, cudaStream_t st);
 // Zeroes the per-call counters (as reset_call_ctl does from a snapshot)
 // of n systems' control blocks on the device.
 void ctl_reset_launch(rg::Ctl* const* d_ctls, int n, cudaStream_t st);
-void ctl_zero_time_launch(rg::Ctl* const* d_ctls, int n, cudaStream_t st);  // member_ns only
+void ctl_zero_time_launch(rg::Ctl* const* d_ctls, int n, cudaStream_t st);  // member_ns, serial_ns
 void finish_snapshot(rg_system* s, Snapshot& sn);  // after the stream synchronised
 cudaError_t restore_snapshot(rg_system* s, const Snapshot& sn);
 cudaError_t reset_call_ctl(rg_system* s, const Snapshot& sn);

@@ -70,8 +70,10 @@ __device__ inline void load_b(const __nv_bfloat16* W, int ldk, int nt, int kt, i
   b1 = *reinterpret_cast<const unsigned*>(row + 8);
 }
 
-// One hidden layer 128 -> 128: a[kt] (4 regs each, 8 k-tiles) -> out a.
-__device__ inline void hidden_layer(unsigned (&a)[8][4], const __nv_bfloat16* W, const float* bias, int lane) {
+// One hidden layer 128 -> 128: a[kt] (4 regs each, 8 k-tiles) -> out a;
+// W row-major [n][k] with leading dimension ldw.
+__device__ inline void hidden_layer(unsigned (&a)[8][4], const __nv_bfloat16* W, int ldw, const float* bias,
+                                    int lane) {
   const int t = lane & 3;
   unsigned na[8][4];
 #pragma unroll
@@ -85,7 +87,7 @@ __device__ inline void hidden_layer(unsigned (&a)[8][4], const __nv_bfloat16* W,
 #pragma unroll
       for (int kt = 0; kt < 8; ++kt) {
         unsigned b0, b1;
-        load_b(W, kMlpH, nt, kt, lane, b0, b1);
+        load_b(W, ldw, nt, kt, lane, b0, b1);
         mma_bf16(acc[h], a[kt][0], a[kt][1], a[kt][2], a[kt][3], b0, b1);
       }
     }
@@ -100,13 +102,22 @@ __device__ inline void hidden_layer(unsigned (&a)[8][4], const __nv_bfloat16* W,
     for (int r = 0; r < 4; ++r) a[kk][r] = na[kk][r];
 }
 
-// Evaluates the MLP for rows row0..row0+15 of feat (float, [8][ld]) and
-// writes the unscaled outputs times out_scale to out ([3][ld]); rows >= n
-// are ignored.  All 32 lanes of the warp must call it.
-__device__ inline void mlp_warp(const MlpDev& M, const float* feat, int ld, int row0, int n, float* out,
-                                int lane) {
+// Small parameters of one evaluation: biases, b4 padded to 8 with zeros,
+// input normalisation and output scales (global parameter vector or a
+// staged shared-memory copy).
+struct MlpSmall {
+  const float *b1, *b2, *b3, *b4, *in_mean, *in_scale, *out_scale;
+};
+__device__ inline MlpSmall mlp_small_global(const float* P) {
+  return MlpSmall{P + kOffB1, P + kOffB2, P + kOffB3, P + kOffB4, P + kOffInMean, P + kOffInScale,
+                  P + kOffOutScale};
+}
+
+// Layer 1 (8 -> 128, SiLU) for rows row0..row0+15 of feat (float, [8][ld]);
+// rows >= n read as zero.  w1 row-major [128][k], leading dimension ld1.
+__device__ inline void mlp_layer1(const __nv_bfloat16* w1, int ld1, const MlpSmall& q, const float* feat, int ld,
+                                  int row0, int n, int lane, unsigned (&a)[8][4]) {
   const int g = lane >> 2, t = lane & 3;
-  const float* P = M.p;
   // layer 1 input fragment: X (16 rows x 16 k, inputs 8..15 are zero)
   unsigned x0, x1;
   {
@@ -117,23 +128,22 @@ __device__ inline void mlp_warp(const MlpDev& M, const float* feat, int ld, int 
         int k = 2 * t + cc;
         int r = rows[rr];
         float f = r < n ? feat[(size_t)k * ld + r] : 0.0f;
-        v[rr * 2 + cc] = (f - P[kOffInMean + k]) * P[kOffInScale + k];
+        v[rr * 2 + cc] = (f - q.in_mean[k]) * q.in_scale[k];
       }
     }
     x0 = pack_bf16(v[0], v[1]);
     x1 = pack_bf16(v[2], v[3]);
   }
-  unsigned a[8][4];
 #pragma unroll
   for (int kk = 0; kk < 8; ++kk) {
     float acc[2][4];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int nt = 2 * kk + h;
-      const float bl = P[kOffB1 + nt * 8 + 2 * t], bh = P[kOffB1 + nt * 8 + 2 * t + 1];
+      const float bl = q.b1[nt * 8 + 2 * t], bh = q.b1[nt * 8 + 2 * t + 1];
       acc[h][0] = bl; acc[h][1] = bh; acc[h][2] = bl; acc[h][3] = bh;
       unsigned b0, b1;
-      load_b(M.w1, kW1Pad, nt, 0, lane, b0, b1);
+      load_b(w1, ld1, nt, 0, lane, b0, b1);
       mma_bf16(acc[h], x0, x1, 0u, 0u, b0, b1);
     }
     a[kk][0] = pack_bf16(silu(acc[0][0]), silu(acc[0][1]));
@@ -141,17 +151,23 @@ __device__ inline void mlp_warp(const MlpDev& M, const float* feat, int ld, int 
     a[kk][2] = pack_bf16(silu(acc[1][0]), silu(acc[1][1]));
     a[kk][3] = pack_bf16(silu(acc[1][2]), silu(acc[1][3]));
   }
-  hidden_layer(a, M.w2, P + kOffB2, lane);
-  hidden_layer(a, M.w3, P + kOffB3, lane);
+}
+
+// Output layer (128 -> 3): writes the outputs times out_scale to out
+// ([3][ld]); rows >= n are skipped.  w4 row-major [8][128], leading
+// dimension ld4 (rows 3..7 zero).
+__device__ inline void mlp_layer4(const unsigned (&a)[8][4], const __nv_bfloat16* w4, int ld4, const MlpSmall& q,
+                                  float* out, int ld, int row0, int n, int lane) {
+  const int g = lane >> 2, t = lane & 3;
   float acc[4];
   {
-    const float bl = 2 * t < kMlpOut ? P[kOffB4 + 2 * t] : 0.0f;
-    const float bh = 2 * t + 1 < kMlpOut ? P[kOffB4 + 2 * t + 1] : 0.0f;
+    const float bl = 2 * t < kMlpOut ? q.b4[2 * t] : 0.0f;
+    const float bh = 2 * t + 1 < kMlpOut ? q.b4[2 * t + 1] : 0.0f;
     acc[0] = bl; acc[1] = bh; acc[2] = bl; acc[3] = bh;
 #pragma unroll
     for (int kt = 0; kt < 8; ++kt) {
       unsigned b0, b1;
-      load_b(M.w4, kMlpH, 0, kt, lane, b0, b1);
+      load_b(w4, ld4, 0, kt, lane, b0, b1);
       mma_bf16(acc, a[kt][0], a[kt][1], a[kt][2], a[kt][3], b0, b1);
     }
   }
@@ -162,8 +178,77 @@ __device__ inline void mlp_warp(const MlpDev& M, const float* feat, int ld, int 
     if (r >= n) continue;
     for (int cc = 0; cc < 2; ++cc) {
       int o = 2 * t + cc;
-      if (o < kMlpOut) out[(size_t)o * ld + r] = acc[rr * 2 + cc] * P[kOffOutScale + o];
+      if (o < kMlpOut) out[(size_t)o * ld + r] = acc[rr * 2 + cc] * q.out_scale[o];
     }
+  }
+}
+
+// Evaluates the MLP for rows row0..row0+15 of feat (float, [8][ld]) and
+// writes the unscaled outputs times out_scale to out ([3][ld]); rows >= n
+// are ignored.  All 32 lanes of the warp must call it.  Weights are read
+// from global memory.
+__device__ inline void mlp_warp(const MlpDev& M, const float* feat, int ld, int row0, int n, float* out,
+                                int lane) {
+  const MlpSmall q = mlp_small_global(M.p);
+  unsigned a[8][4];
+  mlp_layer1(M.w1, kW1Pad, q, feat, ld, row0, n, lane, a);
+  hidden_layer(a, M.w2, kMlpH, q.b2, lane);
+  hidden_layer(a, M.w3, kMlpH, q.b3, lane);
+  mlp_layer4(a, M.w4, kMlpH, q, out, ld, row0, n, lane);
+}
+
+// ---- shared-memory staging of the weights ---------------------------------
+// Padded row strides: eight rows of a B fragment fall in distinct banks.
+constexpr int kW1Ld = kW1Pad + 8;          // 24 (48 B rows)
+constexpr int kWhLd = kMlpH + 8;           // 136 (272 B rows)
+constexpr int kStageW1 = kMlpH * kW1Ld;    // elements
+constexpr int kStageW4 = kW4Pad * kWhLd;
+constexpr int kStageWh = kMlpH * kWhLd;    // one hidden layer
+constexpr int kStageFloats = 3 * kMlpH + 8 + 8 + 8 + 8;  // b1 b2 b3 b4(8) mean scale outscale(8)
+// bytes of the small part (W1, W4, floats)
+constexpr int kStageSmallBytes = 2 * (kStageW1 + kStageW4) + 4 * kStageFloats;
+
+struct MlpStage {
+  __nv_bfloat16* w1;  // kStageW1
+  __nv_bfloat16* w4;  // kStageW4
+  float* f;           // kStageFloats
+  __device__ MlpSmall small() const {
+    return MlpSmall{f, f + kMlpH, f + 2 * kMlpH, f + 3 * kMlpH, f + 3 * kMlpH + 8, f + 3 * kMlpH + 16,
+                    f + 3 * kMlpH + 24};
+  }
+};
+// Carves the small part from a 16-byte aligned buffer of kStageSmallBytes.
+__device__ inline MlpStage mlp_stage_at(void* buf) {
+  MlpStage s;
+  s.w1 = reinterpret_cast<__nv_bfloat16*>(buf);
+  s.w4 = s.w1 + kStageW1;
+  s.f = reinterpret_cast<float*>(s.w4 + kStageW4);
+  return s;
+}
+
+// Block-cooperative copy of rows x cols BF16 (cols a multiple of 8, both
+// 16-byte aligned) into a padded shared-memory matrix.
+__device__ inline void stage_bf16(__nv_bfloat16* dst, int ldd, const __nv_bfloat16* src, int rows, int cols) {
+  const int vpr = cols / 8;
+  for (int v = threadIdx.x; v < rows * vpr; v += blockDim.x) {
+    const int r = v / vpr, c = v - r * vpr;
+    *reinterpret_cast<uint4*>(dst + (size_t)r * ldd + c * 8) =
+        *reinterpret_cast<const uint4*>(src + (size_t)r * cols + c * 8);
+  }
+}
+// Block-cooperative copy of W1, W4 and the small parameters.
+__device__ inline void stage_small(const MlpStage& s, const MlpDev& M) {
+  stage_bf16(s.w1, kW1Ld, M.w1, kMlpH, kW1Pad);
+  stage_bf16(s.w4, kWhLd, M.w4, kW4Pad, kMlpH);
+  const float* P = M.p;
+  for (int i = threadIdx.x; i < kStageFloats; i += blockDim.x) {
+    float v = 0.0f;
+    if (i < 3 * kMlpH) v = P[(i < kMlpH ? kOffB1 : i < 2 * kMlpH ? kOffB2 - kMlpH : kOffB3 - 2 * kMlpH) + i];
+    else if (i < 3 * kMlpH + 8) v = i - 3 * kMlpH < kMlpOut ? P[kOffB4 + i - 3 * kMlpH] : 0.0f;
+    else if (i < 3 * kMlpH + 16) v = P[kOffInMean + i - 3 * kMlpH - 8];
+    else if (i < 3 * kMlpH + 24) v = P[kOffInScale + i - 3 * kMlpH - 16];
+    else v = i - 3 * kMlpH - 24 < kMlpOut ? P[kOffOutScale + i - 3 * kMlpH - 24] : 0.0f;
+    s.f[i] = v;
   }
 }
 

@@ -98,8 +98,11 @@ struct PhaseClock {
   }
 };
 
+// Dynamic shared memory of the persistent step: the small-solve arrays, or
+// the list-build tiles while a rebuild runs (phases never overlap).
+extern __shared__ __align__(16) unsigned char nsc_dyn_smem[];
+
 struct SmemNsc {
-  BuildSmem build;
   double red_d[32];
   int red_i[32];
   int scan_w[32];
@@ -228,7 +231,7 @@ __device__ __noinline__ bool rebuild_phase(const Team& T, const NscView& V, Smem
     // crowded cells: the block splits the pairs of one home cell at a time
     for (int cell = rank; cell < g.ncells; cell += T.nb)
       build_cell_pairs(V.seg, g, V.box, invL, V.cell_start, V.cell_rods, V.margin, V.skin, V.all_pairs,
-                       V.nbr_cnt, V.nbr, V.maxnb, cell, sm.build, overflow);
+                       V.nbr_cnt, V.nbr, V.maxnb, cell, *reinterpret_cast<BuildSmem*>(nsc_dyn_smem), overflow);
   }
   if (!team_sync(T)) return false;
   for (int i = tid; i < n; i += TS) {
@@ -260,7 +263,7 @@ __device__ __noinline__ bool rebuild_phase(const Team& T, const NscView& V, Smem
 // near list is the exact one.  Contacts come out in near-list order, which
 // is (a, b) order.
 __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double delta, SmemNsc& sm,
-                                        bool lists_rebuilt) {
+                                        bool lists_rebuilt, bool position_level) {
   Ctl* ctl = V.ctl;
   const int n = V.st.n;
   const int rank = T.rank();
@@ -318,19 +321,45 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
   const int plo = rank * segp < P ? rank * segp : P;
   const int phi = plo + segp < P ? plo + segp : P;
   unsigned long long* bits = V.mask;  // one bit per near pair
-  for (int w = (plo >> 6) + threadIdx.x; w < ((phi + 63) >> 6); w += blockDim.x) bits[w] = 0ull;
-  __syncthreads();
   const double* im = V.st.inv_mass;
   int mine = 0;
-  for (int p = plo + threadIdx.x; p < phi; p += blockDim.x) {
-    const int2 pr = V.near[p];
-    if (!(im[pr.x] > 0.0) && !(im[pr.y] > 0.0)) continue;
-    const Seg A = V.seg[pr.x], B = V.seg[pr.y];
-    if (seg_far(A, B, prefilter_offset(A, B, V.box, invL, mode), A.r + B.r + delta)) continue;
-    const Narrow nr = narrow_pair(A, B, V.box);
-    if (contact_test(nr.d2, A.r + B.r, delta)) {
-      atomicOr(&bits[p >> 6], 1ull << (p & 63));
-      ++mine;
+  // The velocity-level detection follows the previous step's position-level
+  // one over the same near list; only the position projection and the
+  // periodic wrap moved rods in between.  A pair of two unmoved rods has
+  // bit-identical segments, so its hit bit carries over; the other pairs
+  // are tested again.
+  const bool carry = !position_level && !rebuild_near && V.moved && *(volatile int*)&ctl->det_valid;
+  if (carry) {
+    for (int p = plo + threadIdx.x; p < phi; p += blockDim.x) {
+      const int2 pr = V.near[p];
+      const bool was = (bits[p >> 6] >> (p & 63)) & 1ull;
+      bool hit = was;
+      if (V.moved[pr.x] | V.moved[pr.y]) {
+        hit = false;
+        if (im[pr.x] > 0.0 || im[pr.y] > 0.0) {
+          const Seg A = V.seg[pr.x], B = V.seg[pr.y];
+          if (!seg_far(A, B, prefilter_offset(A, B, V.box, invL, mode), A.r + B.r + delta)) {
+            const Narrow nr = narrow_pair(A, B, V.box);
+            hit = contact_test(nr.d2, A.r + B.r, delta);
+          }
+        }
+        if (hit != was) atomicXor(&bits[p >> 6], 1ull << (p & 63));
+      }
+      mine += hit ? 1 : 0;
+    }
+  } else {
+    for (int w = (plo >> 6) + threadIdx.x; w < ((phi + 63) >> 6); w += blockDim.x) bits[w] = 0ull;
+    __syncthreads();
+    for (int p = plo + threadIdx.x; p < phi; p += blockDim.x) {
+      const int2 pr = V.near[p];
+      if (!(im[pr.x] > 0.0) && !(im[pr.y] > 0.0)) continue;
+      const Seg A = V.seg[pr.x], B = V.seg[pr.y];
+      if (seg_far(A, B, prefilter_offset(A, B, V.box, invL, mode), A.r + B.r + delta)) continue;
+      const Narrow nr = narrow_pair(A, B, V.box);
+      if (contact_test(nr.d2, A.r + B.r, delta)) {
+        atomicOr(&bits[p >> 6], 1ull << (p & 63));
+        ++mine;
+      }
     }
   }
   const int bsum = block_reduce_sum_i(mine, sm.red_i);
@@ -356,19 +385,23 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
     }
     run += tot;
   }
-  if (rank == 0 && threadIdx.x == 0) ctl->contacts = total;
+  if (rank == 0 && threadIdx.x == 0) {
+    ctl->contacts = total;
+    ctl->det_valid = position_level ? 1 : 0;
+  }
   if (!team_sync(T)) return -1;
   return total;
 }
 
-__device__ __noinline__ int detect_phase(const Team& T, const NscView& V, double delta, SmemNsc& sm) {
+__device__ __noinline__ int detect_phase(const Team& T, const NscView& V, double delta, SmemNsc& sm,
+                                         bool position_level) {
   Ctl* ctl = V.ctl;
   const int n = V.st.n;
   const int rank = T.rank();
   const bool need = *(volatile int*)&ctl->rebuild ||
                     (!V.all_pairs && *(volatile double*)&ctl->maxdisp >= 0.5 * V.skin * (1.0 - 1e-9));
   if (need && !rebuild_phase(T, V, sm)) return -1;
-  if (V.near) return detect_near(T, V, delta, sm, need);
+  if (V.near) return detect_near(T, V, delta, sm, need, position_level);
   const int seg = (n + T.nb - 1) / T.nb;
   const int lo = rank * seg < n ? rank * seg : n;
   const int hi = lo + seg < n ? lo + seg : n;
@@ -685,6 +718,7 @@ __device__ __noinline__ bool project_rows(const NscView& V, int C, int K, int na
       for (int side = 0; side < 2; ++side) {
         int bd = side ? V.con.b[c] : V.con.a[c];
         if (st.inv_mass[bd] <= 0.0 || V.owner[bd] != c) continue;
+        if (V.moved) V.moved[bd] = 1;
         st.x.st(bd, st.x.ld(bd) + DX.ld(bd));
         d3 th = DT.ld(bd);
         double ang = len(th);
@@ -737,7 +771,11 @@ struct SmallSmem {
   float feat[kMlpIn * kSmallC];      // learned warm start features [8][kSmallC]
   float pred[kMlpOut * kSmallC];     // predicted impulse changes [3][kSmallC]
   int mtile[kSmallC / 16];           // 16-contact tiles that need the network
+  // one hidden layer of the network (the rest is staged in pmax/cmask)
+  alignas(16) __nv_bfloat16 wh[kStageWh];
 };
+static_assert(sizeof(unsigned long long) * 3 * kSmallB >= kStageSmallBytes, "MLP staging space");
+static_assert(sizeof(SmallSmem) >= sizeof(BuildSmem), "list-build tiles share the small-solve memory");
 
 __device__ inline double small_block_max(double v, SmallSmem& S) {
   v = warp_max(v);
@@ -915,9 +953,29 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
       __syncthreads();
       if (want) S.mtile[t >> 4] = 1;
       if (__syncthreads_or(want)) {
-        // one warp per 16 contacts on the tensor cores, then the cone
-        const int row0 = (t >> 5) * 16;
-        if (row0 < C && S.mtile[t >> 5]) mlp_warp(V.mlp, S.feat, kSmallC, row0, C, S.pred, t & 31);
+        // one warp per 16 contacts on the tensor cores, then the cone.  The
+        // weights come from shared memory: W1, W4 and the small parameters
+        // in pmax/cmask (free after colouring and degrees), the hidden
+        // layers one after the other in wh.
+        const MlpStage ms = mlp_stage_at(S.pmax);
+        stage_small(ms, V.mlp);
+        stage_bf16(S.wh, kWhLd, V.mlp.w2, kMlpH, kMlpH);
+        __syncthreads();
+        const int row0 = (t >> 5) * 16, lane = t & 31;
+        const bool mine = row0 < C && S.mtile[t >> 5];
+        const MlpSmall q = ms.small();
+        unsigned a[8][4];
+        if (mine) {
+          mlp_layer1(ms.w1, kW1Ld, q, S.feat, kSmallC, row0, C, lane, a);
+          hidden_layer(a, S.wh, kWhLd, q.b2, lane);
+        }
+        __syncthreads();
+        stage_bf16(S.wh, kWhLd, V.mlp.w3, kMlpH, kMlpH);
+        __syncthreads();
+        if (mine) {
+          hidden_layer(a, S.wh, kWhLd, q.b3, lane);
+          mlp_layer4(a, ms.w4, kWhLd, q, S.pred, kSmallC, row0, C, lane);
+        }
         __syncthreads();
         if (want) mlp_apply(R, S.pred, kSmallC, t, cfg.nsc_mu);
         __syncthreads();
@@ -1104,6 +1162,7 @@ __device__ __noinline__ bool small_project(const NscView& V, int C, SmallSmem& S
     for (int s = t; s < S.nloc; s += blockDim.x) {
       int x = S.body[s];
       if (x < 0 || !S.dyn[s]) continue;
+      if (V.moved) V.moved[x] = 1;
       st.x.st(x, st.x.ld(x) + mk3(DX[s], DX[kSmallB + s], DX[2 * kSmallB + s]));
       d3 th{DX[3 * kSmallB + s], DX[4 * kSmallB + s], DX[5 * kSmallB + s]};
       double ang = len(th);
@@ -1154,14 +1213,16 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
   }
   pc.mark(0);
   // 2) detection, colouring, manifold rows
-  int C = detect_phase(T, V, 0.0, sm);
+  int C = detect_phase(T, V, 0.0, sm, false);
   if (C < 0) return false;
   pc.mark(1);
   const bool small = C <= kSmallC;
   if (small) {
     // colouring, rows, PSOR and warm cache in one block, on chip
     bool ok = true;
+    const unsigned long long ts = (rank == 0 && threadIdx.x == 0) ? gtimer() : 0ull;
     if (rank == 0) ok = small_solve(V, C, S, pc);
+    if (rank == 0 && threadIdx.x == 0) ctl->serial_ns += (long long)(gtimer() - ts);
     if (!ok) atomicOr(&ctl->err, ERR_COLOR);
     pc.mark(10);
     if (!team_sync(T)) return false;
@@ -1201,15 +1262,28 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
       }
       if (V.use_mlp && (W == 0 || *(volatile int*)&ctl->sweeps_last > V.mlp_min_sweeps)) {
         // each warp of the team evaluates tiles of 16 slots on the tensor
-        // cores; its own lanes then apply the tile's predictions
+        // cores; its own lanes then apply the tile's predictions.  Every
+        // block stages the whole network in its (here unused) small-solve
+        // shared memory: W1, W4 and the small parameters in pmax/cmask, W2
+        // in wh, W3 over the rows.
+        const MlpStage ms = mlp_stage_at(S.pmax);
+        __nv_bfloat16* w3s = reinterpret_cast<__nv_bfloat16*>(S.row);
+        stage_small(ms, V.mlp);
+        stage_bf16(S.wh, kWhLd, V.mlp.w2, kMlpH, kMlpH);
+        stage_bf16(w3s, kWhLd, V.mlp.w3, kMlpH, kMlpH);
         __syncthreads();
         if (!team_sync(T)) return false;
+        const MlpSmall q = ms.small();
         const int lane = threadIdx.x & 31, gw = tid >> 5, nw = TS >> 5;
         for (int row0 = gw * 16; row0 < C; row0 += nw * 16) {
           const int p = row0 + (lane & 15);
           const bool want = lane < 16 && p < C && (V.mlp_all || !warm_cached(V, V.order[p], W));
           if (!__ballot_sync(0xffffffffu, want)) continue;  // no row of this tile needs the network
-          mlp_warp(V.mlp, V.feat, V.ccap, row0, C, V.pred, lane);
+          unsigned a[8][4];
+          mlp_layer1(ms.w1, kW1Ld, q, V.feat, V.ccap, row0, C, lane, a);
+          hidden_layer(a, S.wh, kWhLd, q.b2, lane);
+          hidden_layer(a, w3s, kWhLd, q.b3, lane);
+          mlp_layer4(a, ms.w4, kWhLd, q, V.pred, V.ccap, row0, C, lane);
           __syncwarp();
           if (want) mlp_apply(R, V.pred, V.ccap, p, cfg.nsc_mu);
           __syncwarp();
@@ -1265,7 +1339,7 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     for (int k = 0; k < 3; ++k)
       if (V.box.L[k] > 0.0) invL[k] = 1.0 / V.box.L[k];
     for (int i = tid; i < n; i += TS)
-      bad |= position_update_fused(st, i, cfg, V.ref, ref2, n, V.box, invL, V.seg, dmax, dnear);
+      bad |= position_update_fused(st, i, cfg, V.ref, ref2, n, V.box, invL, V.seg, dmax, dnear, V.moved);
     if (bad) atomicOr(&ctl->err, ERR_NONFINITE);
     double bm = block_reduce_max(dmax, sm.red_d);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
@@ -1280,12 +1354,14 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
   pc.mark(5);
   // 5) position projection (nsc_contact.cpp:659-880)
   if (cfg.nsc_position_stabilization) {
-    int C2 = detect_phase(T, V, 0.0, sm);
+    int C2 = detect_phase(T, V, 0.0, sm, true);
     if (C2 < 0) return false;
     pc.mark(6);
     if (C2 <= kSmallC) {
       bool ok = true;
+      const unsigned long long ts = (rank == 0 && threadIdx.x == 0) ? gtimer() : 0ull;
       if (rank == 0) ok = small_project(V, C2, S);
+      if (rank == 0 && threadIdx.x == 0) ctl->serial_ns += (long long)(gtimer() - ts);
       if (!ok) atomicOr(&ctl->err, ERR_COLOR);
       if (!team_sync(T)) return false;
     } else {
@@ -1297,7 +1373,7 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
   }
   // 6) PBC wrap + clear forces (main.cpp:4508-4527); the next step touches
   // rod i from this same thread, so no barrier is needed here.
-  for (int i = tid; i < n; i += TS) wrap_clear_body(st, V.box, i);
+  for (int i = tid; i < n; i += TS) wrap_clear_body(st, V.box, i, V.moved);
   return true;
 }
 
@@ -1370,6 +1446,7 @@ NscView make_view(rg_system* s) {
   V.slot_of = N.slot_of;
   V.near = d.near;
   V.ref2 = d.ref2;
+  V.moved = d.moved;
   V.near_skin = d.near_skin;
   V.feat = s->d_feat;
   V.pred = s->d_pred;

@@ -320,7 +320,7 @@ __device__ inline void free_flight_fused(const State& st, int i, d3 g, double dt
 // returns 1 when the new state is not finite.
 __device__ inline int position_update_fused(const State& st, int i, const rg_config& cfg, const double* ref,
                                             const double* ref2, int n, const Box& box, const double* invL,
-                                            Seg* seg_out, double& dmax, double& dnear) {
+                                            Seg* seg_out, double& dmax, double& dnear, unsigned char* moved) {
   const double dt = cfg.dt;
   const double ld = 1.0 - cfg.lin_damp * dt, ad = 1.0 - cfg.ang_damp * dt;
   d3 v = st.v.ld(i), w = st.w.ld(i);
@@ -346,6 +346,7 @@ __device__ inline int position_update_fused(const State& st, int i, const rg_con
   st.w.st(i, w);
   const Seg s = seg_of(x, q, h, r);
   seg_out[i] = s;
+  if (moved) moved[i] = 0;
   dmax = fmax(dmax, disp_from(s, rf, box, invL));
   if (ref2) dnear = fmax(dnear, disp_from(s, rf2, box, invL));
   return (x.x == x.x && x.y == x.y && x.z == x.z && v.x == v.x) ? 0 : 1;
@@ -364,11 +365,13 @@ __device__ inline void wrap_pos(const Box& box, d3& p) {
   }
 }
 
-__device__ inline void wrap_clear_body(const State& st, const Box& box, int i) {
+__device__ inline void wrap_clear_body(const State& st, const Box& box, int i, unsigned char* moved = nullptr) {
   if (box.pbc) {
-    d3 x = st.x.ld(i);
+    const d3 x0 = st.x.ld(i);
+    d3 x = x0;
     wrap_pos(box, x);
     st.x.st(i, x);
+    if (moved && (x.x != x0.x || x.y != x0.y || x.z != x0.z)) moved[i] = 1;
   }
   st.f.st(i, mk3(0, 0, 0));
   st.tau.st(i, mk3(0, 0, 0));
@@ -410,6 +413,7 @@ struct NscView {
   int* slot_of;  // per-body local slot of the in-block solver (-1 when unused)
   int2* near;    // near list (see Detector); null: test the whole lists
   double* ref2;
+  unsigned char* moved;  // see Detector
   double near_skin;
   // learned warm start: features [8][ccap] and predictions [3][ccap] of the
   // team path, the network, and the record buffers ([n][8], [n][3])

@@ -494,7 +494,9 @@ class Batch:
         k = min(nt.value, cap)
         return ms[:k], nb[:k], nm[:k]
 
-    def autotune(self, candidates=(0, 1024, 2048, 4096, 8192), trial_steps=10):
+    def autotune(self, candidates=(-1, 0, 1024, 2048, 4096, 8192), trial_steps=10):
+        """Times each schedule candidate (rods per block; -1 the balanced
+        plan, 0 all single-block) and keeps the fastest: (best, {R: ms})."""
         c = (ctypes.c_int * len(candidates))(*candidates)
         best = ctypes.c_int()
         ms = np.zeros(len(candidates))

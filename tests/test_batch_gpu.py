@@ -61,7 +61,7 @@ def _check_same(b, alone):
             assert np.array_equal(got[key], st[key]), (k, key)
 
 
-@pytest.mark.parametrize("rods_per_block,graph", [(0, True), (1024, True), (512, False)])
+@pytest.mark.parametrize("rods_per_block,graph", [(0, True), (1024, True), (512, False), (-1, True)])
 def test_batch_equals_members_alone(specs, alone, rods_per_block, graph):
     b = _batch(specs)
     b.set_schedule(rods_per_block, graph)
@@ -79,8 +79,8 @@ def test_batch_autotune_keeps_state(specs, alone):
     b = _batch(specs)
     b.step(15)
     before = [b.get_state(k) for k in range(len(specs))]
-    best, times = b.autotune(candidates=(0, 1024, 4096), trial_steps=5)
-    assert best in (0, 1024, 4096) and all(t > 0 for t in times.values())
+    best, times = b.autotune(candidates=(-1, 0, 1024, 4096), trial_steps=5)
+    assert best in (-1, 0, 1024, 4096) and all(t > 0 for t in times.values())
     for k in range(len(specs)):
         now = b.get_state(k)
         for key in ("x", "q", "v", "w"):

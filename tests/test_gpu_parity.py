@@ -190,3 +190,20 @@ def test_list_rebuild_keeps_exact_contacts():
     a, b = g.get_state(), o.get_state()
     assert rel_err(a["x"], b["x"]) < 1e-9
     assert_contacts_equal(g, o, 0.0)
+
+
+@pytest.mark.parametrize("team", [1, 4])
+def test_nsc_long_call_carries_exact_contacts(team):
+    # many steps in one call: the velocity-level detection reuses the hit
+    # bits of the previous position-level one for rods that neither the
+    # projection nor the periodic wrap moved; fast rods cross the box
+    sc = packed_scene(1500, d=0.05, phi=0.2, seed=16, squeeze=0.97, sigma_v=3.0, sigma_w=2.0)
+    g, o = make_pair(sc, model="nsc", dt=5e-4, nsc_velocity_iters=500, team_blocks=team)
+    sg = g.step(8)
+    so = o.step(8)
+    a, b = g.get_state(), o.get_state()
+    for k in ("x", "q", "v", "w"):
+        assert rel_err(a[k], b[k]) < TOL, k
+    assert sg["psor_sweeps"] == so["psor_sweeps"]
+    assert sg["contacts"] == so["contacts"]
+    assert_contacts_equal(g, o, 0.0)
