@@ -53,6 +53,8 @@ void bind_state(rg_system* s) {
   st.r = p; st.h = p + n; st.mass = p + 2 * n; st.inv_mass = p + 3 * n; st.rest = p + 4 * n;
   st.I = {p + 5 * n, p + 6 * n, p + 7 * n};
   st.Iinv = {p + 8 * n, p + 9 * n, p + 10 * n};
+  st.sbase = b;
+  st.pbase = p;
 }
 
 size_t ctl_size(const rg_config& c) {

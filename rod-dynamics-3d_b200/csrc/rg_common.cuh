@@ -109,6 +109,25 @@ struct State {
   QuatA q;
   const double *r, *h, *mass, *inv_mass, *rest;
   Vec3A I, Iinv;
+  // the buffers behind the component arrays: state (x 0-2, q 3-6, v 7-9,
+  // w 10-12, f 13-15, tau 16-18) and properties (r 0, h 1, mass 2,
+  // inv_mass 3, rest 4, I 5-7, Iinv 8-10), component k at base + k n
+  double* sbase;
+  const double* pbase;
+};
+
+// A system's state addressed from its two buffer bases.  Per-rod loops hold
+// this in three registers instead of re-reading some thirty component
+// pointers from the system's view after every store.
+struct StateBase {
+  double* s;
+  const double* p;
+  int n;
+  __device__ double* c(int k) const { return s + (size_t)k * n; }
+  __device__ const double* pc(int k) const { return p + (size_t)k * n; }
+  __device__ d3 ld3(int k, int i) const { return {c(k)[i], c(k + 1)[i], c(k + 2)[i]}; }
+  __device__ void st3(int k, int i, d3 v) const { c(k)[i] = v.x; c(k + 1)[i] = v.y; c(k + 2)[i] = v.z; }
+  __device__ d3 pld3(int k, int i) const { return {pc(k)[i], pc(k + 1)[i], pc(k + 2)[i]}; }
 };
 
 // Packed per-detection segment record (two 32-byte sectors).

@@ -322,7 +322,9 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
   const int phi = plo + segp < P ? plo + segp : P;
   unsigned long long* bits = V.mask;  // one bit per near pair
   const double* im = V.st.inv_mass;
-  int mine = 0;
+  // the block's words (none for an empty range: plo is then P, whose word
+  // may belong to the block before)
+  const int wlo = plo >> 6, whi = plo < phi ? (phi + 63) >> 6 : wlo;
   // The velocity-level detection follows the previous step's position-level
   // one over the same near list; only the position projection and the
   // periodic wrap moved rods in between.  A pair of two unmoved rods has
@@ -330,14 +332,25 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
   // are tested again.
   const bool carry = !position_level && !rebuild_near && V.moved && *(volatile int*)&ctl->det_valid;
   if (carry) {
-    for (int p = plo + threadIdx.x; p < phi; p += blockDim.x) {
-      const int2 pr = V.near[p];
-      const bool was = (bits[p >> 6] >> (p & 63)) & 1ull;
-      bool hit = was;
-      if (V.moved[pr.x] | V.moved[pr.y]) {
-        hit = false;
-        if (im[pr.x] > 0.0 || im[pr.y] > 0.0) {
-          const Seg A = V.seg[pr.x], B = V.seg[pr.y];
+    constexpr int U = 4;  // pairs per thread and round: independent loads in flight
+    for (int p0 = plo + threadIdx.x; p0 < phi; p0 += U * blockDim.x) {
+      int2 pr[U];
+      bool mv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int p = p0 + u * blockDim.x;
+        pr[u] = p < phi ? V.near[p] : make_int2(0, 0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) mv[u] = p0 + u * (int)blockDim.x < phi && (V.moved[pr[u].x] | V.moved[pr[u].y]);
+#pragma unroll 1
+      for (int u = 0; u < U; ++u) {
+        if (!mv[u]) continue;
+        const int p = p0 + u * blockDim.x;
+        const bool was = (__ldcg(&bits[p >> 6]) >> (p & 63)) & 1ull;
+        bool hit = false;
+        if (im[pr[u].x] > 0.0 || im[pr[u].y] > 0.0) {
+          const Seg A = V.seg[pr[u].x], B = V.seg[pr[u].y];
           if (!seg_far(A, B, prefilter_offset(A, B, V.box, invL, mode), A.r + B.r + delta)) {
             const Narrow nr = narrow_pair(A, B, V.box);
             hit = contact_test(nr.d2, A.r + B.r, delta);
@@ -345,10 +358,9 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
         }
         if (hit != was) atomicXor(&bits[p >> 6], 1ull << (p & 63));
       }
-      mine += hit ? 1 : 0;
     }
   } else {
-    for (int w = (plo >> 6) + threadIdx.x; w < ((phi + 63) >> 6); w += blockDim.x) bits[w] = 0ull;
+    for (int w = wlo + threadIdx.x; w < whi; w += blockDim.x) bits[w] = 0ull;
     __syncthreads();
     for (int p = plo + threadIdx.x; p < phi; p += blockDim.x) {
       const int2 pr = V.near[p];
@@ -356,12 +368,12 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
       const Seg A = V.seg[pr.x], B = V.seg[pr.y];
       if (seg_far(A, B, prefilter_offset(A, B, V.box, invL, mode), A.r + B.r + delta)) continue;
       const Narrow nr = narrow_pair(A, B, V.box);
-      if (contact_test(nr.d2, A.r + B.r, delta)) {
-        atomicOr(&bits[p >> 6], 1ull << (p & 63));
-        ++mine;
-      }
+      if (contact_test(nr.d2, A.r + B.r, delta)) atomicOr(&bits[p >> 6], 1ull << (p & 63));
     }
   }
+  __syncthreads();
+  int mine = 0;
+  for (int w = wlo + threadIdx.x; w < whi; w += blockDim.x) mine += __popcll(__ldcg(&bits[w]));
   const int bsum = block_reduce_sum_i(mine, sm.red_i);
   if (threadIdx.x == 0) V.blk[rank] = bsum;
   if (!team_sync(T)) return -1;
@@ -371,17 +383,20 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
     if (rank == 0 && threadIdx.x == 0) atomicOr(&ctl->err, ERR_CONTACT_CAP);
     return -1;
   }
+  // contacts in pair order: one word (64 pairs) per thread, scanned by
+  // population count
   int run = prefix;
-  for (int base = plo; base < phi; base += blockDim.x) {
-    const int p = base + threadIdx.x;
-    const int f = (p < phi && ((bits[p >> 6] >> (p & 63)) & 1ull)) ? 1 : 0;
+  for (int wb = wlo; wb < whi; wb += blockDim.x) {
+    const int w = wb + threadIdx.x;
+    const unsigned long long m = w < whi ? __ldcg(&bits[w]) : 0ull;
     int tot;
-    const int ex = block_excl_scan(f, sm.scan_w, tot);
-    if (f) {
+    int slot = run + block_excl_scan(__popcll(m), sm.scan_w, tot);
+    for (unsigned long long r = m; r; r &= r - 1) {
+      const int p = (w << 6) + __ffsll((long long)r) - 1;
       const int2 pr = V.near[p];
       const Seg A = V.seg[pr.x], B = V.seg[pr.y];
       const Narrow nr = narrow_pair(A, B, V.box);
-      write_contact(V.con, run + ex, pr.x, pr.y, A.r + B.r, nr);
+      write_contact(V.con, slot++, pr.x, pr.y, A.r + B.r, nr);
     }
     run += tot;
   }
@@ -1201,8 +1216,12 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     double invL[3] = {1.0, 1.0, 1.0};
     for (int k = 0; k < 3; ++k)
       if (V.box.L[k] > 0.0) invL[k] = 1.0 / V.box.L[k];
-    for (int i = tid; i < n; i += TS)
-      free_flight_fused(st, i, g, cfg.dt, V.ref, ref2, n, V.box, invL, V.seg, dmax, dnear);
+    const StateBase SB{st.sbase, st.pbase, n};
+    const double dt = cfg.dt;
+    const double* ref = V.ref;
+    Seg* seg = V.seg;
+    const Box box = V.box;
+    for (int i = tid; i < n; i += TS) free_flight_fused(SB, i, g, dt, ref, ref2, box, invL, seg, dmax, dnear);
     double bm = block_reduce_max(dmax, sm.red_d);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
     if (V.near) {
@@ -1338,8 +1357,17 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     double invL[3] = {1.0, 1.0, 1.0};
     for (int k = 0; k < 3; ++k)
       if (V.box.L[k] > 0.0) invL[k] = 1.0 / V.box.L[k];
-    for (int i = tid; i < n; i += TS)
-      bad |= position_update_fused(st, i, cfg, V.ref, ref2, n, V.box, invL, V.seg, dmax, dnear, V.moved);
+    {
+      const StateBase SB{st.sbase, st.pbase, n};
+      const double dt = cfg.dt, w_max = cfg.w_max;
+      const double ld = 1.0 - cfg.lin_damp * dt, ad = 1.0 - cfg.ang_damp * dt;
+      const double* ref = V.ref;
+      Seg* seg = V.seg;
+      unsigned char* moved = V.moved;
+      const Box box = V.box;
+      for (int i = tid; i < n; i += TS)
+        bad |= position_update_fused(SB, i, dt, ld, ad, w_max, ref, ref2, box, invL, seg, dmax, dnear, moved);
+    }
     if (bad) atomicOr(&ctl->err, ERR_NONFINITE);
     double bm = block_reduce_max(dmax, sm.red_d);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
@@ -1373,7 +1401,12 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
   }
   // 6) PBC wrap + clear forces (main.cpp:4508-4527); the next step touches
   // rod i from this same thread, so no barrier is needed here.
-  for (int i = tid; i < n; i += TS) wrap_clear_body(st, V.box, i, V.moved);
+  {
+    const StateBase SB{st.sbase, st.pbase, n};
+    const Box box = V.box;
+    unsigned char* moved = V.moved;
+    for (int i = tid; i < n; i += TS) wrap_clear_body(SB, box, i, moved);
+  }
   return true;
 }
 

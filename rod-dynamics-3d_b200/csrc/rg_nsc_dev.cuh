@@ -288,16 +288,17 @@ __device__ inline Seg seg_of(d3 x, dq q, double h, double r) {
 // displacement bounds against ref (and ref2 when given), with every input
 // loaded before the first store: one round trip to memory per rod instead
 // of three.  Same arithmetic as the separate functions.
-__device__ inline void free_flight_fused(const State& st, int i, d3 g, double dt, const double* ref,
-                                         const double* ref2, int n, const Box& box, const double* invL,
-                                         Seg* seg_out, double& dmax, double& dnear) {
-  const double im = st.inv_mass[i];
-  const dq q = st.q.ld(i);
-  d3 w = st.w.ld(i);
-  d3 v = st.v.ld(i);
-  const d3 f = st.f.ld(i), tau = st.tau.ld(i), I = st.I.ld(i), Iinv = st.Iinv.ld(i);
-  const d3 x = st.x.ld(i);
-  const double h = st.h[i], r = st.r[i];
+__device__ inline void free_flight_fused(const StateBase& S, int i, d3 g, double dt, const double* ref,
+                                         const double* ref2, const Box& box, const double* invL, Seg* seg_out,
+                                         double& dmax, double& dnear) {
+  const int n = S.n;
+  const double im = S.pc(3)[i];
+  const dq q{S.c(3)[i], S.c(4)[i], S.c(5)[i], S.c(6)[i]};
+  d3 v = S.ld3(7, i);
+  d3 w = S.ld3(10, i);
+  const d3 f = S.ld3(13, i), tau = S.ld3(16, i), I = S.pld3(5, i), Iinv = S.pld3(8, i);
+  const d3 x = S.ld3(0, i);
+  const double h = S.pc(1)[i], r = S.pc(0)[i];
   double rf[6], rf2[6];
   for (int k = 0; k < 6; ++k) rf[k] = ref[(size_t)k * n + i];
   if (ref2)
@@ -307,8 +308,8 @@ __device__ inline void free_flight_fused(const State& st, int i, d3 g, double dt
     d3 Iw_w = rot_diag_apply(q, I, w);
     d3 gyro = cross(w, Iw_w);
     w = w + rot_diag_apply(q, Iinv, tau - gyro) * dt;
-    st.v.st(i, v);
-    st.w.st(i, w);
+    S.st3(7, i, v);
+    S.st3(10, i, w);
   }
   const Seg s = seg_of(x, q, h, r);
   seg_out[i] = s;
@@ -317,16 +318,17 @@ __device__ inline void free_flight_fused(const State& st, int i, d3 g, double dt
 }
 
 // Position update of rod i (nsc_position_update_body) fused the same way;
-// returns 1 when the new state is not finite.
-__device__ inline int position_update_fused(const State& st, int i, const rg_config& cfg, const double* ref,
-                                            const double* ref2, int n, const Box& box, const double* invL,
-                                            Seg* seg_out, double& dmax, double& dnear, unsigned char* moved) {
-  const double dt = cfg.dt;
-  const double ld = 1.0 - cfg.lin_damp * dt, ad = 1.0 - cfg.ang_damp * dt;
-  d3 v = st.v.ld(i), w = st.w.ld(i);
-  d3 x = st.x.ld(i);
-  dq q = st.q.ld(i);
-  const double h = st.h[i], r = st.r[i];
+// ld, ad: the damping factors 1 - c dt.  Returns 1 when the new state is
+// not finite.
+__device__ inline int position_update_fused(const StateBase& S, int i, double dt, double ld, double ad,
+                                            double w_max, const double* ref, const double* ref2, const Box& box,
+                                            const double* invL, Seg* seg_out, double& dmax, double& dnear,
+                                            unsigned char* moved) {
+  const int n = S.n;
+  d3 v = S.ld3(7, i), w = S.ld3(10, i);
+  d3 x = S.ld3(0, i);
+  dq q{S.c(3)[i], S.c(4)[i], S.c(5)[i], S.c(6)[i]};
+  const double h = S.pc(1)[i], r = S.pc(0)[i];
   double rf[6], rf2[6];
   for (int k = 0; k < 6; ++k) rf[k] = ref[(size_t)k * n + i];
   if (ref2)
@@ -339,11 +341,11 @@ __device__ inline int position_update_fused(const State& st, int i, const rg_con
   v = v * ld;
   w = w * ad;
   double wl = len(w);
-  if (wl > cfg.w_max) w = w * (cfg.w_max / wl);
-  st.x.st(i, x);
-  st.q.st(i, q);
-  st.v.st(i, v);
-  st.w.st(i, w);
+  if (wl > w_max) w = w * (w_max / wl);
+  S.st3(0, i, x);
+  S.c(3)[i] = q.w; S.c(4)[i] = q.x; S.c(5)[i] = q.y; S.c(6)[i] = q.z;
+  S.st3(7, i, v);
+  S.st3(10, i, w);
   const Seg s = seg_of(x, q, h, r);
   seg_out[i] = s;
   if (moved) moved[i] = 0;
@@ -375,6 +377,20 @@ __device__ inline void wrap_clear_body(const State& st, const Box& box, int i, u
   }
   st.f.st(i, mk3(0, 0, 0));
   st.tau.st(i, mk3(0, 0, 0));
+}
+// The same from the buffer bases (persistent step).
+__device__ inline void wrap_clear_body(const StateBase& S, const Box& box, int i, unsigned char* moved) {
+  if (box.pbc) {
+    const d3 x0 = S.ld3(0, i);
+    d3 x = x0;
+    wrap_pos(box, x);
+    if (x.x != x0.x || x.y != x0.y || x.z != x0.z) {
+      S.st3(0, i, x);
+      if (moved) moved[i] = 1;
+    }
+  }
+  S.st3(13, i, mk3(0, 0, 0));
+  S.st3(16, i, mk3(0, 0, 0));
 }
 
 // Everything one team needs to step one system (device copy per system).

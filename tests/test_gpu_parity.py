@@ -207,3 +207,18 @@ def test_nsc_long_call_carries_exact_contacts(team):
     assert sg["psor_sweeps"] == so["psor_sweeps"]
     assert sg["contacts"] == so["contacts"]
     assert_contacts_equal(g, o, 0.0)
+
+
+def test_nsc_team_larger_than_pair_ranges():
+    # a team with more blocks than 64-pair words in the near list: the last
+    # blocks own no pairs, and must neither clear nor count the last word
+    sc = packed_scene(600, d=0.05, phi=0.2, seed=17, squeeze=0.97)
+    g, o = make_pair(sc, model="nsc", dt=5e-4, nsc_velocity_iters=500, team_blocks=24)
+    sg = g.step(6)
+    so = o.step(6)
+    a, b = g.get_state(), o.get_state()
+    for k in ("x", "q", "v", "w"):
+        assert rel_err(a[k], b[k]) < TOL, k
+    assert sg["psor_sweeps"] == so["psor_sweeps"]
+    assert sg["contacts"] == so["contacts"]
+    assert_contacts_equal(g, o, 0.0)
