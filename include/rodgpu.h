@@ -146,7 +146,8 @@ typedef struct rg_step_stats {
   int64_t psor_row_sweeps;  /* NSC: Σ over steps of contacts x sweeps         */
   int64_t kernel_launches;  /* kernels this library launched during the call  */
   int64_t contact_steps;    /* NSC: Σ over steps of velocity-solve contacts   */
-  int64_t reserved[2];
+  int64_t near_rebuilds;    /* NSC: near-list rebuilds in this call           */
+  int64_t reserved[1];
 } rg_step_stats;
 
 /* Stage timers (CUDA events on the system's stream), enabled per system.

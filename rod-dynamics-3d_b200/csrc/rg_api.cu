@@ -215,25 +215,57 @@ cudaError_t snapshot_alloc(rg_system* s) {
   return e;
 }
 
+// The snapshot copies of one system: the whole state, and of the history
+// table and the warm cache only their live entries (counts read on the
+// device; restore_snapshot copies whole arrays back, and nothing reads an
+// entry beyond the live count).
 void snapshot_segments(rg_system* s, std::vector<CopySeg>& out) {
   const History& H = s->hist;
   const Nsc& N = s->nsc;
-  const size_t wl_bytes = sizeof(double) * 3 * (size_t)N.wcap + sizeof(int) * (size_t)N.wcap;
-  out.push_back({s->d_state, s->d_snap, sizeof(double) * 19 * (size_t)s->n});
-  out.push_back({H.key[H.cur], s->snap_hkey, sizeof(unsigned long long) * H.cap});
-  out.push_back({H.val[H.cur], s->snap_hval, sizeof(double) * 3 * (size_t)H.cap});
-  out.push_back({H.frame[H.cur], s->snap_hframe, sizeof(long long) * H.cap});
-  out.push_back({N.wkey, s->snap_wkey, sizeof(unsigned long long) * N.wcap});
-  out.push_back({N.wlam, s->snap_wlam, wl_bytes});
+  const int* hn = &s->d_ctl->hist_n;
+  const size_t hc = (size_t)H.cap, wc = (size_t)N.wcap;
+  out.push_back({s->d_state, s->d_snap, sizeof(double) * 19 * (size_t)s->n, nullptr, 0, 0});
+  out.push_back({H.key[H.cur], s->snap_hkey, sizeof(unsigned long long) * hc, hn, 8, 0});
+  for (int c = 0; c < 3; ++c)
+    out.push_back({H.val[H.cur] + c * hc, s->snap_hval + c * hc, sizeof(double) * hc, hn, 8, 0});
+  out.push_back({H.frame[H.cur], s->snap_hframe, sizeof(long long) * hc, hn, 8, 0});
+  out.push_back({N.wkey, s->snap_wkey, sizeof(unsigned long long) * wc, N.wn, 8, 0});
+  for (int c = 0; c < 3; ++c)
+    out.push_back({N.wlam + c * wc, s->snap_wlam + c * wc, sizeof(double) * wc, N.wn, 8, 0});
+  out.push_back({N.wlam + 3 * wc, s->snap_wlam + 3 * wc, sizeof(int) * wc, N.wn, 4, 0});
 }
 
-// One block per segment (strided): 16-byte words when both ends allow it,
-// else 4-byte words (every buffer here is 4-byte aligned and sized).
+// One block per segment (strided; segments are split into pieces of at most
+// kCopyChunk bytes by the caller): 16-byte words when both ends allow it,
+// each thread loading all of its words before storing any, else 4-byte
+// words (every buffer here is 4-byte aligned and sized).
 __global__ void k_copy_segments(const CopySeg* segs, int n) {
+  constexpr int kPer = kCopyChunk / 16 / 256;  // 16-byte words per thread
   for (int k = blockIdx.x; k < n; k += gridDim.x) {
-    const CopySeg g = segs[k];
+    CopySeg g = segs[k];
+    if (g.count) {  // live part only
+      const int c = *g.count;
+      const unsigned long long live = c > 0 ? (unsigned long long)c * g.elem : 0ull;
+      if (g.off >= live) continue;
+      if (g.bytes > live - g.off) g.bytes = live - g.off;
+    }
     const unsigned long long a = (unsigned long long)g.src | (unsigned long long)g.dst | g.bytes;
-    if ((a & 15ull) == 0) {
+    if ((a & 15ull) == 0 && g.bytes <= (unsigned long long)kCopyChunk && blockDim.x == 256) {
+      const uint4* src = static_cast<const uint4*>(g.src);
+      uint4* dst = static_cast<uint4*>(g.dst);
+      const int nv = (int)(g.bytes / 16);
+      uint4 r[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int i = threadIdx.x + u * 256;
+        if (i < nv) r[u] = src[i];
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int i = threadIdx.x + u * 256;
+        if (i < nv) dst[i] = r[u];
+      }
+    } else if ((a & 15ull) == 0) {
       const uint4* src = static_cast<const uint4*>(g.src);
       uint4* dst = static_cast<uint4*>(g.dst);
       for (unsigned long long i = threadIdx.x; i < g.bytes / 16; i += blockDim.x) dst[i] = src[i];
@@ -243,6 +275,16 @@ __global__ void k_copy_segments(const CopySeg* segs, int n) {
       for (unsigned long long i = threadIdx.x; i < g.bytes / 4; i += blockDim.x) dst[i] = src[i];
     }
   }
+}
+
+void split_segments(const std::vector<CopySeg>& in, std::vector<CopySeg>& out) {
+  out.clear();
+  for (const CopySeg& g : in)
+    for (unsigned long long off = 0; off < g.bytes; off += kCopyChunk) {
+      const unsigned long long nb = g.bytes - off < (unsigned long long)kCopyChunk ? g.bytes - off : kCopyChunk;
+      out.push_back({static_cast<const char*>(g.src) + off, static_cast<char*>(g.dst) + off, nb, g.count, g.elem,
+                     g.off + off});
+    }
 }
 
 void copy_segments_launch(const CopySeg* d_segs, int n, cudaStream_t st) {
@@ -260,6 +302,7 @@ __global__ void k_ctl_reset(Ctl* const* ctls, int n) {
     c->max_residual = 0;
     c->row_sweeps = 0;
     c->contact_steps = 0;
+    c->near_rebuilds = 0;
     c->member_ns = 0;
     c->serial_ns = 0;
     c->det_valid = 0;
@@ -630,6 +673,7 @@ cudaError_t reset_call_ctl(rg_system* s, const Snapshot& sn) {
   h->max_residual = 0;
   h->row_sweeps = 0;
   h->contact_steps = 0;
+  h->near_rebuilds = 0;
   h->member_ns = 0;
   h->serial_ns = 0;
   h->det_valid = 0;
@@ -678,6 +722,7 @@ void fill_stats(rg_system* s, int nsteps, rg_step_stats* stats, bool ke_launched
   stats->psor_row_sweeps = h->row_sweeps;
   stats->kernel_launches = s->last_call_launches;
   stats->contact_steps = h->contact_steps;
+  stats->near_rebuilds = h->near_rebuilds;
   stats->kinetic_energy = ke_launched ? ke_sum(s) : kinetic_energy(s);
 }
 

@@ -54,6 +54,10 @@ struct rg_batch {
   unsigned int* d_bars = nullptr;
   long long* d_team_ns = nullptr;
   int cap_members = 0, cap_teams = 0;
+  // what the device holds now (uploads are skipped when nothing changed)
+  std::vector<NscView> up_views;
+  std::vector<TeamDesc> up_teams;
+  std::vector<int> up_members;
   // graph of (barrier reset + persistent launch) for graph_steps steps
   cudaGraphExec_t graph = nullptr;
   int graph_steps = -1;
@@ -357,19 +361,36 @@ cudaError_t ensure_dev(rg_batch* b, size_t nteams, size_t nmembers) {
 // Uploads the views of all members (buffer addresses change when buffers
 // grow) and the team plan.  The views array is indexed by member number.
 cudaError_t upload(rg_batch* b, std::vector<TeamDesc>& teams, const std::vector<int>& members) {
+  const int cm = b->cap_members, ct = b->cap_teams;
   cudaError_t e = ensure_dev(b, teams.size(), members.size());
   if (e) return e;
+  const bool moved = cm != b->cap_members || ct != b->cap_teams;  // device tables reallocated
   std::vector<NscView> views(b->n);
-  for (int k = 0; k < b->n; ++k)
+  for (int k = 0; k < b->n; ++k) {
+    std::memset(&views[k], 0, sizeof(NscView));
     if (b->sys[k]->cfg.model == RG_MODEL_NSC) views[k] = make_view(b->sys[k]);
+  }
   for (size_t t = 0; t < teams.size(); ++t) {
     teams[t].bar = b->d_bars + 4 * t;
     teams[t].t_ns = b->d_team_ns + t;
   }
-  cudaMemcpyAsync(b->d_views, views.data(), sizeof(NscView) * b->n, cudaMemcpyHostToDevice, b->stream);
-  cudaMemcpyAsync(b->d_teams, teams.data(), sizeof(TeamDesc) * teams.size(), cudaMemcpyHostToDevice, b->stream);
-  cudaMemcpyAsync(b->d_members, members.data(), sizeof(int) * members.size(), cudaMemcpyHostToDevice, b->stream);
-  return cudaStreamSynchronize(b->stream);
+  bool any = false;
+  if (moved || b->up_views.size() != views.size() ||
+      std::memcmp(b->up_views.data(), views.data(), sizeof(NscView) * views.size()) != 0) {
+    cudaMemcpyAsync(b->d_views, views.data(), sizeof(NscView) * b->n, cudaMemcpyHostToDevice, b->stream);
+    b->up_views = views;
+    any = true;
+  }
+  if (moved || b->up_teams.size() != teams.size() ||
+      std::memcmp(b->up_teams.data(), teams.data(), sizeof(TeamDesc) * teams.size()) != 0 ||
+      b->up_members != members) {
+    cudaMemcpyAsync(b->d_teams, teams.data(), sizeof(TeamDesc) * teams.size(), cudaMemcpyHostToDevice, b->stream);
+    cudaMemcpyAsync(b->d_members, members.data(), sizeof(int) * members.size(), cudaMemcpyHostToDevice, b->stream);
+    b->up_teams = teams;
+    b->up_members = members;
+    any = true;
+  }
+  return any ? cudaStreamSynchronize(b->stream) : cudaSuccess;
 }
 
 void drop_graph(rg_batch* b) {
@@ -427,7 +448,9 @@ int ctl_setup(rg_batch* b) {
 }
 
 // Runs the copy segments on the device (one upload, one kernel).
-int run_segments(rg_batch* b, const std::vector<CopySeg>& segs) {
+int run_segments(rg_batch* b, const std::vector<CopySeg>& whole) {
+  std::vector<CopySeg> segs;
+  split_segments(whole, segs);
   if ((int)segs.size() > b->cap_segs) {
     cudaFree(b->d_segs);
     b->cap_segs = (int)segs.size() * 2;

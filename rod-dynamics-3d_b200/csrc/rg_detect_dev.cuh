@@ -399,13 +399,23 @@ __device__ inline int near_count_lanes(int i, bool valid, const Seg* seg, const 
     const int* list = nbr + (size_t)i * maxnb;
     const Seg A = seg[i];
     const bool a_static = !(inv_mass[i] > 0.0);
-    for (int k = l; k < cnt; k += G) {
-      const int j = list[k];
-      if (a_static && !(inv_mass[j] > 0.0)) continue;
-      const Seg B = seg[j];
-      if (seg_far(A, B, prefilter_offset(A, B, box, invL, mode), A.r + B.r + extra)) continue;
-      atomicOr(&mask[(size_t)i * words + (k >> 6)], 1ull << (k & 63));
-      ++hits;
+    // two entries per round: both gathers are in flight before either test
+    for (int k = l; k < cnt; k += 2 * G) {
+      const bool has1 = k + G < cnt;
+      const int j0 = list[k];
+      const int j1 = has1 ? list[k + G] : j0;
+      const Seg B0 = seg[j0];
+      const Seg B1 = seg[j1];
+      if (!(a_static && !(inv_mass[j0] > 0.0)) &&
+          !seg_far(A, B0, prefilter_offset(A, B0, box, invL, mode), A.r + B0.r + extra)) {
+        atomicOr(&mask[(size_t)i * words + (k >> 6)], 1ull << (k & 63));
+        ++hits;
+      }
+      if (has1 && !(a_static && !(inv_mass[j1] > 0.0)) &&
+          !seg_far(A, B1, prefilter_offset(A, B1, box, invL, mode), A.r + B1.r + extra)) {
+        atomicOr(&mask[(size_t)i * words + ((k + G) >> 6)], 1ull << ((k + G) & 63));
+        ++hits;
+      }
     }
   }
 #pragma unroll
@@ -418,8 +428,9 @@ __device__ inline void near_write_rod(int i, int o, const int* nbr_cnt, const in
                                       const unsigned long long* mask, int2* out) {
   const int cnt = nbr_cnt[i];
   const int* list = nbr + (size_t)i * maxnb;
-  for (int k = 0; k < cnt; ++k)
-    if ((mask[(size_t)i * words + (k >> 6)] >> (k & 63)) & 1ull) out[o++] = make_int2(i, list[k]);
+  for (int w = 0; w < words && w * 64 < cnt; ++w)
+    for (unsigned long long m = __ldcg(&mask[(size_t)i * words + w]); m; m &= m - 1)
+      out[o++] = make_int2(i, list[w * 64 + __ffsll((long long)m) - 1]);
 }
 
 // Contact record o of pair (i, j) from its narrow-phase result.

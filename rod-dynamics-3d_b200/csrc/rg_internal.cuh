@@ -46,6 +46,7 @@ struct Ctl {
   long long member_ns;  // device time of this system's steps in the call (batch cost model)
   long long serial_ns;  // of which in the single-block solves (no team speed-up)
   long long contact_steps;  // Σ velocity-solve contacts over steps
+  long long near_rebuilds;  // near-list rebuilds (per call)
   int vel_contacts;     // NSC: contacts of the last velocity solve (lastHitCount)
   int prof_phases;      // 1: the persistent step records phase times
   long long phase_ns[12];  // persistent-step phase time accumulators
@@ -309,7 +310,16 @@ struct CopySeg {
   const void* src;
   void* dst;
   unsigned long long bytes;
+  // optional: only the first (*count) x elem bytes of the whole segment are
+  // live (read on the device when the copy runs); off = this piece's offset
+  // within the segment
+  const int* count;
+  unsigned elem;
+  unsigned long long off;
 };
+constexpr int kCopyChunk = 32768;  // largest piece one block of k_copy_segments moves
+// Splits segments into pieces of at most kCopyChunk bytes (same copies).
+void split_segments(const std::vector<CopySeg>& in, std::vector<CopySeg>& out);
 cudaError_t snapshot_alloc(rg_system* s);
 void snapshot_segments(rg_system* s, std::vector<CopySeg>& out);
 void copy_segments_launch(const CopySeg* d_segs, int n, cudaStream_t st);

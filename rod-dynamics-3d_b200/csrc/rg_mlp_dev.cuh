@@ -226,17 +226,30 @@ __device__ inline MlpStage mlp_stage_at(void* buf) {
   return s;
 }
 
-// Block-cooperative copy of rows x cols BF16 (cols a multiple of 8, both
-// 16-byte aligned) into a padded shared-memory matrix.
+// 16-byte asynchronous copy global -> shared (no register round trip; all
+// of a thread's copies are in flight together until stage_wait).
+__device__ inline void cp_async16(void* smem_dst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+// Waits for this thread's asynchronous copies; a block barrier must follow
+// before other threads read them.
+__device__ inline void stage_wait() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Block-cooperative asynchronous copy of rows x cols BF16 (cols a multiple
+// of 8, both 16-byte aligned) into a padded shared-memory matrix; complete
+// after stage_wait and a block barrier.
 __device__ inline void stage_bf16(__nv_bfloat16* dst, int ldd, const __nv_bfloat16* src, int rows, int cols) {
   const int vpr = cols / 8;
   for (int v = threadIdx.x; v < rows * vpr; v += blockDim.x) {
     const int r = v / vpr, c = v - r * vpr;
-    *reinterpret_cast<uint4*>(dst + (size_t)r * ldd + c * 8) =
-        *reinterpret_cast<const uint4*>(src + (size_t)r * cols + c * 8);
+    cp_async16(dst + (size_t)r * ldd + c * 8, src + (size_t)r * cols + c * 8);
   }
 }
-// Block-cooperative copy of W1, W4 and the small parameters.
+// Block-cooperative copy of W1, W4 (asynchronous, see stage_bf16) and the
+// small parameters.
 __device__ inline void stage_small(const MlpStage& s, const MlpDev& M) {
   stage_bf16(s.w1, kW1Ld, M.w1, kMlpH, kW1Pad);
   stage_bf16(s.w4, kWhLd, M.w4, kW4Pad, kMlpH);

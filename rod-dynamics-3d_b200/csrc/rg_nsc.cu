@@ -293,7 +293,10 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
     const int bsum = block_reduce_sum_i(mine, sm.red_i);
     if (threadIdx.x == 0) V.blk[rank] = bsum;
     if (!team_sync(T)) return -1;
-    if (rank == 0 && threadIdx.x == 0) ctl->near_disp = 0.0;  // every block has read it
+    if (rank == 0 && threadIdx.x == 0) {
+      ctl->near_disp = 0.0;  // every block has read it
+      ctl->near_rebuilds += 1;
+    }
     block_prefix(V.blk, T.nb, rank, prefix, total, sm);
     int run = prefix;
     for (int base = lo; base < hi; base += blockDim.x) {
@@ -786,6 +789,7 @@ struct SmallSmem {
   float feat[kMlpIn * kSmallC];      // learned warm start features [8][kSmallC]
   float pred[kMlpOut * kSmallC];     // predicted impulse changes [3][kSmallC]
   int mtile[kSmallC / 16];           // 16-contact tiles that need the network
+  unsigned char cached[kSmallC];     // 1: the slot's contact is in the warm cache
   // one hidden layer of the network (the rest is staged in pmax/cmask)
   alignas(16) __nv_bfloat16 wh[kStageWh];
 };
@@ -923,10 +927,18 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
   Ctl* ctl = V.ctl;
   const rg_config& cfg = V.cfg;
   const int t = threadIdx.x;
+  // the learned start's gate is known now: its first hidden layer travels to
+  // shared memory while the colouring and the rows are built
+  const bool mlp_gate = V.use_mlp && (*(volatile int*)V.wn == 0 ||
+                                      *(volatile int*)&ctl->sweeps_last > V.mlp_min_sweeps);
+  if (mlp_gate) stage_bf16(S.wh, kWhLd, V.mlp.w2, kMlpH, kMlpH);
   small_map(V, C, S);
   pc.mark(10);
   int K = small_color(V, C, S);
-  if (K < 0) return false;
+  if (K < 0) {
+    if (mlp_gate) stage_wait();
+    return false;
+  }
   pc.mark(2);
   // body velocities on chip
   for (int s = t; s < S.nloc; s += blockDim.x) {
@@ -946,7 +958,10 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
   int coll = 0;
   if (t < C) {
     const int c = S.order[t];
-    coll = build_row(V.st, V.con, cfg, c, t, R, V.wkey, V.wlam, W, V.wcap, V.feat_on ? S.feat : nullptr, kSmallC);
+    const int br = build_row(V.st, V.con, cfg, c, t, R, V.wkey, V.wlam, W, V.wcap, V.feat_on ? S.feat : nullptr,
+                             kSmallC);
+    coll = br & 1;
+    S.cached[t] = (unsigned char)(br >> 1);
     if (V.feat_on) {
       if (S.dyn[S.la[c]]) atomicAdd(&deg[S.la[c]], 1);
       if (S.dyn[S.lb[c]]) atomicAdd(&deg[S.lb[c]], 1);
@@ -960,10 +975,10 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
       S.feat[7 * kSmallC + t] = (float)((S.dyn[sa] ? deg[sa] - 1 : 0) + (S.dyn[sb] ? deg[sb] - 1 : 0));
     }
     __syncthreads();
-    if (V.use_mlp && (W == 0 || *(volatile int*)&ctl->sweeps_last > V.mlp_min_sweeps)) {
+    if (mlp_gate) {
       // the contacts the learned start is for (every contact, or those new
       // since the last step); the network runs only on tiles that hold one
-      const bool want = t < C && (V.mlp_all || !warm_cached(V, S.order[t], W));
+      const bool want = t < C && (V.mlp_all || !S.cached[t]);
       if (t < kSmallC / 16) S.mtile[t] = 0;
       __syncthreads();
       if (want) S.mtile[t >> 4] = 1;
@@ -973,8 +988,8 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
         // in pmax/cmask (free after colouring and degrees), the hidden
         // layers one after the other in wh.
         const MlpStage ms = mlp_stage_at(S.pmax);
-        stage_small(ms, V.mlp);
-        stage_bf16(S.wh, kWhLd, V.mlp.w2, kMlpH, kMlpH);
+        stage_small(ms, V.mlp);  // W2 is already on its way (start of the solve)
+        stage_wait();
         __syncthreads();
         const int row0 = (t >> 5) * 16, lane = t & 31;
         const bool mine = row0 < C && S.mtile[t >> 5];
@@ -986,6 +1001,7 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
         }
         __syncthreads();
         stage_bf16(S.wh, kWhLd, V.mlp.w3, kMlpH, kMlpH);
+        stage_wait();
         __syncthreads();
         if (mine) {
           hidden_layer(a, S.wh, kWhLd, q.b3, lane);
@@ -997,6 +1013,7 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
       }
     }
   }
+  if (mlp_gate) stage_wait();  // no copy outlives the solve
   pc.mark(3);
   Vel Vv{Vec3A{S.vel, S.vel + kSmallB, S.vel + 2 * kSmallB},
          Vec3A{S.vel + 3 * kSmallB, S.vel + 4 * kSmallB, S.vel + 5 * kSmallB}};
@@ -1264,7 +1281,7 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     int coll = 0;
     for (int p = tid; p < C; p += TS) {
       const int c = V.order[p];
-      coll += build_row(st, V.con, cfg, c, p, R, V.wkey, V.wlam, W, V.wcap, V.feat_on ? V.feat : nullptr, V.ccap);
+      coll += build_row(st, V.con, cfg, c, p, R, V.wkey, V.wlam, W, V.wcap, V.feat_on ? V.feat : nullptr, V.ccap) & 1;
       if (V.feat_on) {
         if (im[V.con.a[c]] > 0.0) atomicAdd(&deg[V.con.a[c]], 1);
         if (im[V.con.b[c]] > 0.0) atomicAdd(&deg[V.con.b[c]], 1);
@@ -1290,6 +1307,7 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
         stage_small(ms, V.mlp);
         stage_bf16(S.wh, kWhLd, V.mlp.w2, kMlpH, kMlpH);
         stage_bf16(w3s, kWhLd, V.mlp.w3, kMlpH, kMlpH);
+        stage_wait();
         __syncthreads();
         if (!team_sync(T)) return false;
         const MlpSmall q = ms.small();

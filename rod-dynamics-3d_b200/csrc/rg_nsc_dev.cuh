@@ -101,10 +101,12 @@ __device__ inline int build_row(const State& st, const Contacts& con, const rg_c
   R.r(R_PHI, p) = phi;
   R.r(R_VNPRE, p) = vnp;
   double l0 = 0, l1 = 0, l2 = 0;
+  int cached = 0;
   if (cfg.nsc_warm_start != RG_WARM_NONE && W > 0) {
     unsigned long long k = ((unsigned long long)(unsigned)a << 32) | (unsigned)b;
     int q = lower_bound_key(wkey, W, k);
     if (q < W && wkey[q] == k) {
+      cached = 2;
       l0 = smax(0.0, wlam[q]);
       l1 = wlam[wcap + q];
       l2 = wlam[2 * wcap + q];
@@ -122,7 +124,7 @@ __device__ inline int build_row(const State& st, const Contacts& con, const rg_c
     feat[5 * fld + p] = (float)l1;
     feat[6 * fld + p] = (float)l2;
   }
-  return vnp < -1e-6 ? 1 : 0;
+  return (vnp < -1e-6 ? 1 : 0) | cached;  // bit 0: impact, bit 1: in the warm cache
 }
 
 // Learned warm start of slot p: previous impulse (already in R.lam) plus the

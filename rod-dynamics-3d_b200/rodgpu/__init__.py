@@ -57,7 +57,7 @@ class RgStepStats(ctypes.Structure):
         ("potential_energy", _d), ("kinetic_energy", _d), ("max_residual", _d),
         ("not_converged", ctypes.c_int64), ("device_ms", _d), ("psor_row_sweeps", ctypes.c_int64),
         ("kernel_launches", ctypes.c_int64), ("contact_steps", ctypes.c_int64),
-        ("reserved", ctypes.c_int64 * 2),
+        ("near_rebuilds", ctypes.c_int64), ("reserved", ctypes.c_int64 * 1),
     ]
 
     def as_dict(self):
