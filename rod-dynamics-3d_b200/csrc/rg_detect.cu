@@ -166,13 +166,15 @@ __global__ void __launch_bounds__(kTile) k_build_lists(const Seg* seg, int n, co
   if (ctl->err || !ctl->rebuild) return;
   const GridDev g = *gdev;
   __shared__ BuildSmem sm;
+  constexpr int kQ = 4 * kTile;  // candidate queues of the compacted build
+  __shared__ unsigned q1[kQ], q2[kQ];
   int overflow = 0;
   double invL[3] = {1.0, 1.0, 1.0};
   for (int k = 0; k < 3; ++k)
     if (box.L[k] > 0.0) invL[k] = 1.0 / box.L[k];
   for (int cell = blockIdx.x; cell < g.ncells; cell += gridDim.x)
     build_cell_pairs(seg, g, box, invL, cell_start, cell_rods, margin, skin, all_pairs, nbr_cnt, nbr, maxnb,
-                     cell, sm, overflow);
+                     cell, sm, q1, q2, kQ, overflow);
   if (overflow) atomicOr(&ctl->err, ERR_NBR_CAP);
   (void)n;
   (void)cut_center;
@@ -311,7 +313,7 @@ cudaError_t detector_alloc(rg_system* s) {
   // Default skin: half a diameter, but at least a tenth of the rod length,
   // so thin rods (whose lists stay short, and whose per-step narrow phase
   // runs over the near list only) rebuild rarely.
-  d.skin = c.skin > 0 ? c.skin : fmax(0.5 * (dsum / n), 0.1 * (lsum / n)) + 1e-6;
+  d.skin = c.skin > 0 ? c.skin : fmax(0.5 * (dsum / n), 0.075 * (lsum / n)) + 1e-6;
   d.cut_center = 2.0 * (hmax + rmax) + d.margin + d.skin;
   d.all_pairs = false;
   GridDev gd{};
@@ -358,7 +360,7 @@ cudaError_t detector_alloc(rg_system* s) {
   if (c.model == RG_MODEL_NSC) {
     // all-pairs boxes rebuild the near list from every pair: a wider near
     // skin makes those rebuilds rare
-    d.near_skin = (c.near_skin_pct > 0 ? 0.01 * c.near_skin_pct : (d.all_pairs ? 0.5 : 0.05)) * d.skin;
+    d.near_skin = (c.near_skin_pct > 0 ? 0.01 * c.near_skin_pct : (d.all_pairs ? 0.5 : 0.1)) * d.skin;
     if ((e = cudaMalloc(&d.near, sizeof(int2) * (size_t)n * d.maxnb))) return e;
     if ((e = cudaMalloc(&d.ref2, sizeof(double) * 6 * (size_t)n))) return e;
     if ((e = cudaMalloc(&d.moved, (size_t)n))) return e;

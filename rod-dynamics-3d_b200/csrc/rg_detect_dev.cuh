@@ -75,7 +75,10 @@ struct BuildSmem {
   SegTile home;
   int hidx[kTile];
   int ncl[27];
+  int nstart[27];  // first entry of each neighbour cell in cell_rods
+  int npre[28];    // prefix of the neighbour cells' rod counts
   int nn;
+  int qn[2];       // queue fills (see build_cell_pairs)
 };
 
 __device__ inline int list_insert(int* list, int cnt, int cap, int j, int& overflow) {
@@ -136,9 +139,34 @@ __device__ inline bool seg_far(const Seg& A, const Seg& B, d3 d, double lim) {
 __device__ inline void build_cell_pairs(const Seg* seg, const GridDev& g, const Box& box, const double* invL,
                                         const int* cell_start, const int* cell_rods, double margin,
                                         double skin, int all_pairs, int* nbr_cnt, int* nbr, int maxnb,
-                                        int cell, BuildSmem& sm, int& overflow) {
+                                        int cell, BuildSmem& sm, unsigned* q1, unsigned* q2, int qcap,
+                                        int& overflow) {
   int cx = cell % g.n[0], cy = (cell / g.n[0]) % g.n[1], cz = cell / (g.n[0] * g.n[1]);
-  if (threadIdx.x == 0) {
+  // Half shell: the home cell (pairs j > i) and the 13 cells ahead of it
+  // (every pair), each unordered pair met once and listed under its lower
+  // index.  Needs distinct neighbour cells: three or more cells along every
+  // periodic axis, and not the all-pairs scan.
+  const bool half = !all_pairs && !(box.pbc && (g.n[0] < 3 || g.n[1] < 3 || g.n[2] < 3));
+  if (threadIdx.x == 0 && half) {
+    int cnt = 0;
+    const int c3[3] = {cx, cy, cz};
+    for (int o = 0; o < 27; ++o) {
+      const int off[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1};
+      // home first, then the forward half (z, then y, then x decides)
+      const bool fwd = off[2] > 0 || (off[2] == 0 && (off[1] > 0 || (off[1] == 0 && off[0] > 0)));
+      if (!fwd) continue;
+      int X = c3[0] + off[0], Y = c3[1] + off[1], Z = c3[2] + off[2];
+      if (box.pbc) {
+        X = (X + g.n[0]) % g.n[0]; Y = (Y + g.n[1]) % g.n[1]; Z = (Z + g.n[2]) % g.n[2];
+      } else if (X < 0 || Y < 0 || Z < 0 || X >= g.n[0] || Y >= g.n[1] || Z >= g.n[2]) {
+        continue;
+      }
+      sm.ncl[1 + cnt++] = (Z * g.n[1] + Y) * g.n[0] + X;
+    }
+    sm.ncl[0] = cell;
+    sm.nn = 1 + cnt;
+  }
+  if (threadIdx.x == 0 && !half) {
     int cnt = 0;
     int lo[3], hi[3];
     int c3[3] = {cx, cy, cz};
@@ -164,53 +192,146 @@ __device__ inline void build_cell_pairs(const Seg* seg, const GridDev& g, const 
   }
   __syncthreads();
   const int nn = sm.nn;
+  if ((int)threadIdx.x < nn) {
+    const int c = sm.ncl[threadIdx.x];
+    sm.nstart[threadIdx.x] = cell_start[c];
+    sm.npre[threadIdx.x + 1] = cell_start[c + 1] - cell_start[c];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sm.npre[0] = 0;
+    for (int c = 0; c < nn; ++c) sm.npre[c + 1] += sm.npre[c];
+  }
+  // (read after the barrier at the top of the home-tile loop)
   const int hs = cell_start[cell], he = cell_start[cell + 1];
   for (int h0 = hs; h0 < he; h0 += kTile) {
     const int H = he - h0 < kTile ? he - h0 : kTile;
+    // G threads per home rod, each scanning every G-th rod of a tile: no
+    // per-pair index division, the home rod's centre stays in registers
+    const int G = (int)blockDim.x / H > 0 ? (int)blockDim.x / H : 1;
+    const int hslot = (int)threadIdx.x / G, sub = (int)threadIdx.x - hslot * G;
     __syncthreads();
     if ((int)threadIdx.x < H) {
       int i = cell_rods[h0 + threadIdx.x];
       sm.hidx[threadIdx.x] = i;
       sm.home.put(threadIdx.x, seg[i]);
     }
-    for (int c = 0; c < nn; ++c) {
-      int ns = cell_start[sm.ncl[c]], ne = cell_start[sm.ncl[c] + 1];
-      for (int t0 = ns; t0 < ne; t0 += kTile) {
-        const int m = ne - t0 < kTile ? ne - t0 : kTile;
+    __syncthreads();
+    const bool mine = hslot < H;
+    const int i = mine ? sm.hidx[hslot] : 0;
+    const double hcx = mine ? sm.home.cx[hslot] : 0.0, hcy = mine ? sm.home.cy[hslot] : 0.0;
+    const double hcz = mine ? sm.home.cz[hslot] : 0.0;
+    const double hhr = mine ? sm.home.h[hslot] : 0.0, hrr = mine ? sm.home.r[hslot] : 0.0;
+    // the neighbourhood's rods as one sequence (cell after cell), staged in
+    // full tiles: fewer, fuller tiles than one per neighbour cell
+    const int total = sm.npre[nn];
+    {
+      for (int t0 = 0; t0 < total; t0 += kTile) {
+        const int m = total - t0 < kTile ? total - t0 : kTile;
         __syncthreads();
         if ((int)threadIdx.x < m) {
-          int j = cell_rods[t0 + threadIdx.x];
+          const int v = t0 + (int)threadIdx.x;
+          int lo = 0, hi = nn;  // last cell with npre <= v
+          while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (sm.npre[mid] <= v) lo = mid;
+            else hi = mid;
+          }
+          int j = cell_rods[sm.nstart[lo] + (v - sm.npre[lo])];
           sm.tidx[threadIdx.x] = j;
           sm.tile.put(threadIdx.x, seg[j]);
         }
         __syncthreads();
-        const int pairs = H * m;
-        for (int q = threadIdx.x; q < pairs; q += blockDim.x) {
-          const int h = q / m, u = q - h * m;
-          const int i = sm.hidx[h], j = sm.tidx[u];
-          if (j <= i) continue;
-          if (!all_pairs) {
-            // centre test from the staged centres only (same arithmetic as
-            // centre_offset)
-            d3 d{sm.tile.cx[u] - sm.home.cx[h], sm.tile.cy[u] - sm.home.cy[h], sm.tile.cz[u] - sm.home.cz[h]};
+        if (all_pairs) {
+          // tiny periodic boxes: every pair is listed
+          if (!mine) continue;
+          for (int u = sub; u < m; u += G) {
+            const int j = sm.tidx[u];
+            if (j <= i) continue;
+            int pos = atomicAdd(&nbr_cnt[i], 1);
+            if (pos < maxnb) nbr[(size_t)i * maxnb + pos] = j;
+            else overflow = 1;
+          }
+          continue;
+        }
+        // Three block-wide stages per round, each over compacted work, so a
+        // warp's lanes run the same test: centre test of every candidate ->
+        // queue q1; axial/line prefilter of q1 -> queue q2; exact distance
+        // of q2 -> lists.  (Tested lane by lane, one lane's exact test held
+        // up its whole warp.)  per = candidates per thread and round.
+        constexpr int kAhead = 4;
+        const int per = (qcap / (int)blockDim.x) / kAhead * kAhead;
+        const int cand = (m + G - 1) / G;  // most candidates of any thread
+        const int rounds = (cand + per - 1) / per;
+        const unsigned lane = threadIdx.x & 31u;
+        for (int rd = 0; rd < rounds; ++rd) {
+          if (threadIdx.x == 0) { sm.qn[0] = 0; sm.qn[1] = 0; }
+          __syncthreads();
+          for (int c0 = 0; c0 < per; c0 += kAhead) {
+            // kAhead candidates with independent loads and FP64 chains
+            bool pass[kAhead];
+#pragma unroll
+            for (int k = 0; k < kAhead; ++k) {
+              const int u = sub + (rd * per + c0 + k) * G;
+              const bool ok = mine && u < m;
+              const int uu = ok ? u : 0;
+              const int j = sm.tidx[uu];
+              // centre test from the staged centres only (same arithmetic as
+              // centre_offset)
+              d3 d{sm.tile.cx[uu] - hcx, sm.tile.cy[uu] - hcy, sm.tile.cz[uu] - hcz};
+              if (box.pbc) {
+                if (box.L[0] > 0.0) d.x -= box.L[0] * rint(d.x * invL[0]);
+                if (box.L[1] > 0.0) d.y -= box.L[1] * rint(d.y * invL[1]);
+                if (box.L[2] > 0.0) d.z -= box.L[2] * rint(d.z * invL[2]);
+              }
+              const double hr = hhr + sm.tile.h[uu] + hrr + sm.tile.r[uu];
+              const double cc = hr + margin + skin;
+              const bool order = (half && t0 + uu >= sm.npre[1]) ? j != i : j > i;
+              pass[k] = ok && order && !(dot(d, d) > cc * cc * (1.0 + 1e-9));
+            }
+#pragma unroll
+            for (int k = 0; k < kAhead; ++k) {
+              const unsigned bal = __ballot_sync(0xffffffffu, pass[k]);
+              int base = 0;
+              if (lane == 0 && bal) base = atomicAdd(&sm.qn[0], __popc(bal));
+              base = __shfl_sync(0xffffffffu, base, 0);
+              const int u = sub + (rd * per + c0 + k) * G;
+              if (pass[k]) q1[base + __popc(bal & ((1u << lane) - 1u))] = ((unsigned)hslot << 16) | (unsigned)u;
+            }
+          }
+          __syncthreads();
+          const int n1 = sm.qn[0];
+          for (int e = threadIdx.x; e < n1; e += blockDim.x) {
+            const unsigned w = q1[e];
+            const int h = (int)(w >> 16), u = (int)(w & 0xffffu);
+            const Seg A = sm.home.get(h);
+            const Seg B = sm.tile.get(u);
+            d3 d{B.cx - A.cx, B.cy - A.cy, B.cz - A.cz};
             if (box.pbc) {
               if (box.L[0] > 0.0) d.x -= box.L[0] * rint(d.x * invL[0]);
               if (box.L[1] > 0.0) d.y -= box.L[1] * rint(d.y * invL[1]);
               if (box.L[2] > 0.0) d.z -= box.L[2] * rint(d.z * invL[2]);
             }
-            const double hr = sm.home.h[h] + sm.tile.h[u] + sm.home.r[h] + sm.tile.r[u];
-            double cc = hr + margin + skin;
-            if (dot(d, d) > cc * cc * (1.0 + 1e-9)) continue;
+            const double lim = A.r + B.r + margin + skin;
+            if (!seg_far(A, B, d, lim)) q2[atomicAdd(&sm.qn[1], 1)] = w;
+          }
+          __syncthreads();
+          const int n2 = sm.qn[1];
+          for (int e = threadIdx.x; e < n2; e += blockDim.x) {
+            const unsigned w = q2[e];
+            const int h = (int)(w >> 16), u = (int)(w & 0xffffu);
             const Seg A = sm.home.get(h);
             const Seg B = sm.tile.get(u);
-            double lim = A.r + B.r + margin + skin;
-            if (seg_far(A, B, d, lim)) continue;
+            const double lim = A.r + B.r + margin + skin;
             Narrow nr = narrow_pair(A, B, box);
             if (!(nr.d2 < lim * lim)) continue;
+            const int a = sm.hidx[h], b = sm.tidx[u];
+            const int ii = a < b ? a : b, j = a < b ? b : a;  // listed under the lower index
+            int pos = atomicAdd(&nbr_cnt[ii], 1);
+            if (pos < maxnb) nbr[(size_t)ii * maxnb + pos] = j;
+            else overflow = 1;
           }
-          int pos = atomicAdd(&nbr_cnt[i], 1);
-          if (pos < maxnb) nbr[(size_t)i * maxnb + pos] = j;
-          else overflow = 1;
+          __syncthreads();
         }
       }
     }

@@ -101,6 +101,9 @@ struct PhaseClock {
 // Dynamic shared memory of the persistent step: the small-solve arrays, or
 // the list-build tiles while a rebuild runs (phases never overlap).
 extern __shared__ __align__(16) unsigned char nsc_dyn_smem[];
+// list-build candidate queues, after the tiles
+constexpr int kBuildQ = 4096;
+constexpr size_t kBuildQOff = (sizeof(BuildSmem) + 15) & ~(size_t)15;
 
 struct SmemNsc {
   double red_d[32];
@@ -231,7 +234,9 @@ __device__ __noinline__ bool rebuild_phase(const Team& T, const NscView& V, Smem
     // crowded cells: the block splits the pairs of one home cell at a time
     for (int cell = rank; cell < g.ncells; cell += T.nb)
       build_cell_pairs(V.seg, g, V.box, invL, V.cell_start, V.cell_rods, V.margin, V.skin, V.all_pairs,
-                       V.nbr_cnt, V.nbr, V.maxnb, cell, *reinterpret_cast<BuildSmem*>(nsc_dyn_smem), overflow);
+                       V.nbr_cnt, V.nbr, V.maxnb, cell, *reinterpret_cast<BuildSmem*>(nsc_dyn_smem),
+                       reinterpret_cast<unsigned*>(nsc_dyn_smem + kBuildQOff),
+                       reinterpret_cast<unsigned*>(nsc_dyn_smem + kBuildQOff) + kBuildQ, kBuildQ, overflow);
   }
   if (!team_sync(T)) return false;
   for (int i = tid; i < n; i += TS) {
@@ -794,16 +799,17 @@ struct SmallSmem {
   alignas(16) __nv_bfloat16 wh[kStageWh];
 };
 static_assert(sizeof(unsigned long long) * 3 * kSmallB >= kStageSmallBytes, "MLP staging space");
-static_assert(sizeof(SmallSmem) >= sizeof(BuildSmem), "list-build tiles share the small-solve memory");
+static_assert(sizeof(SmallSmem) >= kBuildQOff + 2 * sizeof(unsigned) * kBuildQ,
+              "list-build tiles and queues share the small-solve memory");
 
 __device__ inline double small_block_max(double v, SmallSmem& S) {
   v = warp_max(v);
   __syncthreads();
   if ((threadIdx.x & 31) == 0) S.red[threadIdx.x >> 5] = v;
   __syncthreads();
-  double r = 0.0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, S.red[w]);
-  return r;  // every thread
+  // every warp combines the per-warp maxima itself (one load per lane)
+  const int lane = threadIdx.x & 31;
+  return warp_max(lane < (int)(blockDim.x >> 5) ? S.red[lane] : 0.0);  // every thread
 }
 
 // True when contact c has an entry in the warm cache of the previous step
