@@ -111,7 +111,7 @@ typedef struct rg_config {
   int32_t psor_order;            /* rg_psor_order; device supports COLORED */
 
   /* Neighbour-list broad phase (project-specific, no reference field). */
-  double skin;                   /* Verlet skin; <= 0: max(d/2, 0.075 L), means */
+  double skin;                   /* Verlet skin; <= 0: max(d/2, L/10), means */
   int32_t max_neighbors;         /* initial per-rod list capacity; <= 0 auto */
   int32_t team_blocks;           /* blocks of the persistent NSC team; 0 auto */
   int32_t nsc_mlp_scope;         /* learned start for: 0 contacts new since
@@ -122,7 +122,7 @@ typedef struct rg_config {
                                     warm cache is empty (default 3; -1: in
                                     every step)                              */
   int32_t near_skin_pct;         /* near-list skin, % of the Verlet skin (0:
-                                    automatic: 10 %, 50 % in all-pairs boxes) */
+                                    automatic: 5 %, 50 % in all-pairs boxes) */
   int32_t reserved[3];
 } rg_config;
 

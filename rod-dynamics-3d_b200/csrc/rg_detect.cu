@@ -313,7 +313,7 @@ cudaError_t detector_alloc(rg_system* s) {
   // Default skin: half a diameter, but at least a tenth of the rod length,
   // so thin rods (whose lists stay short, and whose per-step narrow phase
   // runs over the near list only) rebuild rarely.
-  d.skin = c.skin > 0 ? c.skin : fmax(0.5 * (dsum / n), 0.075 * (lsum / n)) + 1e-6;
+  d.skin = c.skin > 0 ? c.skin : fmax(0.5 * (dsum / n), 0.1 * (lsum / n)) + 1e-6;
   d.cut_center = 2.0 * (hmax + rmax) + d.margin + d.skin;
   d.all_pairs = false;
   GridDev gd{};
@@ -360,7 +360,7 @@ cudaError_t detector_alloc(rg_system* s) {
   if (c.model == RG_MODEL_NSC) {
     // all-pairs boxes rebuild the near list from every pair: a wider near
     // skin makes those rebuilds rare
-    d.near_skin = (c.near_skin_pct > 0 ? 0.01 * c.near_skin_pct : (d.all_pairs ? 0.5 : 0.1)) * d.skin;
+    d.near_skin = (c.near_skin_pct > 0 ? 0.01 * c.near_skin_pct : (d.all_pairs ? 0.5 : 0.05)) * d.skin;
     if ((e = cudaMalloc(&d.near, sizeof(int2) * (size_t)n * d.maxnb))) return e;
     if ((e = cudaMalloc(&d.ref2, sizeof(double) * 6 * (size_t)n))) return e;
     if ((e = cudaMalloc(&d.moved, (size_t)n))) return e;
