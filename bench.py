@@ -289,9 +289,7 @@ def run_ours(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded RSA packings, Gaussian velocities)",
-        "config": {"workload": f"batch: {len(items)} NSC systems, N log-uniform [500, 20000] "
-                               f"(total {n_total} rods), AR 5/10/20/40, phi U[0.05,0.25] capped 1.6/AR, "
-                               f"mu U[0,1], PSOR omega=1 tol=1e-6 max 500 sweeps, dt=5e-4, learned warm start",
+        "config": {"workload": batch_workload(len(items)),
                    "rods": n_total, "systems": len(items), "parallelism": f"replicas x{world}",
                    "schedule": sched, "autotune_ms": tune,
                    "l2": "no flush: state persists step to step (inputs 133 MB > L2 across members)"},
@@ -384,6 +382,14 @@ def run_single(args, rank, world):
     return out
 
 
+def batch_workload(nsys):
+    """The headline workload's name (both arms print it; the rod count is
+    the separate 'rods' key)."""
+    return (f"batch: {nsys} NSC systems, N log-uniform [500, 20000], AR 5/10/20/40, "
+            f"phi U[0.05,0.25] capped 1.6/AR, mu U[0,1], PSOR omega=1 tol=1e-6 max 500 sweeps, dt=5e-4, "
+            f"learned warm start")
+
+
 def run_reference(args, steps, warmup, threads=0):
     """The reference's own FP32 CPU path (oracle/_ref) on a sample of the
     batch members (every 8th by size), stepped one after the other."""
@@ -439,10 +445,13 @@ def main():
         except Exception as e:  # noqa: BLE001
             print(json.dumps({"impl": "reference", "unavailable": f"reference build not loadable: {e}"}))
             return
+        from rodgpu import scene
+        specs = [s for s in scene.batch_members(256, seed=args.seed) if s["model"] == "nsc"]
         line = {"impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": "rod-steps/s",
-                "n_gpus": 0, "steps": max(1, min(args.steps, 2)), "warmup": min(args.warmup, 1),
+                "n_gpus": world, "steps": max(1, min(args.steps, 2)), "warmup": min(args.warmup, 1),
                 "higher_is_better": True, "dtype": "f32",
-                "config": {"workload": "batch (NSC half): sample of the same 128 seeded systems"},
+                "config": {"workload": batch_workload(len(specs)),
+                           "sample": "every 8th system by size, stepped one after the other on the host"},
                 "cpu_baseline": {"value": round(v, 2), "unit": "rod-steps/s", "cores": th, "kind": "reference",
                                  "sample": sample},
                 "e2e": {"value": round(v, 2), "unit": "rod-steps/s", "h2d_bytes_per_step": 0,
