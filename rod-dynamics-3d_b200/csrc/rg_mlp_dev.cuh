@@ -51,9 +51,12 @@ __device__ inline unsigned pack_bf16(float lo, float hi) {
 }
 __device__ inline float silu(float z) { return z / (1.0f + __expf(-z)); }
 
+// Not volatile: the MMA has no side effects, so the compiler may interleave
+// independent accumulator chains (a volatile statement keeps every MMA in
+// program order, and each then waits for the one before it).
 __device__ inline void mma_bf16(float* c, unsigned a0, unsigned a1, unsigned a2, unsigned a3, unsigned b0,
                                 unsigned b1) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
       "{%0,%1,%2,%3};\n"
       : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
@@ -71,30 +74,39 @@ __device__ inline void load_b(const __nv_bfloat16* W, int ldk, int nt, int kt, i
 }
 
 // One hidden layer 128 -> 128: a[kt] (4 regs each, 8 k-tiles) -> out a;
-// W row-major [n][k] with leading dimension ldw.
+// W row-major [n][k] with leading dimension ldw.  Four n-tiles at a time:
+// their accumulation chains are independent, so four MMAs are in flight
+// (each chain still adds its k-tiles in order).
 __device__ inline void hidden_layer(unsigned (&a)[8][4], const __nv_bfloat16* W, int ldw, const float* bias,
                                     int lane) {
   const int t = lane & 3;
   unsigned na[8][4];
 #pragma unroll
-  for (int kk = 0; kk < 8; ++kk) {
-    float acc[2][4];
+  for (int grp = 0; grp < 4; ++grp) {
+    float acc[4][4];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int nt = 2 * kk + h;
+    for (int h = 0; h < 4; ++h) {
+      const int nt = 4 * grp + h;
       const float bl = bias[nt * 8 + 2 * t], bh = bias[nt * 8 + 2 * t + 1];
       acc[h][0] = bl; acc[h][1] = bh; acc[h][2] = bl; acc[h][3] = bh;
+    }
 #pragma unroll
-      for (int kt = 0; kt < 8; ++kt) {
+    for (int kt = 0; kt < 8; ++kt) {
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
         unsigned b0, b1;
-        load_b(W, ldw, nt, kt, lane, b0, b1);
+        load_b(W, ldw, 4 * grp + h, kt, lane, b0, b1);
         mma_bf16(acc[h], a[kt][0], a[kt][1], a[kt][2], a[kt][3], b0, b1);
       }
     }
-    na[kk][0] = pack_bf16(silu(acc[0][0]), silu(acc[0][1]));
-    na[kk][1] = pack_bf16(silu(acc[0][2]), silu(acc[0][3]));
-    na[kk][2] = pack_bf16(silu(acc[1][0]), silu(acc[1][1]));
-    na[kk][3] = pack_bf16(silu(acc[1][2]), silu(acc[1][3]));
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int kk = 2 * grp + q;
+      na[kk][0] = pack_bf16(silu(acc[2 * q][0]), silu(acc[2 * q][1]));
+      na[kk][1] = pack_bf16(silu(acc[2 * q][2]), silu(acc[2 * q][3]));
+      na[kk][2] = pack_bf16(silu(acc[2 * q + 1][0]), silu(acc[2 * q + 1][1]));
+      na[kk][3] = pack_bf16(silu(acc[2 * q + 1][2]), silu(acc[2 * q + 1][3]));
+    }
   }
 #pragma unroll
   for (int kk = 0; kk < 8; ++kk)
