@@ -49,7 +49,10 @@ __device__ inline unsigned pack_bf16(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<unsigned*>(&v);
 }
-__device__ inline float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU with the fast exponential and division: the network runs in BF16, so
+// their few-ulp FP32 error is far below its resolution, and a warp's
+// inference is a long chain of these (three layers x 64 values per lane).
+__device__ inline float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 
 // Not volatile: the MMA has no side effects, so the compiler may interleave
 // independent accumulator chains (a volatile statement keeps every MMA in
