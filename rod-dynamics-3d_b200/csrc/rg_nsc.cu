@@ -392,7 +392,9 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
     return -1;
   }
   // contacts in pair order: one word (64 pairs) per thread, scanned by
-  // population count
+  // population count, places each hit's pair in its slot; then one thread
+  // per slot runs the exact narrow phase (a word may hold several hits,
+  // which one thread would otherwise evaluate one after the other)
   int run = prefix;
   for (int wb = wlo; wb < whi; wb += blockDim.x) {
     const int w = wb + threadIdx.x;
@@ -400,13 +402,19 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
     int tot;
     int slot = run + block_excl_scan(__popcll(m), sm.scan_w, tot);
     for (unsigned long long r = m; r; r &= r - 1) {
-      const int p = (w << 6) + __ffsll((long long)r) - 1;
-      const int2 pr = V.near[p];
-      const Seg A = V.seg[pr.x], B = V.seg[pr.y];
-      const Narrow nr = narrow_pair(A, B, V.box);
-      write_contact(V.con, slot++, pr.x, pr.y, A.r + B.r, nr);
+      const int2 pr = V.near[(w << 6) + __ffsll((long long)r) - 1];
+      V.con.a[slot] = pr.x;
+      V.con.b[slot] = pr.y;
+      ++slot;
     }
     run += tot;
+  }
+  __syncthreads();
+  for (int c = prefix + (int)threadIdx.x; c < run; c += blockDim.x) {
+    const int a = V.con.a[c], b = V.con.b[c];
+    const Seg A = V.seg[a], B = V.seg[b];
+    const Narrow nr = narrow_pair(A, B, V.box);
+    write_contact(V.con, c, a, b, A.r + B.r, nr);
   }
   if (rank == 0 && threadIdx.x == 0) {
     ctl->contacts = total;
