@@ -222,3 +222,18 @@ def test_nsc_team_larger_than_pair_ranges():
     assert sg["psor_sweeps"] == so["psor_sweeps"]
     assert sg["contacts"] == so["contacts"]
     assert_contacts_equal(g, o, 0.0)
+
+
+def test_nsc_25_step_call_keeps_exact_contacts():
+    # 25 steps in one call (carried hit bits, near-list rebuilds inside the
+    # launch, a two-block team): the contact sets stay the oracle's
+    sc = packed_scene(1200, d=0.05, phi=0.2, seed=18, squeeze=0.97, sigma_v=0.5, sigma_w=0.5)
+    g, o = make_pair(sc, model="nsc", dt=5e-4, nsc_velocity_iters=500, team_blocks=2)
+    sg = g.step(25)
+    so = o.step(25)
+    a, b = g.get_state(), o.get_state()
+    for k in ("x", "q", "v", "w"):
+        assert rel_err(a[k], b[k]) < TOL, k
+    assert sg["psor_sweeps"] == so["psor_sweeps"]
+    assert sg["contacts"] == so["contacts"]
+    assert_contacts_equal(g, o, 0.0)
