@@ -648,7 +648,6 @@ bool grow(rg_system* s, int err) {
   }
   if (err & ERR_NBR_CAP) {
     int nb = s->det.maxnb * 2;
-    int ncells = s->det.ncells;
     detector_free(s);
     s->det.maxnb = nb;
     if (detector_alloc(s)) return false;
@@ -656,7 +655,6 @@ bool grow(rg_system* s, int err) {
       s->scan.free_();
       s->scan.alloc(s->det.ncells + 1);
     }
-    (void)ncells;
     grew = true;
   }
   return grew;
