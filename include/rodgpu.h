@@ -123,7 +123,17 @@ typedef struct rg_config {
                                     every step)                              */
   int32_t near_skin_pct;         /* near-list skin, % of the Verlet skin (0:
                                     automatic: 5 %, 50 % in all-pairs boxes) */
-  int32_t reserved[3];
+  /* Bounded device waits.  Every team barrier of the persistent step polls
+   * at most spin_limit times (0: the default 2e7 polls, about 1-2 s) and
+   * then records RG_ERR_TIMEOUT; every block of the launch then returns and
+   * the call restores the state it started from. */
+  int32_t spin_limit;
+  /* Test hook for failure detection, 0 in normal use: the team barriers of
+   * the persistent step expect this many more blocks than the team has, so
+   * their waits run out after spin_limit polls and the call returns
+   * RG_ERR_TIMEOUT (no fault, no hang: the wait is the bounded one above). */
+  int32_t test_absent_blocks;
+  int32_t reserved[1];
 } rg_config;
 
 /* Per-call statistics (the profile-CSV columns of main.cpp:3276-3355). */
@@ -245,7 +255,12 @@ int rg_get_phase_times(const rg_system* sys, double* ms, int n);
  *   pbc_min / pbc_max: HOST arrays of 3 (ignored when pbc_enabled == 0).
  *   pairs[2*cap], geom[12*cap] (may be NULL): device outputs, layout of
  *     rg_detect; count[1]: device, receives the contact count even when it
- *     exceeds cap (then only cap contacts are written).
+ *     exceeds cap (then only the first cap contacts are written).  Unlike
+ *     rg_detect, an overflow is NOT reported by the return code: the count
+ *     is known only on the device, after the call has returned.  Read
+ *     *count once the stream has synchronised and compare it with cap; a
+ *     larger count means the list is truncated and the call must be
+ *     repeated with more room.
  *   stream: a cudaStream_t (NULL: the default stream).  The call only
  *     enqueues work; synchronise the stream before reading the outputs.
  * Returns RG_ERR_CAPACITY when n > RG_NOALLOC_MAX_BODIES and RG_ERR_ARG for

@@ -18,7 +18,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "librodoracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "librodref.so")
-REF_TREE = "/root/reference"
+# The reference source tree: $RG_REFERENCE_TREE, else a checkout named
+# "reference" beside this repository.  Absent on machines that only run the
+# prebuilt libraries.
+REF_TREE = os.environ.get("RG_REFERENCE_TREE") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 _d = ctypes.c_double
 _i = ctypes.c_int32
@@ -29,7 +32,7 @@ def build(ref=True):
     """Compiles the oracle (and the reference, when its tree is present)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if ref and os.path.isdir(REF_TREE):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
 
 
 def _p(a, t=_d):

@@ -546,6 +546,11 @@ int rg_set_state(rg_system* s, const double* x, const double* q, const double* v
     }
     for (int k = 0; k < 4; ++k) b[(size_t)(3 + k) * n + i] = q[4 * i + k];
   }
+  // A NaN or infinite component would reach the cell grid and every force
+  // law; it is refused here, before any device work, and the device state
+  // stays what it was.
+  for (size_t k = 0; k < 19 * (size_t)n; ++k)
+    if (!std::isfinite(b[k])) return fail(s, RG_ERR_NONFINITE, "non-finite component in the uploaded state");
   // The neighbour lists need no forced rebuild: the displacement check
   // against the positions of the last build catches any jump of the state.
   RG_TRY(cudaMemcpyAsync(s->d_state, b, sizeof(double) * 19 * (size_t)n, cudaMemcpyHostToDevice,
@@ -685,11 +690,21 @@ cudaError_t reset_call_ctl(rg_system* s, const Snapshot& sn) {
 int resolve_call(rg_system* s, Snapshot& sn, int err, bool* retry) {
   *retry = false;
   if (!err) return RG_OK;
+  // Every failure puts back the state, history and warm cache the call
+  // started from, so the handle stays usable after an error status.
+  cudaError_t e = restore_snapshot(s, sn);
+  if (e) return cuda_fail(s, e, "restore");
+  if (err & (ERR_TIMEOUT | ERR_NONFINITE | ERR_COLOR)) {
+    std::memcpy(s->h_ctl, sn.ctl.data(), s->ctl_bytes);
+    reinterpret_cast<Ctl*>(s->h_ctl)->rebuild = 1;
+    s->contacts_fresh = false;
+    e = cudaMemcpyAsync(s->d_ctl, s->h_ctl, s->ctl_bytes, cudaMemcpyHostToDevice, s->stream);
+    if (!e) e = cudaStreamSynchronize(s->stream);
+    if (e) return cuda_fail(s, e, "restore control words");
+  }
   if (err & ERR_TIMEOUT) return fail(s, RG_ERR_TIMEOUT, "a device-side barrier timed out");
   if (err & ERR_NONFINITE) return fail(s, RG_ERR_NONFINITE, "non-finite body state");
   if (err & ERR_COLOR) return fail(s, RG_ERR_CAPACITY, "contact graph needs more than 64 colours");
-  cudaError_t e = restore_snapshot(s, sn);
-  if (e) return cuda_fail(s, e, "restore");
   if (!grow(s, err)) return fail(s, RG_ERR_CAPACITY, "could not grow device buffers");
   e = take_snapshot(s, sn);
   if (e) return cuda_fail(s, e, "snapshot");
@@ -781,21 +796,26 @@ int rg_detect(rg_system* s, double delta, int32_t* pairs, double* geom, double* 
     RG_TRY(cudaMemcpyAsync(h, s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost, s->stream), "ctl");
     RG_TRY(cudaStreamSynchronize(s->stream), "detect");
     if (!h->err) break;
+    if (h->err & ERR_TIMEOUT) return fail(s, RG_ERR_TIMEOUT, "a device-side wait timed out in detection");
+    if (h->err & ERR_NONFINITE) return fail(s, RG_ERR_NONFINITE, "non-finite body state");
+    if (attempt == 7) return fail(s, RG_ERR_CAPACITY, "capacity retries exhausted");
     if (!grow(s, h->err)) return fail(s, RG_ERR_CAPACITY, "could not grow device buffers");
     force_rebuild(s);
   }
   s->contacts_fresh = false;  // the force path must rebuild its CSR
   const int C = s->h_ctl->contacts;
+  if (C < 0 || C > s->ccap) return fail(s, RG_ERR_CAPACITY, "contact count exceeds the contact buffer");
   *n = (size_t)C;
   size_t m = cap < (size_t)C ? cap : (size_t)C;
   if (m) {
     std::vector<int> a(m), b(m), t(m);
-    cudaMemcpy(a.data(), s->con.a, sizeof(int) * m, cudaMemcpyDeviceToHost);
-    cudaMemcpy(b.data(), s->con.b, sizeof(int) * m, cudaMemcpyDeviceToHost);
-    cudaMemcpy(t.data(), s->con.type, sizeof(int) * m, cudaMemcpyDeviceToHost);
+    RG_TRY(cudaMemcpy(a.data(), s->con.a, sizeof(int) * m, cudaMemcpyDeviceToHost), "contacts");
+    RG_TRY(cudaMemcpy(b.data(), s->con.b, sizeof(int) * m, cudaMemcpyDeviceToHost), "contacts");
+    RG_TRY(cudaMemcpy(t.data(), s->con.type, sizeof(int) * m, cudaMemcpyDeviceToHost), "contacts");
     std::vector<double> g(14 * m);
     for (int k = 0; k < 14; ++k)
-      cudaMemcpy(g.data() + (size_t)k * m, s->con.comp(k), sizeof(double) * m, cudaMemcpyDeviceToHost);
+      RG_TRY(cudaMemcpy(g.data() + (size_t)k * m, s->con.comp(k), sizeof(double) * m, cudaMemcpyDeviceToHost),
+             "contacts");
     for (size_t i = 0; i < m; ++i) {
       if (pairs) { pairs[2 * i] = a[i]; pairs[2 * i + 1] = b[i]; }
       if (geom) {
@@ -857,7 +877,10 @@ int rg_compute_forces(rg_system* s, double* f, double* tau, double* pe) {
     RG_TRY(cudaMemcpyAsync(h, s->d_ctl, s->ctl_bytes, cudaMemcpyDeviceToHost, s->stream), "ctl");
     RG_TRY(cudaStreamSynchronize(s->stream), "forces");
     if (!h->err) break;
-    if (h->err & (ERR_TIMEOUT | ERR_NONFINITE | ERR_COLOR)) return fail(s, RG_ERR_CUDA, "force evaluation failed");
+    if (h->err & ERR_TIMEOUT) return fail(s, RG_ERR_TIMEOUT, "a device-side wait timed out in force evaluation");
+    if (h->err & ERR_NONFINITE) return fail(s, RG_ERR_NONFINITE, "non-finite body state");
+    if (h->err & ERR_COLOR) return fail(s, RG_ERR_CAPACITY, "force evaluation failed");
+    if (attempt == 7) return fail(s, RG_ERR_CAPACITY, "capacity retries exhausted");
     int err = h->err;
     RG_TRY(restore_snapshot(s, sn), "restore");
     if (!grow(s, err)) return fail(s, RG_ERR_CAPACITY, "could not grow device buffers");

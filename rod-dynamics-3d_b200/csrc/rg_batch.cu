@@ -84,6 +84,8 @@ struct rg_batch {
   // bulk state transfer: member table and device staging (x, q, v, w)
   void* d_bulk = nullptr;
   double* d_stage = nullptr;
+  int* d_bulk_bad = nullptr;   // non-finite flag of the last bulk upload
+  int* h_bulk_bad = nullptr;   // page-locked mirror
   long long total = 0;
 };
 
@@ -107,8 +109,20 @@ __device__ inline int bulk_find(const BulkMember* m, int nm, long long g) {
 // Concatenated host-layout arrays (x[3T], q[4T], v[3T], w[3T]) into every
 // member's component arrays; forces and torques are cleared, as
 // rg_set_state does without them.
+// Flags a non-finite value among the staged x, q, v, w (13 T doubles,
+// contiguous); the scatter that follows leaves every member's state as it
+// was when the flag is set.
+__global__ void k_bulk_check(const double* staged, long long count, int* bad) {
+  int any = 0;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < count;
+       g += (long long)gridDim.x * blockDim.x)
+    any |= !isfinite(staged[g]);
+  if (__syncthreads_or(any) && threadIdx.x == 0) atomicOr(bad, 1);
+}
+
 __global__ void k_bulk_scatter(const BulkMember* m, int nm, long long T, const double* x, const double* q,
-                               const double* v, const double* w) {
+                               const double* v, const double* w, const int* bad) {
+  if (*(volatile const int*)bad) return;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < T;
        g += (long long)gridDim.x * blockDim.x) {
     const BulkMember M = m[bulk_find(m, nm, g)];
@@ -678,7 +692,8 @@ int rg_batch_destroy(rg_batch* b) {
     rg_destroy(s);
   }
   cudaFree(b->d_views); cudaFree(b->d_teams); cudaFree(b->d_members); cudaFree(b->d_bars); cudaFree(b->d_team_ns);
-  cudaFree(b->d_bulk); cudaFree(b->d_stage);
+  cudaFree(b->d_bulk); cudaFree(b->d_stage); cudaFree(b->d_bulk_bad);
+  if (b->h_bulk_bad) cudaFreeHost(b->h_bulk_bad);
   cudaFree(b->d_segs); cudaFree(b->d_ctls); cudaFree(b->d_ctlbuf);
   if (b->h_ctlbuf) cudaFreeHost(b->h_ctlbuf);
   if (b->ev0) cudaEventDestroy(b->ev0);
@@ -726,7 +741,8 @@ int bulk_setup(rg_batch* b) {
   }
   b->total = off;
   if (cudaMalloc(&b->d_bulk, sizeof(BulkMember) * b->n) ||
-      cudaMalloc(&b->d_stage, sizeof(double) * 13 * (size_t)off)) {
+      cudaMalloc(&b->d_stage, sizeof(double) * 13 * (size_t)off) ||
+      cudaMalloc(&b->d_bulk_bad, sizeof(int)) || cudaMallocHost(&b->h_bulk_bad, sizeof(int))) {
     cudaGetLastError();
     return bfail(b, RG_ERR_CUDA, "bulk staging allocation");
   }
@@ -752,10 +768,15 @@ int rg_batch_set_state_all(rg_batch* b, const double* x, const double* q, const 
   cudaMemcpyAsync(sq, q, sizeof(double) * 4 * T, cudaMemcpyHostToDevice, b->stream);
   cudaMemcpyAsync(sv, v, sizeof(double) * 3 * T, cudaMemcpyHostToDevice, b->stream);
   cudaMemcpyAsync(sw, w, sizeof(double) * 3 * T, cudaMemcpyHostToDevice, b->stream);
-  RGL k_bulk_scatter<<<592, 256, 0, b->stream>>>(static_cast<const BulkMember*>(b->d_bulk), b->n, T, sx, sq, sv, sw);
+  cudaMemsetAsync(b->d_bulk_bad, 0, sizeof(int), b->stream);
+  RGL k_bulk_check<<<592, 256, 0, b->stream>>>(sx, 13 * T, b->d_bulk_bad);
+  RGL k_bulk_scatter<<<592, 256, 0, b->stream>>>(static_cast<const BulkMember*>(b->d_bulk), b->n, T, sx, sq, sv, sw,
+                                                 b->d_bulk_bad);
+  cudaMemcpyAsync(b->h_bulk_bad, b->d_bulk_bad, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
   cudaError_t e = cudaStreamSynchronize(b->stream);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e) return bfail(b, RG_ERR_CUDA, std::string("bulk set_state: ") + cudaGetErrorString(e));
+  if (*b->h_bulk_bad) return bfail(b, RG_ERR_NONFINITE, "non-finite component in the uploaded states (nothing changed)");
   for (rg_system* s : b->sys) {
     s->state_set = true;
     s->contacts_fresh = false;

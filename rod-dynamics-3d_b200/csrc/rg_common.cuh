@@ -268,19 +268,25 @@ __device__ inline int block_excl_scan(int v, int* sh_warp, int& total) {
 
 // ---- bounded grid barrier ----------------------------------------------------
 // Sense-free generation barrier for co-resident (cooperatively launched)
-// blocks.  Every wait is bounded: after kSpinLimit polls the block records
-// ERR_TIMEOUT and returns false; callers then leave the kernel.
+// blocks.  Every wait is bounded: after `limit` polls (kSpinLimit by
+// default) the block records ERR_TIMEOUT and returns false; the other
+// waiters see the bit within 64 polls and return false too; callers then
+// leave the kernel.  `absent` counts blocks that are expected but never
+// arrive (a failure-detection test hook, 0 in normal use).
+constexpr long long kSpinLimit = 20000000;  // ~1-2 s with the backoff below
 struct GridBar {
   unsigned int* count;
   unsigned int* gen;
   int* err;
+  long long limit = kSpinLimit;
+  unsigned int absent = 0;
 };
-constexpr long long kSpinLimit = 20000000;  // ~1-2 s with the backoff below
 
 // nb = number of participating blocks (blocks 0..nb-1); nb == 1 is a plain
-// __syncthreads.
+// __syncthreads unless blocks are marked absent.
 __device__ inline bool grid_sync(const GridBar& g, unsigned int nb) {
   __syncthreads();
+  nb += g.absent;
   if (nb <= 1) return !(*(volatile int*)g.err & ERR_TIMEOUT);
   __shared__ int s_ok;
   if (threadIdx.x == 0) {
@@ -298,7 +304,7 @@ __device__ inline bool grid_sync(const GridBar& g, unsigned int nb) {
       while (gen.load(cuda::memory_order_acquire) == my) {
         ++it;
         if ((it & 63) == 0 && (*(volatile int*)g.err & ERR_TIMEOUT)) { s_ok = 0; break; }
-        if (it > kSpinLimit) {
+        if (it > g.limit) {
           atomicOr(g.err, ERR_TIMEOUT);
           s_ok = 0;
           break;

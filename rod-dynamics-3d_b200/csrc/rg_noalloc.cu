@@ -59,18 +59,28 @@ __device__ inline bool na_pair(const Seg& A, const Seg& B, const Box& box, doubl
 }
 
 // Contacts of rod i with every j > i (both static: skipped, as the naive
-// detector does, contact_detector.cpp:236-239).
+// detector does, contact_detector.cpp:236-239).  One warp per rod i, its
+// lanes striding over j: rows are triangular (rod 0 tests n-1 partners, rod
+// n-1 none), and many small warp tasks keep the SMs evenly loaded.
+__device__ inline bool na_candidate(int i, int j, const Seg& A, const Seg* seg, const Box& box, double delta,
+                                    const double* inv_mass, bool a_static, Narrow& nr) {
+  if (a_static && !(inv_mass[j] > 0.0)) return false;
+  return na_pair(A, seg[j], box, delta, nr);
+}
+
 __global__ void k_na_count(int n, Box box, double delta, const double* inv_mass, NoAllocScratch* S) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
     const Seg A = S->seg[i];
     const bool a_static = inv_mass && !(inv_mass[i] > 0.0);
     int c = 0;
-    for (int j = i + 1; j < n; ++j) {
-      if (a_static && !(inv_mass[j] > 0.0)) continue;
+    for (int j = i + 1 + lane; j < n; j += 32) {
       Narrow nr;
-      if (na_pair(A, S->seg[j], box, delta, nr)) ++c;
+      if (na_candidate(i, j, A, S->seg, box, delta, inv_mass, a_static, nr)) ++c;
     }
-    S->count[i] = c;
+    c = warp_sum_i(c);
+    if (lane == 0) S->count[i] = c;
   }
 }
 
@@ -89,33 +99,41 @@ __global__ void k_na_scan(int n, NoAllocScratch* S) {
   if (threadIdx.x == 0) S->offset[n] = carry;
 }
 
+// Writes rod i's contacts in ascending j: each round of 32 candidates is
+// ballot-compacted, so the output order is the (i, j) order of rg_detect.
 __global__ void k_na_write(int n, Box box, double delta, const double* inv_mass, NoAllocScratch* S,
                            int32_t* pairs, double* geom, int cap, int32_t* count_out) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *count_out = S->offset[n];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
     if (S->count[i] == 0) continue;
     const Seg A = S->seg[i];
     const bool a_static = inv_mass && !(inv_mass[i] > 0.0);
     int o = S->offset[i];
-    for (int j = i + 1; j < n; ++j) {
-      if (a_static && !(inv_mass[j] > 0.0)) continue;
+    for (int j0 = i + 1; j0 < n; j0 += 32) {
+      const int j = j0 + lane;
       Narrow nr;
-      if (!na_pair(A, S->seg[j], box, delta, nr)) continue;
-      if (o < cap) {
-        pairs[2 * o] = i;
-        pairs[2 * o + 1] = j;
+      const bool hit = j < n && na_candidate(i, j, A, S->seg, box, delta, inv_mass, a_static, nr);
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      const int slot = o + __popc(m & lt);
+      if (hit && slot < cap) {
+        pairs[2 * slot] = i;
+        pairs[2 * slot + 1] = j;
         if (geom) {
+          const Seg B = S->seg[j];
           double dist = sqrt(nr.d2);
           d3 diff = nr.pb - nr.pa;
           d3 nv = dist > 1e-10 ? diff / dist : mk3(1, 0, 0);
-          double* gg = geom + 12 * (size_t)o;
+          double* gg = geom + 12 * (size_t)slot;
           gg[0] = nr.pa.x; gg[1] = nr.pa.y; gg[2] = nr.pa.z;
           gg[3] = nr.pb.x; gg[4] = nr.pb.y; gg[5] = nr.pb.z;
           gg[6] = nv.x; gg[7] = nv.y; gg[8] = nv.z;
-          gg[9] = dist; gg[10] = A.r + S->seg[j].r; gg[11] = (double)contact_type(nr.s, nr.t);
+          gg[9] = dist; gg[10] = A.r + B.r; gg[11] = (double)contact_type(nr.s, nr.t);
         }
       }
-      ++o;
+      o += __popc(m);
     }
   }
 }
@@ -168,11 +186,12 @@ extern "C" int rg_detect_noalloc(const double* x, const double* q, const double*
   if (rc != RG_OK) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int g = n > 0 ? (n + kNaBS - 1) / kNaBS : 1;
+  const int gw = n > 0 ? (n + kNaBS / 32 - 1) / (kNaBS / 32) : 1;  // one warp per rod
   if (n > 0) {
     RGL k_na_seg<<<g, kNaBS, 0, st>>>(x, q, radius, half_height, n, S);
-    RGL k_na_count<<<g, kNaBS, 0, st>>>(n, box, delta, inv_mass, S);
+    RGL k_na_count<<<gw, kNaBS, 0, st>>>(n, box, delta, inv_mass, S);
   }
   RGL k_na_scan<<<1, 1024, 0, st>>>(n, S);
-  RGL k_na_write<<<g, kNaBS, 0, st>>>(n, box, delta, inv_mass, S, pairs, geom, cap, count);
+  RGL k_na_write<<<gw, kNaBS, 0, st>>>(n, box, delta, inv_mass, S, pairs, geom, cap, count);
   return cudaGetLastError() == cudaSuccess ? RG_OK : RG_ERR_CUDA;
 }

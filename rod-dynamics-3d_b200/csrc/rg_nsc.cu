@@ -44,18 +44,20 @@ struct Team {
   int b0, nb;
   unsigned int* bar;
   int* err;
+  long long spin_limit;   // polls per barrier wait before ERR_TIMEOUT
+  unsigned int absent;    // test hook: blocks the barriers wait for in vain
   __device__ int rank() const { return (int)blockIdx.x - b0; }
   __device__ int tid() const { return rank() * (int)blockDim.x + (int)threadIdx.x; }
   __device__ int size() const { return nb * (int)blockDim.x; }
 };
 
 __device__ inline bool team_sync(const Team& T) {
-  GridBar g{T.bar, T.bar + 1, T.err};
+  GridBar g{T.bar, T.bar + 1, T.err, T.spin_limit, T.absent};
   return grid_sync(g, (unsigned)T.nb);
 }
 // Barrier among the first nsub blocks of the team (the others must not call it).
 __device__ inline bool team_sync_sub(const Team& T, int nsub) {
-  GridBar g{T.bar + 2, T.bar + 3, T.err};
+  GridBar g{T.bar + 2, T.bar + 3, T.err, T.spin_limit, T.absent};
   return grid_sync(g, (unsigned)nsub);
 }
 
@@ -1470,7 +1472,9 @@ __global__ void __launch_bounds__(kBlock, 1) k_nsc_run(const NscView* views, con
     bool any = false;
     for (int m = td.first; m < td.first + td.count; ++m) {
       const NscView& V = views[members ? members[m] : m];
-      Team T{td.b0, td.nb, td.bar, &V.ctl->err};
+      Team T{td.b0, td.nb, td.bar, &V.ctl->err,
+             V.cfg.spin_limit > 0 ? (long long)V.cfg.spin_limit : kSpinLimit,
+             V.cfg.test_absent_blocks > 0 ? (unsigned)V.cfg.test_absent_blocks : 0u};
       const bool timer = threadIdx.x == 0 && (int)blockIdx.x == td.b0;
       const unsigned long long t0 = timer ? gtimer() : 0ull;
       any |= nsc_step(T, V, sm, S);

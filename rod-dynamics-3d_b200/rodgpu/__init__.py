@@ -44,7 +44,8 @@ class RgConfig(ctypes.Structure):
         ("nsc_tol", _d), ("nsc_velocity_iters", _i), ("nsc_position_stabilization", _i),
         ("nsc_position_iters", _i), ("nsc_position_psor_iters", _i), ("nsc_warm_start", _i),
         ("psor_order", _i), ("skin", _d), ("max_neighbors", _i), ("team_blocks", _i),
-        ("nsc_mlp_scope", _i), ("nsc_mlp_min_sweeps", _i), ("near_skin_pct", _i), ("reserved", _i * 3),
+        ("nsc_mlp_scope", _i), ("nsc_mlp_min_sweeps", _i), ("near_skin_pct", _i),
+        ("spin_limit", _i), ("test_absent_blocks", _i), ("reserved", _i * 1),
     ]
 
 

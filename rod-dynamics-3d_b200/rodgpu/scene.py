@@ -7,7 +7,7 @@ V = pi r^2 L + 4/3 pi r^3 used by the reference's broad-phase benchmark
 (src/tools/benchmark_broadphase.cpp:104-106).
 
 Workloads (rod counts and physics as stated; values the description leaves
-open are fixed here and documented in DESIGN.md):
+open are fixed here):
   hm_small    N=1000,  L=1, d=0.1,  phi=0.10, Hertz-Mindlin E=1e5 nu=0.3 e=0.5
               mu=0.5, dt=1e-4, 1000 steps
   nsc_dense   N=20000, L=1, d=0.05, phi=0.20, PSOR mu=0.3, omega=1, tol 1e-6,
