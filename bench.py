@@ -289,10 +289,10 @@ def run_ours(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded RSA packings, Gaussian velocities)",
-        "config": {"workload": batch_workload(len(items)),
-                   "rods": n_total, "systems": len(items), "parallelism": f"replicas x{world}",
-                   "schedule": sched, "autotune_ms": tune,
-                   "l2": "no flush: state persists step to step (inputs 133 MB > L2 across members)"},
+        "config": headline_config(n_total, len(items)),
+        "parallelism": f"replicas x{world}",
+        "tuning": {"schedule": sched, "autotune_ms": tune},
+        "psor_compliance": compliance(res, len(items), args.steps),
         "comparison": {"plain_single_system": single,
                        "plain_batched": {k: v for k, v in res_plain.items() if k not in ("ms", "bytes")},
                        "learned_batched": {k: v for k, v in res.items() if k not in ("ms", "bytes")},
@@ -308,6 +308,18 @@ def run_ours(args, rank, world):
         "clocks": clk.summary(),
     }
     return out
+
+
+def compliance(res, nsys, steps):
+    """How many system-steps met the PSOR tolerance (residual <= 1e-6 by the
+    reference's definition, nsc_contact.cpp:546-551) and how many stopped at
+    the sweep cap; 'value' counts every rod-step, the capped ones included."""
+    total = nsys * steps
+    nc = int(res["not_converged_steps"])
+    return {"system_steps": total, "met_tolerance": total - nc, "stopped_at_max_sweeps": nc,
+            "fraction_met": round((total - nc) / total, 5) if total else None,
+            "max_final_residual": res["max_residual"],
+            "value_includes_capped_steps": True}
 
 
 def run_batch_only(args, rank, world):
@@ -390,15 +402,28 @@ def batch_workload(nsys):
             f"learned warm start")
 
 
-def run_reference(args, steps, warmup, threads=0):
-    """The reference's own FP32 CPU path (oracle/_ref) on a sample of the
-    batch members (every 8th by size), stepped one after the other."""
-    from oracle import Reference
-    import rodgpu
-    from rodgpu import scene
+def reference_scenes(args, every=1):
+    """The batch members as (config, scene), built by the reference library
+    oracle/_ref/librodref.so, which compiles this repository's scene
+    generator and config defaults beside the reference's physics sources:
+    the packings and configurations are bit-identical to the GPU arm's, and
+    no library of this repository is loaded.  every=k keeps every k-th
+    member by size (the bounded cpu_baseline sample)."""
+    from oracle import ref_lib
+    from rodgpu import abi, scene  # pure Python (ctypes mirrors, member specs): loads no library
+    gen = abi.bind_scene_lib(ref_lib())
     specs = [s for s in scene.batch_members(256, seed=args.seed) if s["model"] == "nsc"]
-    specs = sorted(specs, key=lambda s: s["n"])[::8]
-    items = scene.batch_scenes(specs)
+    if every > 1:
+        specs = sorted(specs, key=lambda s: s["n"])[::every]
+    return scene.batch_scenes(specs, gen=gen)
+
+
+def run_reference(items, steps, warmup, threads=0):
+    """The reference's own FP32 CPU path (oracle/_ref: the reference's
+    src/physics compiled with OpenMP, spatial hash, plain PSOR) on every
+    given system, one after the other on all host threads: warmup untimed
+    steps, then steps timed with a steady clock."""
+    from oracle import Reference
     rod_steps = 0
     dt = 0.0
     th = 0
@@ -414,15 +439,33 @@ def run_reference(args, steps, warmup, threads=0):
         dt += time.perf_counter() - t0
         rod_steps += n * steps
         th = r.threads()
-    sample = (f"{len(items)} of the 128 batch systems (every 8th by size, {sum(sc['n'] for _, sc in items)} rods), "
-              f"{steps} steps each, reference src/physics compiled FP32 + OpenMP, spatial hash, plain PSOR")
-    return rod_steps / dt, th, sample, dt
+        del r
+    return rod_steps / dt, th, dt
+
+
+def loaded_native_libs():
+    """Shared objects of this repository mapped into this process."""
+    out = set()
+    try:
+        for line in open("/proc/self/maps"):
+            p = line.split()[-1] if line.strip() else ""
+            if p.endswith(".so") and p.startswith(ROOT):
+                out.add(os.path.relpath(p, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def headline_config(n_total, nsys):
+    """The config both arms print (identical keys and values)."""
+    return {"workload": batch_workload(nsys), "rods": n_total, "systems": nsys,
+            "l2": "no flush: state persists step to step (inputs 133 MB > L2 across members)"}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--train-systems", type=int, default=32)
     ap.add_argument("--train-steps", type=int, default=40)
@@ -441,21 +484,26 @@ def main():
         if rank != 0:
             return
         try:
-            v, th, sample, dt = run_reference(args, steps=max(1, min(args.steps, 2)), warmup=min(args.warmup, 1))
+            items = reference_scenes(args)
+            v, th, dt = run_reference(items, steps=args.steps, warmup=args.warmup)
         except Exception as e:  # noqa: BLE001
             print(json.dumps({"impl": "reference", "unavailable": f"reference build not loadable: {e}"}))
             return
-        from rodgpu import scene
-        specs = [s for s in scene.batch_members(256, seed=args.seed) if s["model"] == "nsc"]
+        n_total = sum(sc["n"] for _, sc in items)
+        sample = (f"all {len(items)} batch systems ({n_total} rods), {args.warmup} untimed + {args.steps} timed "
+                  f"steps each, one system after the other; reference src/physics compiled FP32 + OpenMP, "
+                  f"spatial hash, plain PSOR ({dt:.1f} s timed)")
         line = {"impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": "rod-steps/s",
-                "n_gpus": world, "steps": max(1, min(args.steps, 2)), "warmup": min(args.warmup, 1),
-                "higher_is_better": True, "dtype": "f32",
-                "config": {"workload": batch_workload(len(specs)),
-                           "sample": "every 8th system by size, stepped one after the other on the host"},
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(1000.0 * dt / args.steps, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded RSA packings, Gaussian velocities)",
+                "config": headline_config(n_total, len(items)),
                 "cpu_baseline": {"value": round(v, 2), "unit": "rod-steps/s", "cores": th, "kind": "reference",
                                  "sample": sample},
                 "e2e": {"value": round(v, 2), "unit": "rod-steps/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
+                        "d2h_bytes_per_step": 0},
+                "native_libs": loaded_native_libs()}
         print(json.dumps(line))
         return
 
@@ -465,11 +513,15 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     out = run_ours(args, rank, world)
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and args.workload == "batch":
         try:
-            v, th, sample, dt = run_reference(args, steps=1, warmup=0)
-            out["cpu_baseline"] = {"value": round(v, 2), "unit": "rod-steps/s", "cores": th, "kind": "reference",
-                                   "sample": sample + f" ({dt:.1f} s)"}
+            items = reference_scenes(args, every=4)
+            v, th, dt = run_reference(items, steps=4, warmup=1)
+            out["cpu_baseline"] = {
+                "value": round(v, 2), "unit": "rod-steps/s", "cores": th, "kind": "reference",
+                "sample": (f"every 4th batch system by size ({len(items)} systems, "
+                           f"{sum(sc['n'] for _, sc in items)} rods), 1 untimed + 4 timed steps each, reference "
+                           f"src/physics compiled FP32 + OpenMP, spatial hash, plain PSOR ({dt:.1f} s timed)")}
         except Exception as e:  # noqa: BLE001
             out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     if world > 1:

@@ -131,7 +131,7 @@ class Oracle:
         return {"x": x, "q": q, "v": v, "w": w, "f": f, "tau": t}
 
     def step(self, nsteps=1):
-        from rodgpu import RgStepStats  # same struct layout
+        from rodgpu.abi import RgStepStats  # same struct layout (pure Python, loads nothing)
         st = RgStepStats()
         assert self.L.orc_step(self._h, int(nsteps), ctypes.addressof(st)) == 0
         return st.as_dict()

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librodgpu.so")
 HOSTLIB = os.path.join(HERE, "librodhost.so")
-HOST_SRCS = [os.path.join(HERE, "host", "scene_gen.cpp")]
+HOST_SRCS = [os.path.join(HERE, "host", "scene_gen.cpp"), os.path.join(HERE, "host", "config_default.cpp")]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 # -fmad=false: no contraction of a*b+c into FMA, so every FP64 expression
@@ -21,8 +21,13 @@ FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-li
          "-Xcompiler", "-fvisibility=default"]
 
 
+# host C++ compiled into librodgpu.so beside the CUDA sources (the config
+# defaults, shared with the reference-baseline harness)
+LIB_HOST_SRCS = [os.path.join(HERE, "host", "config_default.cpp")]
+
+
 def sources():
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu")) + LIB_HOST_SRCS
 
 
 def headers():

@@ -21,7 +21,16 @@ import math
 
 import numpy as np
 
-from . import host, ptr, default_config
+from .abi import config_from, ptr
+
+
+def _gen(gen):
+    """The library that generates scenes: librodhost.so unless the caller
+    passes another library built from the same host sources."""
+    if gen is not None:
+        return gen
+    from . import host
+    return host()
 
 
 def capsule_volume(L, d):
@@ -34,7 +43,7 @@ def box_side(n, L, d, phi):
 
 
 def make_rods(n, L, d, phi=None, side=None, seed=1, sigma_v=0.1, sigma_w=0.1, density=1.0,
-              restitution=0.2, max_attempts=2000):
+              restitution=0.2, max_attempts=2000, gen=None):
     """RSA packing of n rods; returns a dict of body and state arrays.
 
     'placed' may be below n when the packing jams; arrays are trimmed to it.
@@ -42,7 +51,7 @@ def make_rods(n, L, d, phi=None, side=None, seed=1, sigma_v=0.1, sigma_w=0.1, de
     if side is None:
         side = box_side(n, L, d, phi)
     lo = -0.5 * side
-    H = host()
+    H = _gen(gen)
     x = np.zeros((n, 3))
     q = np.zeros((n, 4))
     placed = H.rg_scene_rsa(int(n), float(L), float(d), float(lo), float(side), int(seed),
@@ -85,16 +94,16 @@ WORKLOADS = {
 }
 
 
-def workload(name, n=None, seed=1, **overrides):
+def workload(name, n=None, seed=1, gen=None, **overrides):
     """(config, scene) for a named workload; n overrides the rod count."""
     w = WORKLOADS[name]
     nn = w["n"] if n is None else n
-    sc = make_rods(nn, w["L"], w["d"], phi=w["phi"], seed=seed)
+    sc = make_rods(nn, w["L"], w["d"], phi=w["phi"], seed=seed, gen=gen)
     kw = dict(w["cfg"])
     kw.update(gravity=(0.0, 0.0, 0.0), lin_damp=0.0, ang_damp=0.0)
     kw.update(pbc_kwargs(sc))
     kw.update(overrides)
-    cfg = default_config(n_bodies=sc["n"], **kw)
+    cfg = config_from(_gen(gen), n_bodies=sc["n"], **kw)
     return cfg, sc
 
 
@@ -132,20 +141,22 @@ def batch_members(n_systems=256, seed=7, n_lo=500, n_hi=20000, ars=(5, 10, 20, 4
     return out
 
 
-def batch_scenes(specs, threads=None, warm="cache"):
+def batch_scenes(specs, threads=None, warm="cache", gen=None):
     """(config, scene) of every member, generated on host threads (the
     generator releases the interpreter lock)."""
     import concurrent.futures as cf
     import os
+    gen = _gen(gen)
     with cf.ThreadPoolExecutor(threads or os.cpu_count() or 4) as ex:
-        return list(ex.map(lambda s: batch_member_scene(s, warm), specs))
+        return list(ex.map(lambda s: batch_member_scene(s, warm, gen), specs))
 
 
-def batch_member_scene(spec, warm="cache"):
+def batch_member_scene(spec, warm="cache", gen=None):
     """(config, scene) of one batch member: NSC dt=5e-4, tol 1e-6, 500
     sweeps; Hertz-Mindlin E=1e5, nu=0.3, e=0.5, dt=1e-4."""
+    gen = _gen(gen)
     d = 1.0 / spec["ar"]
-    sc = make_rods(spec["n"], 1.0, d, phi=spec["phi"], seed=spec["seed"], max_attempts=20000)
+    sc = make_rods(spec["n"], 1.0, d, phi=spec["phi"], seed=spec["seed"], max_attempts=20000, gen=gen)
     kw = dict(gravity=(0.0, 0.0, 0.0), lin_damp=0.0, ang_damp=0.0)
     if spec["model"] == "nsc":
         kw.update(model="nsc", dt=5e-4, nsc_mu=spec["mu"], nsc_omega=1.0, nsc_tol=1e-6, nsc_velocity_iters=500,
@@ -154,4 +165,4 @@ def batch_member_scene(spec, warm="cache"):
         kw.update(model="hertz-mindlin", dt=1e-4, hm_youngs_modulus=1e5, hm_poisson_ratio=0.3,
                   hm_restitution=0.5, hm_friction=spec["mu"])
     kw.update(pbc_kwargs(sc))
-    return default_config(n_bodies=sc["n"], **kw), sc
+    return config_from(gen, n_bodies=sc["n"], **kw), sc
