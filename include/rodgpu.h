@@ -147,7 +147,8 @@ typedef struct rg_step_stats {
   int64_t colors;           /* NSC: colours of the last velocity solve        */
   int64_t history_size;     /* HM / Cundall: live history entries             */
   double residual;          /* NSC: last PSOR residual (max |dλ| sum)         */
-  double jn_sum, jt_sum;    /* NSC: Σλn, Σ|λt| of the last step               */
+  double jn_sum, jt_sum;    /* NSC: Σ|λn| and Σ(|λt1|+|λt2|) of the last step
+                               (the profile CSV's sums, main.cpp:3339-3343)   */
   double potential_energy;  /* soft / HM: last contact potential energy       */
   double kinetic_energy;    /* ½Σ m|v|² + ½Σ ω·Iω after the call              */
   double max_residual;      /* NSC: worst final residual over the call        */

@@ -272,8 +272,28 @@ std::vector<Contact> detect(const orc_system& S, double delta) {
   for (int i = 0; i < n; ++i) maxext = std::max(maxext, S.body[i].h + S.body[i].r);
   double cut = 2.0 * maxext + delta;
   cut = cut * (1.0 + 1e-12) + 1e-12;
+  // Two conservative prefilters skip the narrow phase of pairs that cannot
+  // touch; neither changes the set.  (1) Centre distance: the segment
+  // distance is at least |dc| - h_a - h_b.  (2) Axis-line distance: the
+  // distance of the two infinite lines is a lower bound of the segment
+  // distance.  Both reject only beyond the activation distance plus a
+  // relative 1e-9 and absolute 1e-12 margin, far above their rounding error.
+  std::vector<V3> axis(n);
+  for (int i = 0; i < n; ++i) axis[i] = axis_y(S.q[i]);
   auto test = [&](int i, int j) {
     if (S.body[i].inv_mass <= 0.0 && S.body[j].inv_mass <= 0.0) return;
+    const Body& A = S.body[i];
+    const Body& B = S.body[j];
+    V3 dc = (S.x[j] + min_image_shift(S, S.x[i], S.x[j])) - S.x[i];
+    const double act = A.r + B.r + delta;
+    const double cc = A.h + B.h + act;
+    if (dot(dc, dc) > cc * cc * (1.0 + 1e-9) + 1e-12) return;
+    V3 cr = cross(axis[i], axis[j]);
+    double c2 = dot(cr, cr);
+    if (c2 > 1e-6) {
+      double proj = dot(dc, cr);
+      if (proj * proj > (act * act * (1.0 + 1e-9) + 1e-12) * c2) return;
+    }
     Contact c;
     if (narrow(S, i, j, delta, c)) out.push_back(c);
   };
@@ -341,8 +361,8 @@ std::vector<Contact> detect(const orc_system& S, double delta) {
             for (int j : cells[(Z * dims[1] + Y) * dims[0] + X])
               if (j > i) cand.push_back(j);
           }
-      std::sort(cand.begin(), cand.end());
-      cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+      // the 27 cells are distinct (every dimension has at least 3 cells
+      // here), so no candidate repeats; the contacts are sorted below
       for (int j : cand) test(i, j);
     }
   }
@@ -1001,10 +1021,12 @@ void nsc_step(orc_system& S) {
   S.last_collisions = coll;
   // 3) velocity PSOR
   solve_velocities(S, visit_order((int)cs.size(), col, colored));
+  // impulse sums of the profile CSV (main.cpp:3339-3343); collisions above
+  // are NscContactSolver::countImpacts (nsc_contact.hpp:112-117)
   S.jn_sum = 0; S.jt_sum = 0;
   for (const Manifold& m : S.manifolds) {
-    S.jn_sum += m.ln;
-    S.jt_sum += std::sqrt(m.lt1 * m.lt1 + m.lt2 * m.lt2);
+    S.jn_sum += std::abs(m.ln);
+    S.jt_sum += std::abs(m.lt1) + std::abs(m.lt2);
   }
   // 4) position + orientation update with linear damping (main.cpp:4469-4483)
   for (int i = 0; i < S.n; ++i) {

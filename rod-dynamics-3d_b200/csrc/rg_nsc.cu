@@ -1087,8 +1087,8 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
     V.wlam[V.wcap + c] = l1;
     V.wlam[2 * V.wcap + c] = l2;
     reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = S.color[c];
-    jn = l0;
-    jt = sqrt(l1 * l1 + l2 * l2);
+    jn = fabs(l0);  // profile-CSV sums of main.cpp:3339-3343
+    jt = fabs(l1) + fabs(l2);
   }
   jn = warp_sum(jn);
   jt = warp_sum(jt);
@@ -1362,8 +1362,8 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
       V.wlam[V.wcap + c] = l1;
       V.wlam[2 * V.wcap + c] = l2;
       reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = V.color[c];
-      jn += l0;
-      jt += sqrt(l1 * l1 + l2 * l2);
+      jn += fabs(l0);  // profile-CSV sums of main.cpp:3339-3343
+      jt += fabs(l1) + fabs(l2);
     }
     jn = warp_sum(jn);
     jt = warp_sum(jt);
