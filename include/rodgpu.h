@@ -219,6 +219,19 @@ int rg_detect(rg_system* sys, double delta, int32_t* pairs, double* geom,
 int rg_get_impulses(const rg_system* sys, int32_t* pairs, double* lambda,
                     int32_t* color, size_t cap, size_t* n);
 
+/* Contact network of the last NSC velocity solve, the rows
+ * App::logNetworkFrame writes for NSC scenes (src/app/main.cpp:3620-3700,
+ * header "frame,rod_i,rod_j,contact_x..z,normal_x..z,phi,lambda_n,
+ * lambda_t1,lambda_t2,vn_pre,vn_post").  Export must be enabled (it keeps
+ * each manifold's normal, r_a, r_b, phi and v_n_pre on the device, 88 B
+ * per contact) before the steps whose network is wanted.  Sorted by (a,b):
+ * pairs[2*i..] = (rod_i, rod_j); rows[12*i..] = contact point x_a + r_a at
+ * the current state (3), normal (3), phi, lambda_n, lambda_t1, lambda_t2,
+ * v_n before the solve, v_n at the current velocities.  Returns
+ * RG_ERR_CAPACITY (with *n set) when cap is too small. */
+int rg_set_network_export(rg_system* sys, int enable);
+int rg_get_contact_network(const rg_system* sys, int32_t* pairs, double* rows, size_t cap, size_t* n);
+
 /* Per-body force and torque of one force evaluation at the current state
  * (soft or HM model), without integrating: f[3N], tau[3N].  Advances the
  * tangential history exactly like one computeForces call of the reference. */

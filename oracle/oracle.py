@@ -61,6 +61,8 @@ def oracle_lib():
         L.orc_get_impulses.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.POINTER(_i), ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_size_t)]
         L.orc_compute_forces.argtypes = [P, dp, dp, dp]
+        L.orc_get_contact_network.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.c_size_t,
+                                              ctypes.POINTER(ctypes.c_size_t)]
         L.orc_get_history.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.POINTER(ctypes.c_int64),
                                       ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L.orc_color.argtypes = [P, ctypes.POINTER(_i), ctypes.c_size_t, ctypes.POINTER(_i),
@@ -157,6 +159,15 @@ class Oracle:
         self.L.orc_get_impulses(self._h, _p(pairs, _i), _p(lam), _p(col, _i), cap, ctypes.byref(n))
         m = n.value
         return pairs[:m], lam[:m], col[:m]
+
+    def contact_network(self):
+        n = ctypes.c_size_t()
+        self.L.orc_get_contact_network(self._h, None, None, 0, ctypes.byref(n))
+        cap = max(1, n.value)
+        pairs = np.zeros((cap, 2), np.int32)
+        rows = np.zeros((cap, 12))
+        self.L.orc_get_contact_network(self._h, _p(pairs, _i), _p(rows), cap, ctypes.byref(n))
+        return pairs[:n.value], rows[:n.value]
 
     def compute_forces(self):
         f = np.zeros((self.n, 3))

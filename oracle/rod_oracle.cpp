@@ -1199,6 +1199,31 @@ int orc_get_impulses(const orc_system* S, int32_t* pairs, double* lambda, int32_
   return S->manifolds.size() > cap ? RG_ERR_CAPACITY : RG_OK;
 }
 
+// Network rows of the last velocity solve (App::logNetworkFrame NSC branch,
+// main.cpp:3664-3690): point x_a + r_a and v_n after the solve from the
+// current state; phi, impulses and v_n_pre from the manifold.
+int orc_get_contact_network(const orc_system* S, int32_t* pairs, double* rows, size_t cap, size_t* n) {
+  if (!S || !n) return RG_ERR_ARG;
+  const size_t m = S->manifolds.size();
+  *n = m;
+  for (size_t i = 0; i < m && i < cap; ++i) {
+    const Manifold& M = S->manifolds[i];
+    V3 va = S->v[M.a] + cross(S->w[M.a], M.ra);
+    V3 vb = S->v[M.b] + cross(S->w[M.b], M.rb);
+    double vn_post = dot(M.n, vb - va);
+    if (pairs) { pairs[2 * i] = M.a; pairs[2 * i + 1] = M.b; }
+    if (rows) {
+      double* o = rows + 12 * i;
+      V3 pt = S->x[M.a] + M.ra;
+      o[0] = pt.x; o[1] = pt.y; o[2] = pt.z;
+      o[3] = M.n.x; o[4] = M.n.y; o[5] = M.n.z;
+      o[6] = M.phi; o[7] = M.ln; o[8] = M.lt1; o[9] = M.lt2;
+      o[10] = M.v_n_pre; o[11] = vn_post;
+    }
+  }
+  return m > cap ? RG_ERR_CAPACITY : RG_OK;
+}
+
 int orc_compute_forces(orc_system* S, double* f, double* tau, double* pe) {
   if (!S) return RG_ERR_ARG;
   for (int i = 0; i < S->n; ++i) { S->f[i] = v3(0, 0, 0); S->tau[i] = v3(0, 0, 0); }

@@ -32,6 +32,11 @@ int cuda_fail(rg_system* s, cudaError_t e, const char* where) {
   return fail(s, RG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
+#define RG_TRY2(sys, call, where)                   \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return cuda_fail(sys, e_, where); \
+  } while (0)
 #define RG_TRY(call, where)                         \
   do {                                              \
     cudaError_t e_ = (call);                        \
@@ -76,6 +81,7 @@ void free_contact_buffers(rg_system* s) {
   Nsc& N = s->nsc;
   cudaFree(N.row); cudaFree(N.lam); cudaFree(N.color); cudaFree(N.color_tmp); cudaFree(N.order);
   cudaFree(N.color_cnt); cudaFree(N.color_off); cudaFree(N.wkey); cudaFree(N.wlam); cudaFree(N.wn);
+  cudaFree(N.xrow);
   cudaFree(N.dx); cudaFree(N.prow); cudaFree(N.pactive);
   cudaFree(N.pmax); cudaFree(N.cmask); cudaFree(N.owner); cudaFree(N.cursor); cudaFree(N.remaining);
   cudaFree(N.blk); cudaFree(N.slot_of); cudaFree(N.bar); cudaFree(N.view_dev); cudaFree(N.team_dev);
@@ -123,6 +129,7 @@ cudaError_t alloc_contact_buffers(rg_system* s, int ccap, int hcap) {
   if ((e = cudaMalloc(&N.wlam, sizeof(double) * 3 * (size_t)ccap + sizeof(int) * (size_t)ccap))) return e;
   if ((e = cudaMalloc(&N.wn, sizeof(int)))) return e;
   if ((e = cudaMemset(N.wn, 0, sizeof(int)))) return e;
+  if (s->export_on && (e = cudaMalloc(&N.xrow, sizeof(double) * kExportComps * (size_t)ccap))) return e;
   if ((e = cudaMalloc(&N.dx, sizeof(double) * 6 * (size_t)n))) return e;
   if ((e = cudaMemset(N.dx, 0, sizeof(double) * 6 * (size_t)n))) return e;
   if ((e = cudaMalloc(&N.prow, sizeof(double) * kPosComps * (size_t)ccap))) return e;
@@ -828,6 +835,69 @@ int rg_get_impulses(const rg_system* s, int32_t* pairs, double* lambda, int32_t*
       if (pairs) { pairs[2 * i] = (int32_t)(k[i] >> 32); pairs[2 * i + 1] = (int32_t)(k[i] & 0xffffffffu); }
       if (lambda) for (int j = 0; j < 3; ++j) lambda[3 * i + j] = l[(size_t)j * m + i];
       if (color) color[i] = c[i];
+    }
+  }
+  return (size_t)wn > cap ? RG_ERR_CAPACITY : RG_OK;
+}
+
+int rg_set_network_export(rg_system* s, int enable) {
+  if (!s) return RG_ERR_ARG;
+  if (s->cfg.model != RG_MODEL_NSC) return fail(s, RG_ERR_ARG, "the contact-network export needs the nsc model");
+  s->export_on = enable != 0;
+  if (s->export_on && !s->nsc.xrow) {
+    RG_TRY(cudaMalloc(&s->nsc.xrow, sizeof(double) * kExportComps * (size_t)s->nsc.wcap), "export buffer");
+    RG_TRY(cudaMemset(s->nsc.xrow, 0, sizeof(double) * kExportComps * (size_t)s->nsc.wcap), "export buffer");
+  }
+  return RG_OK;
+}
+
+int rg_get_contact_network(const rg_system* s, int32_t* pairs, double* rows, size_t cap, size_t* n) {
+  if (!s || !n) return RG_ERR_ARG;
+  rg_system* m = const_cast<rg_system*>(s);
+  if (!s->export_on || !s->nsc.xrow) return fail(m, RG_ERR_STATE, "enable the export before stepping");
+  int wn = 0;
+  RG_TRY2(m, cudaMemcpy(&wn, s->nsc.wn, sizeof(int), cudaMemcpyDeviceToHost), "network count");
+  *n = (size_t)wn;
+  const size_t k = cap < (size_t)wn ? cap : (size_t)wn;
+  if (k) {
+    const size_t W = (size_t)s->nsc.wcap;
+    std::vector<unsigned long long> key(k);
+    std::vector<double> lam(3 * k), xr(kExportComps * k);
+    RG_TRY2(m, cudaMemcpy(key.data(), s->nsc.wkey, sizeof(unsigned long long) * k, cudaMemcpyDeviceToHost), "keys");
+    for (int j = 0; j < 3; ++j)
+      RG_TRY2(m, cudaMemcpy(lam.data() + j * k, s->nsc.wlam + j * W, sizeof(double) * k, cudaMemcpyDeviceToHost),
+              "impulses");
+    for (int j = 0; j < kExportComps; ++j)
+      RG_TRY2(m, cudaMemcpy(xr.data() + j * k, s->nsc.xrow + j * W, sizeof(double) * k, cudaMemcpyDeviceToHost),
+              "export rows");
+    // contact point and post-solve normal velocity from the current state
+    // (App::logNetworkFrame, main.cpp:3670-3684)
+    const size_t N = (size_t)s->n;
+    std::vector<double> st(19 * N);
+    RG_TRY2(m, cudaMemcpy(st.data(), s->d_state, sizeof(double) * 19 * N, cudaMemcpyDeviceToHost), "state");
+    auto comp = [&](int c, size_t i) { return st[(size_t)c * N + i]; };
+    for (size_t i = 0; i < k; ++i) {
+      const size_t a = (size_t)(key[i] >> 32), b = (size_t)(key[i] & 0xffffffffu);
+      const double nv[3] = {xr[0 * k + i], xr[1 * k + i], xr[2 * k + i]};
+      const double ra[3] = {xr[3 * k + i], xr[4 * k + i], xr[5 * k + i]};
+      const double rb[3] = {xr[6 * k + i], xr[7 * k + i], xr[8 * k + i]};
+      double va[3], vb[3];
+      for (int d = 0; d < 3; ++d) {
+        const int e = (d + 1) % 3, f = (d + 2) % 3;  // (w x r)_d = w_e r_f - w_f r_e
+        va[d] = comp(7 + d, a) + (comp(10 + e, a) * ra[f] - comp(10 + f, a) * ra[e]);
+        vb[d] = comp(7 + d, b) + (comp(10 + e, b) * rb[f] - comp(10 + f, b) * rb[e]);
+      }
+      double vn_post = 0.0;
+      for (int d = 0; d < 3; ++d) vn_post += nv[d] * (vb[d] - va[d]);
+      if (pairs) { pairs[2 * i] = (int32_t)a; pairs[2 * i + 1] = (int32_t)b; }
+      if (rows) {
+        double* o = rows + 12 * i;
+        for (int d = 0; d < 3; ++d) { o[d] = comp(d, a) + ra[d]; o[3 + d] = nv[d]; }
+        o[6] = xr[9 * k + i];
+        o[7] = lam[i]; o[8] = lam[k + i]; o[9] = lam[2 * k + i];
+        o[10] = xr[10 * k + i];
+        o[11] = vn_post;
+      }
     }
   }
   return (size_t)wn > cap ? RG_ERR_CAPACITY : RG_OK;

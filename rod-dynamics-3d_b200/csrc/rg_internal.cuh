@@ -129,6 +129,9 @@ struct Nsc {
   double* wlam = nullptr;
   int* wn = nullptr;  // device count of the warm cache
   int wcap = 0;
+  // contact-network export (enabled per system): kExportComps component
+  // arrays of wcap, warm-cache order - normal, r_a, r_b, phi, v_n_pre
+  double* xrow = nullptr;
   // projection scratch
   double* dx = nullptr;   // 6n: dx(3n), dθ(3n)
   double* prow = nullptr; // kPosComps * ccap
@@ -146,6 +149,7 @@ struct Nsc {
   void* team_dev = nullptr;             // device team descriptor
 };
 constexpr int kRowComps = 42;
+constexpr int kExportComps = 11;
 constexpr int kPosComps = 12;
 
 }  // namespace rg
@@ -196,6 +200,7 @@ struct rg_system {
   double* h_ke = nullptr;        // 64 partial sums
   bool mlp_ready = false;
   bool recording = false;
+  bool export_on = false;     // contact-network export rows saved by the NSC step
   int rec_cap = 0;
   float* d_rec_x = nullptr;
   float* d_rec_y = nullptr;

@@ -1087,6 +1087,7 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
     V.wlam[V.wcap + c] = l1;
     V.wlam[2 * V.wcap + c] = l2;
     reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = S.color[c];
+    if (V.xrow) export_row(V.xrow, V.wcap, c, R, p);
     jn = fabs(l0);  // profile-CSV sums of main.cpp:3339-3343
     jt = fabs(l1) + fabs(l2);
   }
@@ -1362,6 +1363,7 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
       V.wlam[V.wcap + c] = l1;
       V.wlam[2 * V.wcap + c] = l2;
       reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = V.color[c];
+      if (V.xrow) export_row(V.xrow, V.wcap, c, R, p);
       jn += fabs(l0);  // profile-CSV sums of main.cpp:3339-3343
       jt += fabs(l1) + fabs(l2);
     }
@@ -1509,6 +1511,7 @@ NscView make_view(rg_system* s) {
   V.color_cnt = N.color_cnt; V.color_off = N.color_off; V.cursor = N.cursor; V.remaining = N.remaining;
   V.pmax = N.pmax; V.cmask = N.cmask; V.owner = N.owner;
   V.wkey = N.wkey; V.wlam = N.wlam; V.wn = N.wn; V.wcap = N.wcap;
+  V.xrow = s->export_on ? N.xrow : nullptr;
   V.dx = N.dx; V.prow = N.prow; V.pactive = N.pactive;
   V.ccap = s->ccap;
   V.blk = N.blk;

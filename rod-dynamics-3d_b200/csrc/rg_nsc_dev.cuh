@@ -127,6 +127,16 @@ __device__ inline int build_row(const State& st, const Contacts& con, const rg_c
   return (vnp < -1e-6 ? 1 : 0) | cached;  // bit 0: impact, bit 1: in the warm cache
 }
 
+// Contact-network export of slot p (contact c, warm-cache order): the
+// manifold's normal, r_a, r_b, phi and v_n_pre (NscManifold fields that
+// App::logNetworkFrame writes, main.cpp:3670-3690).
+__device__ inline void export_row(double* xrow, int wcap, int c, const RowIO& R, int p) {
+  const int src[kExportComps] = {R_N, R_N + 1, R_N + 2, R_RA, R_RA + 1, R_RA + 2,
+                                 R_RB, R_RB + 1, R_RB + 2, R_PHI, R_VNPRE};
+#pragma unroll
+  for (int k = 0; k < kExportComps; ++k) xrow[(size_t)k * wcap + c] = R.r(src[k], p);
+}
+
 // Learned warm start of slot p: previous impulse (already in R.lam) plus the
 // network's predicted change, projected onto the friction cone.
 __device__ inline void mlp_apply(const RowIO& R, const float* pred, int pld, int p, double mu) {
@@ -424,6 +434,7 @@ struct NscView {
   double* wlam;
   int* wn;
   int wcap;
+  double* xrow;  // contact-network export (null: off), kExportComps x wcap
   double *dx, *prow;
   int* pactive;
   int ccap;

@@ -45,6 +45,11 @@ PYBIND11_MODULE(rod_dynamics_py, m) {
       .def(py::init<const std::string&, const std::string&, bool>(), py::arg("scene_path"),
            py::arg("init_csv_path") = std::string(), py::arg("quiet") = true)
       .def("step", &rgsim::Simulator::step, py::arg("steps") = 1, py::call_guard<py::gil_scoped_release>())
+      .def("enable_csv", &rgsim::Simulator::enable_csv, py::arg("path") = std::string("profile.csv"),
+           "Profile CSV of every frame, the reference App's columns (main.cpp:3276-3355).")
+      .def("enable_network", &rgsim::Simulator::enable_network, py::arg("path") = std::string("network.csv"),
+           py::arg("stride") = 1, py::arg("max_frames") = 0,
+           "NSC contact network CSV every stride frames (main.cpp:3620-3700).")
       .def("diagnostics",
            [](const rgsim::Simulator& s) {
              py::dict d;

@@ -390,11 +390,188 @@ void Simulator::random_init(const rgjson::Value& ri) {
 
 void Simulator::step(int steps) {
   if (steps <= 0) return;
-  check(rg_step(sys_, steps, &stats_), "rg_step");
-  frame_ += steps;
-  last_ke_ = stats_.kinetic_energy;
-  last_hits_ = stats_.contacts;
-  fresh_ = false;
+  if (!csv_ && !net_) {
+    check(rg_step(sys_, steps, &stats_), "rg_step");
+    frame_ += steps;
+    last_ke_ = stats_.kinetic_energy;
+    last_hits_ = stats_.contacts;
+    fresh_ = false;
+    return;
+  }
+  for (int k = 0; k < steps; ++k) {  // one frame per call, each one logged
+    check(rg_step(sys_, 1, &stats_), "rg_step");
+    frame_ += 1;
+    last_ke_ = stats_.kinetic_energy;
+    last_hits_ = stats_.contacts;
+    fresh_ = false;
+    log_frame();
+  }
+}
+
+void Simulator::enable_csv(const std::string& path) {
+  csv_.reset(new std::ofstream(path.empty() ? std::string("profile.csv") : path, std::ios::out | std::ios::trunc));
+  if (!*csv_) {
+    csv_.reset();
+    throw std::runtime_error("cannot open CSV file: " + path);
+  }
+  csv_header_ = false;
+  rg_set_profiling(sys_, 1);  // phase / stage timers for the *_ms columns
+}
+
+void Simulator::enable_network(const std::string& path, int stride, int max_frames) {
+  if (cfg_.model != RG_MODEL_NSC)
+    throw std::runtime_error("the contact-network export is available for nsc scenes");
+  net_.reset(new std::ofstream(path.empty() ? std::string("network.csv") : path, std::ios::out | std::ios::trunc));
+  if (!*net_) {
+    net_.reset();
+    throw std::runtime_error("cannot open network file: " + path);
+  }
+  net_header_ = false;
+  net_stride_ = stride < 1 ? 1 : stride;
+  net_max_ = max_frames;
+  net_written_ = 0;
+  check(rg_set_network_export(sys_, 1), "rg_set_network_export");
+}
+
+// Centre of mass, per axis the circular mean in periodic dimensions
+// (App::computeCOM, main.cpp:3500-3571).
+void Simulator::com(double c[3]) const {
+  const double pi = 3.14159265358979323846;
+  for (int k = 0; k < 3; ++k) {
+    const double L = cfg_.pbc_max[k] - cfg_.pbc_min[k];
+    double m_sum = 0, s0 = 0, s1 = 0;
+    for (int i = 0; i < n_; ++i) {
+      const double m = mass_[i];
+      m_sum += m;
+      if (cfg_.pbc_enabled && L > 0) {
+        const double th = 2.0 * pi * (x_[3 * i + k] - cfg_.pbc_min[k]) / L;
+        s0 += m * std::cos(th);
+        s1 += m * std::sin(th);
+      } else {
+        s0 += m * x_[3 * i + k];
+      }
+    }
+    if (cfg_.pbc_enabled && L > 0) {
+      double a = std::atan2(s1 / m_sum, s0 / m_sum);
+      if (a < 0.0) a += 2.0 * pi;
+      c[k] = cfg_.pbc_min[k] + a / (2.0 * pi) * L;
+    } else {
+      c[k] = s0 / m_sum;
+    }
+  }
+}
+
+namespace {
+double min_image(double d, double L, bool pbc) { return pbc && L > 0 ? d - L * std::floor(d / L + 0.5) : d; }
+}  // namespace
+
+// Mean squared distance from the centre of mass (computeGyrationSq,
+// main.cpp:938-960).
+double Simulator::gyration_sq() const {
+  if (n_ == 0) return 0.0;
+  double c[3];
+  com(c);
+  double sum = 0;
+  for (int i = 0; i < n_; ++i)
+    for (int k = 0; k < 3; ++k) {
+      const double d = min_image(x_[3 * i + k] - c[k], cfg_.pbc_max[k] - cfg_.pbc_min[k], cfg_.pbc_enabled);
+      sum += d * d;
+    }
+  return sum / n_;
+}
+
+// Mean squared displacement since the last logged frame relative to the
+// centre of mass motion (computeRelativeMotionSq, main.cpp:963-1022); 0 on
+// the first call.
+double Simulator::relative_motion_sq() {
+  if (n_ == 0) return 0.0;
+  double c[3];
+  com(c);
+  if (!has_last_pos_ || (int)last_pos_.size() != 3 * n_) {
+    last_pos_ = x_;
+    for (int k = 0; k < 3; ++k) last_com_[k] = c[k];
+    has_last_pos_ = true;
+    return 0.0;
+  }
+  double dc[3];
+  for (int k = 0; k < 3; ++k)
+    dc[k] = min_image(c[k] - last_com_[k], cfg_.pbc_max[k] - cfg_.pbc_min[k], cfg_.pbc_enabled);
+  double sum = 0;
+  for (int i = 0; i < n_; ++i)
+    for (int k = 0; k < 3; ++k) {
+      const double d = min_image(x_[3 * i + k] - last_pos_[3 * i + k], cfg_.pbc_max[k] - cfg_.pbc_min[k],
+                                 cfg_.pbc_enabled) - dc[k];
+      sum += d * d;
+    }
+  last_pos_ = x_;
+  for (int k = 0; k < 3; ++k) last_com_[k] = c[k];
+  return sum / n_;
+}
+
+// One frame of the profile CSV and the network CSV.  Columns this library
+// has no counterpart for are written as the reference writes unavailable
+// values: -1 for the per-phase kinetic energies, 0 for islands, sleeping,
+// render and the entanglement observable.
+void Simulator::log_frame() {
+  sync();
+  if (csv_) {
+    std::ostream& o = *csv_;
+    const bool nsc = cfg_.model == RG_MODEL_NSC;
+    double ph[12] = {0}, st[RG_NSTAGES] = {0};
+    rg_get_phase_times(sys_, ph, 12);
+    rg_get_profile(sys_, st, nullptr);
+    rg_set_profiling(sys_, 1);  // restart the accumulators: per-frame times
+    if (!csv_header_) {
+      if (!nsc)
+        o << "frame,rods,integrate_ms,sleep_ms,broadphase_ms,bpCount_ms,bpPrefix_ms,bpFill_ms,bpPairs_ms,"
+             "solve_ms,pbcWrap_ms,render_ms,contacts,collisions,KE,soft_PE,gyration_sq,reldisp_sq,"
+             "ent_pairs,ent_sum,step_ms\n";
+      else
+        o << "frame,rods,integrate_ms,sleep_ms,broadphase_ms,bpCount_ms,bpPrefix_ms,bpFill_ms,bpPairs_ms,"
+             "bpLongLong_ms,warmstart_ms,buildIslands_ms,solve_ms,floorSolve_ms,posCorrect_ms,pbcWrap_ms,"
+             "render_ms,contacts,collisions,islands,KE,KE_after_integrate,KE_after_warmstart,KE_after_solve,"
+             "KE_after_posCorrect,KE_after_pbcWrap,soft_PE,gyration_sq,reldisp_sq,jn_sum,jt_sum,nsc_residual,"
+             "ent_pairs,ent_sum,step_ms\n";
+      csv_header_ = true;
+    }
+    const double gyr = gyration_sq(), rel = relative_motion_sq();
+    if (!nsc) {
+      // stage timers: 0 integrate, 1 detect, 6 contact forces
+      o << frame_ << ',' << n_ << ',' << st[0] << ",0," << st[1] << ",0,0,0,0," << st[6] << ",0,0,"
+        << stats_.contacts << ",-1," << last_ke_ << ',' << stats_.potential_energy << ',' << gyr << ',' << rel
+        << ",0,0," << stats_.device_ms << '\n';
+    } else {
+      // persistent-step phases: 0 free flight, 1 detection, 2 colouring,
+      // 3 manifold rows + warm start, 4 PSOR, 5 position update + wrap,
+      // 6-8 position projection
+      o << frame_ << ',' << n_ << ',' << (ph[0] + ph[5]) << ",0," << ph[1] << ",0,0,0,0,0," << ph[3] << ','
+        << ph[2] << ',' << ph[4] << ",0," << (ph[6] + ph[7] + ph[8]) << ",0,0," << stats_.contacts << ','
+        << stats_.collisions << ",0," << last_ke_ << ",-1,-1,-1,-1,-1,0," << gyr << ',' << rel << ','
+        << stats_.jn_sum << ',' << stats_.jt_sum << ',' << stats_.residual << ",0,0," << stats_.device_ms
+        << '\n';
+    }
+    if ((frame_ & 0x3F) == 0) o.flush();
+  }
+  if (net_ && frame_ % net_stride_ == 0 && (net_max_ <= 0 || net_written_ < net_max_)) {
+    std::ostream& o = *net_;
+    if (!net_header_) {
+      o << "frame,rod_i,rod_j,contact_x,contact_y,contact_z,normal_x,normal_y,normal_z,phi,lambda_n,"
+           "lambda_t1,lambda_t2,vn_pre,vn_post\n";
+      net_header_ = true;
+    }
+    size_t m = 0;
+    rg_get_contact_network(sys_, nullptr, nullptr, 0, &m);
+    std::vector<int32_t> pairs(2 * m + 2);
+    std::vector<double> rows(12 * m + 12);
+    check(rg_get_contact_network(sys_, pairs.data(), rows.data(), m, &m), "rg_get_contact_network");
+    for (size_t i = 0; i < m; ++i) {
+      o << frame_ << ',' << pairs[2 * i] << ',' << pairs[2 * i + 1];
+      for (int k = 0; k < 12; ++k) o << ',' << rows[12 * i + k];
+      o << '\n';
+    }
+    if ((frame_ & 0x3F) == 0) o.flush();
+    ++net_written_;
+  }
 }
 
 // 1/2 m |v|^2 + 1/2 w . (R I R^T) w over dynamic rods (host copy).

@@ -1,6 +1,8 @@
 // simulator.hpp - host-side session over librodgpu with the surface of the
 // reference's Python simulator (src/python/rod_dynamics_py.cpp:52-91).
 #pragma once
+#include <fstream>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -18,6 +20,14 @@ class Simulator {
   Simulator& operator=(const Simulator&) = delete;
 
   void step(int steps = 1);
+  // Per-frame writers of the reference App (enabled by its CLI there):
+  // the profile CSV (App::enableCsv / logCsvFrame, src/app/main.cpp:162-172,
+  // :3276-3355) and the NSC contact network (logNetworkFrame, :3620-3700,
+  // every `stride` frames, at most max_frames frames when > 0).  While either
+  // is on, step(n) advances one frame per library call so every frame is
+  // logged.
+  void enable_csv(const std::string& path);
+  void enable_network(const std::string& path, int stride = 1, int max_frames = 0);
   int rod_count() const { return n_; }
   long long frame_index() const { return frame_; }
   double dt() const { return cfg_.dt; }
@@ -51,6 +61,10 @@ class Simulator {
   void random_init(const rgjson::Value& ri);
   double kinetic_energy() const;
   void sync() const;
+  void log_frame();
+  void com(double c[3]) const;
+  double gyration_sq() const;
+  double relative_motion_sq();
 
   bool quiet_ = true;
   rg_config cfg_{};
@@ -64,6 +78,15 @@ class Simulator {
   std::vector<double> x_, q_, v_, w_, f_, tau_;
   std::vector<double> radius_, half_, rest_, mass_, inertia_;
   std::vector<int> static_;
+  // writers
+  std::unique_ptr<std::ofstream> csv_;
+  bool csv_header_ = false;
+  std::unique_ptr<std::ofstream> net_;
+  bool net_header_ = false;
+  int net_stride_ = 1, net_max_ = 0, net_written_ = 0;
+  std::vector<double> last_pos_;
+  double last_com_[3] = {0, 0, 0};
+  bool has_last_pos_ = false;
 };
 
 }  // namespace rgsim

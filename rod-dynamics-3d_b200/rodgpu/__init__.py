@@ -31,7 +31,8 @@ _host = None
 ABI_SYMBOLS = [
     "rg_abi_version", "rg_config_default", "rg_status_string", "rg_last_error", "rg_create",
     "rg_destroy", "rg_get_config", "rg_set_bodies", "rg_set_state", "rg_get_state", "rg_step",
-    "rg_detect", "rg_get_impulses", "rg_compute_forces", "rg_get_history", "rg_set_profiling",
+    "rg_detect", "rg_get_impulses", "rg_set_network_export", "rg_get_contact_network",
+    "rg_compute_forces", "rg_get_history", "rg_set_profiling",
     "rg_get_profile", "rg_get_phase_times", "rg_detect_noalloc",
     "rg_mlp_param_count", "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_record",
     "rg_mlp_records", "rg_mlp_train", "rg_mlp_infer", "rg_batch_create", "rg_batch_destroy",
@@ -67,6 +68,9 @@ def lib():
         L.rg_get_impulses.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.POINTER(_i),
                                       ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L.rg_compute_forces.argtypes = [P, dp, dp, dp]
+        L.rg_set_network_export.argtypes = [P, ctypes.c_int]
+        L.rg_get_contact_network.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.c_size_t,
+                                             ctypes.POINTER(ctypes.c_size_t)]
         L.rg_get_history.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.POINTER(ctypes.c_int64),
                                      ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L.rg_set_profiling.argtypes = [P, ctypes.c_int]
@@ -210,6 +214,22 @@ class System:
                                               ctypes.byref(n)), "impulses")
         m = n.value
         return pairs[:m], lam[:m], col[:m]
+
+    def set_network_export(self, on=True):
+        self._check(self._lib.rg_set_network_export(self._h, int(bool(on))), "set_network_export")
+
+    def contact_network(self):
+        """(pairs [C,2], rows [C,12]) of the last NSC velocity solve; rows are
+        contact point (3), normal (3), phi, lambda_n, lambda_t1, lambda_t2,
+        vn_pre, vn_post (the reference's network CSV columns)."""
+        n = ctypes.c_size_t()
+        self._lib.rg_get_contact_network(self._h, None, None, 0, ctypes.byref(n))
+        cap = max(1, n.value)
+        pairs = np.zeros((cap, 2), np.int32)
+        rows = np.zeros((cap, 12))
+        self._check(self._lib.rg_get_contact_network(self._h, ptr(pairs, _i), ptr(rows), cap, ctypes.byref(n)),
+                    "contact_network")
+        return pairs[:n.value], rows[:n.value]
 
     def compute_forces(self):
         f = np.zeros((self.n, 3))
