@@ -171,6 +171,64 @@ def plain_single(rodgpu, args):
             "roofline": roofline(b, ms, "k_nsc_run (single system)", None)}
 
 
+def verlet_bytes(rod_steps, contact_evals):
+    """Algorithmic bytes of soft / Hertz-Mindlin velocity-Verlet steps (FP64
+    SoA model): 896 B per rod-step (half kick + drift, two force
+    evaluations' body reads and force writes, second kick, cell keys) and
+    72 B per contact and force evaluation (pair record 8 + history read 32
+    + write 32), i.e. 144 B per contact-step at two evaluations per step.
+    contact_evals = the sum over the force evaluations of their contacts."""
+    return 896.0 * rod_steps + 72.0 * contact_evals
+
+
+# Hertz-Mindlin workloads timed beside the headline: the small plain
+# soft-contact configuration (N = 1000, d = 0.1, phi 0.10, E = 1e5, mu 0.5,
+# dt 1e-4, 1000 steps) and the large single system (N = 1e6, d = 0.02,
+# E = 1e6, e = 0.3, dt 2e-5, 100 steps; isotropic RSA of aspect-ratio-50
+# rods jams near phi*AR ~ 2.4, so it runs at phi 0.045 instead of 0.15; the
+# packing comes from the device generator).
+HM_LINES = {
+    "hm_small": dict(n=1000, d=0.1, phi=0.10, steps=1000, device_gen=False,
+                     cfg=dict(model="hertz-mindlin", dt=1e-4, hm_youngs_modulus=1e5, hm_poisson_ratio=0.3,
+                              hm_restitution=0.5, hm_friction=0.5)),
+    "hm_large": dict(n=1000000, d=0.02, phi=0.045, steps=100, device_gen=True,
+                     cfg=dict(model="hertz-mindlin", dt=2e-5, hm_youngs_modulus=1e6, hm_poisson_ratio=0.3,
+                              hm_restitution=0.3, hm_friction=0.5)),
+}
+
+
+def hm_line(rodgpu, args, name, n=None):
+    """One Hertz-Mindlin workload: device time of its steps with the state
+    resident in HBM, with the roofline of the whole velocity-Verlet step."""
+    from rodgpu import scene
+    w = HM_LINES[name]
+    nn = w["n"] if n is None else n
+    t0 = time.perf_counter()
+    if w["device_gen"]:
+        sc = scene.make_rods_device(nn, 1.0, w["d"], phi=w["phi"], seed=args.seed, max_attempts=20000)
+    else:
+        sc = scene.make_rods(nn, 1.0, w["d"], phi=w["phi"], seed=args.seed, max_attempts=20000)
+    t_gen = time.perf_counter() - t0
+    kw = dict(w["cfg"], gravity=(0.0, 0.0, 0.0), lin_damp=0.0, ang_damp=0.0)
+    kw.update(scene.pbc_kwargs(sc))
+    s = load_system(rodgpu, rodgpu.default_config(n_bodies=sc["n"], **kw), sc)
+    steps = args.hm_steps or w["steps"]
+    s.step(max(3, args.warmup))
+    st = s.step(steps)
+    ms = st["device_ms"]
+    m = sc["n"]
+    out = {"value": round(m * steps / (ms / 1000.0), 1), "unit": "rod-steps/s", "rods": m,
+           "phi": round(sc["phi"], 4), "steps": steps, "ms_per_step": round(ms / steps, 5),
+           "contacts_per_evaluation": round(st["contact_steps"] / (2.0 * steps), 1),
+           "kernel_launches": int(st["kernel_launches"]),
+           "launches_per_step": round(st["kernel_launches"] / steps, 1),
+           "scene_s": round(t_gen, 2), "scene_generator": "device" if w["device_gen"] else "host",
+           "roofline": roofline(verlet_bytes(m * steps, st["contact_steps"]), ms,
+                                "velocity-Verlet step, all kernels (Hertz-Mindlin)", None)}
+    s.close()
+    return out
+
+
 def train_network(rodgpu, args):
     """Records converged impulses of plain PSOR on separate seeded systems
     and trains the network with the library's kernels."""
@@ -284,6 +342,7 @@ def run_ours(args, rank, world):
 
     roof = roofline(res["bytes"], res["ms"], "k_nsc_run (batched, learned warm start)",
                     profile_traffic("k_nsc_run_batch.md", n_total * args.steps))
+    hm = {} if args.no_hm else {name: hm_line(rodgpu, args, name) for name in HM_LINES}
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "rod-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
@@ -305,6 +364,7 @@ def run_ours(args, rank, world):
                 "path": "rg_batch_set_state_all + rg_batch_step(1) + rg_batch_get_state_all, pinned host arrays"},
         "gpu_launches": res["kernel_launches"],
         "roofline": roof,
+        "hertz_mindlin": hm,
         "clocks": clk.summary(),
     }
     return out
@@ -361,6 +421,15 @@ def run_single(args, rank, world):
     import rodgpu
     import torch
     dev = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload in HM_LINES:
+        with ClockSampler(dev) as clk:
+            r = hm_line(rodgpu, args, args.workload, args.n)
+        return {"metric": "rod-steps/s (Hertz-Mindlin velocity Verlet)", "value": r["value"], "unit": "rod-steps/s",
+                "n_gpus": world, "steps": r["steps"], "warmup": max(3, args.warmup),
+                "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded RSA packing)",
+                "config": {"workload": f"{args.workload}: N={r['rods']}"}, "gpu_launches": r["kernel_launches"],
+                "clocks": clk.summary(), "roofline": r["roofline"], "detail": r}
     if args.workload.startswith("member:"):
         # one member of the batch workload, stepped by a single block (the
         # team the batch schedule gives a member of moderate size)
@@ -476,6 +545,8 @@ def main():
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-hm", action="store_true", help="skip the Hertz-Mindlin workloads")
+    ap.add_argument("--hm-steps", type=int, default=0, help="timed steps of a Hertz-Mindlin workload (0: its own)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -156,7 +156,8 @@ typedef struct rg_step_stats {
   double device_ms;         /* device time of the call (CUDA events, stream)  */
   int64_t psor_row_sweeps;  /* NSC: Σ over steps of contacts x sweeps         */
   int64_t kernel_launches;  /* kernels this library launched during the call  */
-  int64_t contact_steps;    /* NSC: Σ over steps of velocity-solve contacts   */
+  int64_t contact_steps;    /* NSC: Σ over steps of velocity-solve contacts;
+                               soft / HM: Σ over force evaluations of contacts */
   int64_t near_rebuilds;    /* NSC: near-list rebuilds in this call           */
   int64_t reserved[1];
 } rg_step_stats;
@@ -251,6 +252,21 @@ int rg_get_profile(const rg_system* sys, double* ms, int64_t* launches);
  * 5 position update, 6 projection detection, 7 projection colouring,
  * 8 projection sweeps. */
 int rg_get_phase_times(const rg_system* sys, double* ms, int n);
+
+/* ---- seeded packings generated on the device ------------------------------ */
+/* Replaces the host populate of the reference's scenes ("nonoverlap",
+ * src/app/main.cpp:1857-2140): up to n rods of length L and diameter d in
+ * the periodic cube [lo, lo+side)^3, centres uniform, axes uniform on S^2,
+ * no two closer than d (nearest periodic image).  Parallel random
+ * sequential addition: every unplaced rod draws candidates at once, each
+ * round; overlapping survivors keep the lower index.  Stops when every rod
+ * is placed or the first rod has used max_attempts draws (the host loop
+ * stops at its first unplaceable rod too).  x[3n], q[4n] (w,x,y,z): HOST
+ * outputs, placed rods first, in index order; *placed = their number.  The
+ * packing depends only on the arguments (not on thread timing).  Needs
+ * side >= 3 (L + d) (RG_ERR_ARG otherwise).  Allocates device scratch. */
+int rg_scene_rsa_device(int n, double L, double d, double lo, double side, uint64_t seed, int max_attempts,
+                        double* x, double* q, int* placed);
 
 /* ---- detection without device allocation --------------------------------- */
 /* No counterpart in the reference: this entry point exists for callers that

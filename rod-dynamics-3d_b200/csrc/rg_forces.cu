@@ -173,6 +173,7 @@ __global__ void k_hist_finish(const int* toff, const int* koff, Ctl* ctl) {
   if (ctl->err) return;
   int T = toff[ctl->contacts], K = koff[ctl->hist_n];
   ctl->hist_n = T + K;
+  ctl->contact_steps += ctl->contacts;  // contact-evaluations of the call
 }
 
 // ---------------------------------------------------------------------------

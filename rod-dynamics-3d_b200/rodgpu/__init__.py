@@ -33,7 +33,7 @@ ABI_SYMBOLS = [
     "rg_destroy", "rg_get_config", "rg_set_bodies", "rg_set_state", "rg_get_state", "rg_step",
     "rg_detect", "rg_get_impulses", "rg_set_network_export", "rg_get_contact_network",
     "rg_compute_forces", "rg_get_history", "rg_set_profiling",
-    "rg_get_profile", "rg_get_phase_times", "rg_detect_noalloc",
+    "rg_get_profile", "rg_get_phase_times", "rg_scene_rsa_device", "rg_detect_noalloc",
     "rg_mlp_param_count", "rg_mlp_set_params", "rg_mlp_get_params", "rg_mlp_record",
     "rg_mlp_records", "rg_mlp_train", "rg_mlp_infer", "rg_batch_create", "rg_batch_destroy",
     "rg_batch_set_bodies", "rg_batch_set_state", "rg_batch_get_state", "rg_batch_step",
@@ -68,6 +68,8 @@ def lib():
         L.rg_get_impulses.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.POINTER(_i),
                                       ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L.rg_compute_forces.argtypes = [P, dp, dp, dp]
+        L.rg_scene_rsa_device.argtypes = [ctypes.c_int, _d, _d, _d, _d, ctypes.c_uint64, ctypes.c_int, dp, dp,
+                                          ctypes.POINTER(ctypes.c_int)]
         L.rg_set_network_export.argtypes = [P, ctypes.c_int]
         L.rg_get_contact_network.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.c_size_t,
                                              ctypes.POINTER(ctypes.c_size_t)]

@@ -73,6 +73,40 @@ def make_rods(n, L, d, phi=None, side=None, seed=1, sigma_v=0.1, sigma_w=0.1, de
             "restitution": np.full(m, float(restitution)), "x": x, "q": q, "v": v, "w": w}
 
 
+def make_rods_device(n, L, d, phi=None, side=None, seed=1, sigma_v=0.1, sigma_w=0.1, density=1.0,
+                     restitution=0.2, max_attempts=2000):
+    """make_rods with the positions and axes drawn by the device generator
+    (rg_scene_rsa_device: parallel random sequential addition); velocities
+    and mass properties as make_rods.  For packings too large for the host
+    loop."""
+    import ctypes
+    from . import lib
+    if side is None:
+        side = box_side(n, L, d, phi)
+    lo = -0.5 * side
+    x = np.zeros((n, 3))
+    q = np.zeros((n, 4))
+    placed = ctypes.c_int()
+    rc = lib().rg_scene_rsa_device(int(n), float(L), float(d), float(lo), float(side), int(seed),
+                                   int(max_attempts), ptr(x), ptr(q), ctypes.byref(placed))
+    if rc != 0:
+        raise RuntimeError(f"rg_scene_rsa_device failed with status {rc}")
+    m = placed.value
+    H = _gen(None)
+    v = np.zeros((m, 3))
+    w = np.zeros((m, 3))
+    H.rg_scene_velocities(int(m), float(sigma_v), float(sigma_w), int(seed), ptr(v), ptr(w))
+    radius = np.full(m, 0.5 * d)
+    half = np.full(m, 0.5 * L)
+    mass = np.zeros(m)
+    inertia = np.zeros((m, 3))
+    H.rg_capsule_mass(int(m), ptr(radius), ptr(half), ptr(np.full(m, float(density))), ptr(mass), ptr(inertia))
+    return {"n": m, "requested": n, "L": L, "d": d, "side": side, "lo": lo,
+            "phi": m * capsule_volume(L, d) / side ** 3, "radius": radius, "half_height": half, "mass": mass,
+            "inertia": inertia, "restitution": np.full(m, float(restitution)), "x": x[:m].copy(),
+            "q": q[:m].copy(), "v": v, "w": w}
+
+
 def pbc_kwargs(scene):
     lo, side = scene["lo"], scene["side"]
     return {"pbc_enabled": 1, "pbc_min": (lo, lo, lo), "pbc_max": (lo + side, lo + side, lo + side)}
