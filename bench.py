@@ -229,6 +229,60 @@ def hm_line(rodgpu, args, name, n=None):
     return out
 
 
+def secondary_gpu_baseline(rodgpu, args, sizes=(10000, 50000, 100000)):
+    """The reference's own FP32 two-pass CUDA broad phase
+    (cudaDetectCapsulePairsTwoPass: AABB kernel, O(N^2) AABB pair kernel,
+    Lumelsky narrow phase; built for sm_100a from the reference's source)
+    against rg_detect on the same packings: aspect ratio 20 (L = 1,
+    d = 0.05) at phi 0.10, generated at 0.9 d so contacts exist.  Both are
+    timed as whole calls from host arrays to host contact lists (wall
+    clock, median of 3 after one untimed call); the reference's own stage
+    timers are reported beside them.  'ours_first' is the first call on a
+    system, which builds the neighbour lists; 'ours' is a repeated call
+    (lists kept, as in a running simulation)."""
+    from oracle import refcuda_detect
+    from rodgpu import scene
+    out = []
+    for n in sizes:
+        side = scene.box_side(n, 1.0, 0.05, 0.10)
+        sc = scene.make_rods_device(n, 1.0, 0.045, side=side, seed=args.seed + 7)
+        sc["radius"] = np.full(sc["n"], 0.025)
+        kw = dict(model="nsc", gravity=(0.0, 0.0, 0.0))
+        kw.update(scene.pbc_kwargs(sc))
+        s = rodgpu.System(rodgpu.default_config(n_bodies=sc["n"], **kw))
+        s.set_bodies(sc["radius"], sc["half_height"], sc["mass"], sc["inertia"], sc["restitution"])
+        s.set_state(sc["x"], sc["q"], sc["v"], sc["w"])
+        t0 = time.perf_counter()
+        mine, _, _ = s.detect(0.0)
+        first = (time.perf_counter() - t0) * 1e3
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            mine, _, _ = s.detect(0.0)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        s.close()
+        box = (side, side, side)
+        refcuda_detect(sc, 0.0, box)
+        walls, stages = [], []
+        for _ in range(3):
+            theirs, st, wall = refcuda_detect(sc, 0.0, box)
+            walls.append(wall)
+            stages.append(st)
+        st = np.median(np.array(stages), axis=0)
+        a = {tuple(p) for p in mine.tolist()}
+        b = {tuple(p) for p in theirs.tolist()}
+        out.append({"n": int(sc["n"]), "ours_first_ms": round(first, 3), "ours_ms": round(float(np.median(ts)), 3),
+                    "reference_ms": round(float(np.median(walls)), 3),
+                    "reference_kernels_ms": round(float(st[1] + st[2] + st[3]), 3),
+                    "reference_stages_ms": {"upload": round(float(st[0]), 3), "aabb": round(float(st[1]), 3),
+                                            "pair_test": round(float(st[2]), 3),
+                                            "narrow": round(float(st[3]), 3), "download": round(float(st[4]), 3)},
+                    "reference_candidates": int(st[5]),
+                    "contacts": {"ours_fp64": len(a), "reference_fp32": len(b), "common": len(a & b)},
+                    "speedup_call": round(float(np.median(walls)) / max(float(np.median(ts)), 1e-9), 2)})
+    return out
+
+
 def train_network(rodgpu, args):
     """Records converged impulses of plain PSOR on separate seeded systems
     and trains the network with the library's kernels."""
@@ -343,6 +397,10 @@ def run_ours(args, rank, world):
     roof = roofline(res["bytes"], res["ms"], "k_nsc_run (batched, learned warm start)",
                     profile_traffic("k_nsc_run_batch.md", n_total * args.steps))
     hm = {} if args.no_hm else {name: hm_line(rodgpu, args, name) for name in HM_LINES}
+    try:
+        second = secondary_gpu_baseline(rodgpu, args)
+    except Exception as e:  # noqa: BLE001
+        second = {"unavailable": str(e)}
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "rod-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
@@ -365,6 +423,7 @@ def run_ours(args, rank, world):
         "gpu_launches": res["kernel_launches"],
         "roofline": roof,
         "hertz_mindlin": hm,
+        "secondary_gpu_baseline": second,
         "clocks": clk.summary(),
     }
     return out

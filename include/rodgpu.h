@@ -122,7 +122,9 @@ typedef struct rg_config {
                                     warm cache is empty (default 3; -1: in
                                     every step)                              */
   int32_t near_skin_pct;         /* near-list skin, % of the Verlet skin (0:
-                                    automatic: 5 %, 50 % in all-pairs boxes) */
+                                    automatic: 5 %, 50 % in all-pairs boxes;
+                                    negative: the soft / HM detection tests
+                                    the full lists every step)              */
   /* Bounded device waits.  Every team barrier of the persistent step polls
    * at most spin_limit times (0: the default 2e7 polls, about 1-2 s) and
    * then records RG_ERR_TIMEOUT; every block of the launch then returns and

@@ -29,10 +29,11 @@ dp = ctypes.POINTER(_d)
 
 
 def build(ref=True):
-    """Compiles the oracle (and the reference, when its tree is present)."""
+    """Compiles the oracle (and the reference's CPU and CUDA sources, when
+    its tree is present)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if ref and os.path.isdir(REF_TREE):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "refcuda", f"REF={REF_TREE}"], check=True)
 
 
 def _p(a, t=_d):
@@ -97,6 +98,42 @@ def ref_lib():
         L.ref_compute_forces.argtypes = [P, dp, dp]
         _ref = L
     return _ref
+
+
+REFCUDA_LIB = os.path.join(HERE, "_ref", "librodref_cuda.so")
+_refcuda = None
+
+
+def refcuda_lib():
+    """The reference's FP32 two-pass CUDA broad phase (secondary GPU
+    baseline), built for sm_100a by the Makefile's refcuda target."""
+    global _refcuda
+    if _refcuda is None:
+        if not os.path.exists(REFCUDA_LIB):
+            raise RuntimeError("reference CUDA broad phase not built (oracle/Makefile refcuda)")
+        L = ctypes.CDLL(REFCUDA_LIB)
+        L.refcuda_detect.argtypes = [ctypes.c_int, dp, dp, dp, dp, _d, ctypes.c_int, _d, _d, _d,
+                                     ctypes.POINTER(_i), ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), dp, dp]
+        _refcuda = L
+    return _refcuda
+
+
+def refcuda_detect(sc, margin, box):
+    """Pairs (sorted) found by the reference's cudaDetectCapsulePairsTwoPass,
+    its stage times (upload, aabb, broadphase, narrowphase, download ms;
+    candidates; contacts) and the call's wall time in ms."""
+    L = refcuda_lib()
+    n = sc["n"]
+    arr = [np.ascontiguousarray(sc[k], np.float64) for k in ("x", "q", "radius", "half_height")]
+    cap = 64 * n + 16
+    pairs = np.zeros((cap, 2), np.int32)
+    cnt = ctypes.c_size_t()
+    stats = np.zeros(7)
+    wall = ctypes.c_double()
+    rc = L.refcuda_detect(n, *[_p(a) for a in arr], float(margin), 1, float(box[0]), float(box[1]), float(box[2]),
+                          _p(pairs, _i), cap, ctypes.byref(cnt), _p(stats), ctypes.byref(wall))
+    assert rc == 0, rc
+    return pairs[:min(cnt.value, cap)], stats, wall.value
 
 
 class Oracle:

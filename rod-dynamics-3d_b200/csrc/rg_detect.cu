@@ -23,71 +23,94 @@ namespace rg {
 long long g_launches = 0;
 
 // ---------------------------------------------------------------------------
-// Exclusive scan (three launches, capacity-sized grids, device-side n).
+// Exclusive scan in one pass: decoupled look-back (Merrill & Garland, "Single-
+// pass Parallel Prefix Scan with Decoupled Look-back", 2016).  Blocks take
+// tiles in increasing order from a counter; a tile publishes its aggregate,
+// adds the published values of its predecessors until it meets an inclusive
+// prefix, then publishes its own inclusive prefix and writes its outputs.
+// A tile only waits on tiles taken before it by running blocks, and every
+// wait is bounded (ERR_TIMEOUT after kScanSpin polls).  n is read on the
+// device; the tile status words are cleared by a memset before each scan.
 // ---------------------------------------------------------------------------
 constexpr int kScanBS = 1024;
 constexpr int kScanItems = 2;
 constexpr int kScanTile = kScanBS * kScanItems;
+constexpr long long kScanSpin = 1 << 24;
+constexpr unsigned long long kTileAgg = 1ull << 62, kTileInc = 2ull << 62;
 
-__global__ void k_scan_tiles(const int* in, int* out, const int* n_dev, int* blocks) {
+__global__ void k_scan_lookback(const int* in, int* out, const int* n_dev, unsigned long long* status, int* err) {
   __shared__ int shw[32];
-  int n = *n_dev;
-  int ntile = (n + kScanTile - 1) / kScanTile;
-  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
-    int base = t * kScanTile + threadIdx.x * kScanItems;
-    int v0 = base < n ? in[base] : 0;
-    int v1 = base + 1 < n ? in[base + 1] : 0;
-    int tot;
-    int ex = block_excl_scan(v0 + v1, shw, tot);
-    if (base < n) out[base] = ex;
-    if (base + 1 < n) out[base + 1] = ex + v0;
-    if (threadIdx.x == 0) blocks[t] = tot;
+  __shared__ int sh_tile, sh_excl;
+  int* tile_ctr = reinterpret_cast<int*>(status);  // word 0; tile t's status is status[t + 1]
+  const int n = *n_dev;
+  const int ntile = (n + kScanTile - 1) / kScanTile;
+  if (ntile == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = 0;
+    return;
   }
-}
-
-__global__ void k_scan_blocks(int* blocks, const int* n_dev, int* out) {
-  __shared__ int shw[32];
-  int n = *n_dev;
-  int ntile = (n + kScanTile - 1) / kScanTile;
-  int carry = 0;
-  for (int base = 0; base < ntile; base += blockDim.x) {
-    int i = base + threadIdx.x;
-    int v = i < ntile ? blocks[i] : 0;
+  for (;;) {
+    if (threadIdx.x == 0) sh_tile = atomicAdd(tile_ctr, 1);
+    __syncthreads();
+    const int t = sh_tile;
+    if (t >= ntile) return;
+    const int base = t * kScanTile + threadIdx.x * kScanItems;
+    const int v0 = base < n ? in[base] : 0;
+    const int v1 = base + 1 < n ? in[base + 1] : 0;
     int tot;
-    int ex = block_excl_scan(v, shw, tot);
-    if (i < ntile) blocks[i] = carry + ex;
-    carry += tot;
-  }
-  if (threadIdx.x == 0) out[n] = carry;
-}
-
-__global__ void k_scan_add(int* out, const int* n_dev, const int* blocks) {
-  int n = *n_dev;
-  int ntile = (n + kScanTile - 1) / kScanTile;
-  for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
-    int add = blocks[t];
-    if (add == 0) continue;
-    int base = t * kScanTile + threadIdx.x * kScanItems;
-    if (base < n) out[base] += add;
-    if (base + 1 < n) out[base + 1] += add;
+    const int ex = block_excl_scan(v0 + v1, shw, tot);
+    if (threadIdx.x == 0) {
+      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> mine(status[t + 1]);
+      int prefix = 0;
+      if (t == 0) {
+        mine.store(kTileInc | (unsigned)tot, cuda::memory_order_release);
+      } else {
+        mine.store(kTileAgg | (unsigned)tot, cuda::memory_order_release);
+        for (int p = t - 1; p >= 0;) {
+          cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> prev(status[p + 1]);
+          unsigned long long w = prev.load(cuda::memory_order_acquire);
+          long long it = 0;
+          while ((w >> 62) == 0) {
+            if (++it > kScanSpin) {
+              atomicOr(err, ERR_TIMEOUT);
+              break;
+            }
+            if (it > 32) __nanosleep(32);
+            w = prev.load(cuda::memory_order_acquire);
+          }
+          if ((w >> 62) == 0) break;  // gave up: the call fails with ERR_TIMEOUT
+          prefix += (int)(unsigned)(w & 0xffffffffull);
+          if (w & kTileInc) break;
+          --p;
+        }
+        mine.store(kTileInc | (unsigned)(prefix + tot), cuda::memory_order_release);
+      }
+      sh_excl = prefix;
+      if (t == ntile - 1) out[n] = prefix + tot;
+    }
+    __syncthreads();
+    const int add = sh_excl;
+    if (base < n) out[base] = add + ex;
+    if (base + 1 < n) out[base + 1] = add + ex + v0;
+    __syncthreads();  // sh_tile / sh_excl are reused by the next tile
   }
 }
 
 cudaError_t Scan::alloc(int cap_) {
   cap = cap_;
-  return cudaMalloc(&d_blocks, sizeof(int) * ((cap + kScanTile - 1) / kScanTile + 1));
+  const int tiles = (cap + kScanTile - 1) / kScanTile + 1;
+  return cudaMalloc(&d_blocks, sizeof(unsigned long long) * (tiles + 1));
 }
 void Scan::free_() {
   if (d_blocks) cudaFree(d_blocks);
   d_blocks = nullptr;
 }
-void Scan::run(const int* in, int* out, const int* n_dev, cudaStream_t s) const {
-  int tiles = (cap + kScanTile - 1) / kScanTile;
-  int g = tiles < 148 * 4 ? tiles : 148 * 4;
+void Scan::run(const int* in, int* out, const int* n_dev, int* err, cudaStream_t s) const {
+  const int tiles = (cap + kScanTile - 1) / kScanTile + 1;
+  int g = tiles < 148 * 2 ? tiles : 148 * 2;
   if (g < 1) g = 1;
-  RGL k_scan_tiles<<<g, kScanBS, 0, s>>>(in, out, n_dev, d_blocks);
-  RGL k_scan_blocks<<<1, kScanBS, 0, s>>>(d_blocks, n_dev, out);
-  RGL k_scan_add<<<g, kScanBS, 0, s>>>(out, n_dev, d_blocks);
+  unsigned long long* status = reinterpret_cast<unsigned long long*>(d_blocks);
+  cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (tiles + 1), s);
+  RGL k_scan_lookback<<<g, kScanBS, 0, s>>>(in, out, n_dev, status, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -105,37 +128,79 @@ __global__ void k_seg(State st, Seg* seg) {
 }
 
 // Largest displacement bound |Δx| + h|Δu| since the last build; sets the
-// rebuild flag when it reaches skin/2.
-__global__ void k_disp_check(State st, const Seg* seg, const double* ref, Box box, double skin,
-                             Ctl* ctl) {
+// rebuild flag when it reaches skin/2.  With ref2 (near lists), the largest
+// bound since the last near-list build goes to ctl->near_disp.
+__global__ void k_disp_check(State st, const Seg* seg, const double* ref, const double* ref2, Box box,
+                             double skin, Ctl* ctl) {
   if (ctl->err) return;
-  __shared__ double sm[32];
-  double m = 0.0;
+  __shared__ double sm[32], sm2[32];
+  double m = 0.0, m2 = 0.0;
   const int n = st.n;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     Seg s = seg[i];
-    d3 dx{s.cx - ref[i], s.cy - ref[n + i], s.cz - ref[2 * n + i]};
-    if (box.pbc) {
-      if (box.L[0] > 0.0) dx.x -= floor(dx.x / box.L[0] + 0.5) * box.L[0];
-      if (box.L[1] > 0.0) dx.y -= floor(dx.y / box.L[1] + 0.5) * box.L[1];
-      if (box.L[2] > 0.0) dx.z -= floor(dx.z / box.L[2] + 0.5) * box.L[2];
-    }
-    d3 du{s.ux - ref[3 * n + i], s.uy - ref[4 * n + i], s.uz - ref[5 * n + i]};
-    double d = len(dx) + s.h * len(du);
-    if (!(d == d)) d = 1e300;  // non-finite state forces a rebuild
-    m = fmax(m, d);
+    m = fmax(m, seg_disp(s, ref, n, i, box));  // non-finite state: 1e300 forces a rebuild
+    if (ref2) m2 = fmax(m2, seg_disp(s, ref2, n, i, box));
   }
   m = warp_max(m);
-  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+  m2 = warp_max(m2);
+  if ((threadIdx.x & 31) == 0) {
+    sm[threadIdx.x >> 5] = m;
+    sm2[threadIdx.x >> 5] = m2;
+  }
   __syncthreads();
   if (threadIdx.x < 32) {
     double v = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+    double v2 = threadIdx.x < (blockDim.x >> 5) ? sm2[threadIdx.x] : 0.0;
     v = warp_max(v);
+    v2 = warp_max(v2);
     if (threadIdx.x == 0) {
       atomic_max_nonneg(&ctl->maxdisp, v);
       if (v >= 0.5 * skin * (1.0 - 1e-9)) atomicExch(&ctl->rebuild, 1);
+      if (ref2) atomic_max_nonneg(&ctl->near_disp, v2);
     }
   }
+}
+
+// Near lists (multi-kernel detection): rebuilt when the lists were rebuilt
+// (near_valid cleared) or some rod's bound since the near build reached
+// near_skin/2.  A pair left out was, at the build, farther apart than
+// r_a + r_b + margin + near_skin by seg_far's lower bound, and each of its
+// rods has since moved less than near_skin/2 (the segment distance is
+// 1-Lipschitz in the end points), so it cannot be within r_a + r_b + margin.
+__device__ inline bool near_rebuild_due(const Ctl* ctl, double near_skin) {
+  return !ctl->near_valid || ctl->near_disp >= 0.5 * near_skin * (1.0 - 1e-9);
+}
+
+__global__ void k_near_build(const Seg* seg, int n, const double* inv_mass, Box box, double extra,
+                             double near_skin, const int* nbr_cnt, const int* nbr, int maxnb, int* near_cnt,
+                             int* near_nbr, double* ref2, const Ctl* ctl) {
+  if (ctl->err || !near_rebuild_due(ctl, near_skin)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const Seg A = seg[i];
+    const bool a_static = !(inv_mass[i] > 0.0);
+    const int cnt = nbr_cnt[i];
+    const int* list = nbr + (size_t)i * maxnb;
+    int* out = near_nbr + (size_t)i * maxnb;
+    int m = 0;
+    for (int k = 0; k < cnt; ++k) {
+      const int j = list[k];
+      if (a_static && !(inv_mass[j] > 0.0)) continue;
+      const Seg B = seg[j];
+      d3 xa{A.cx, A.cy, A.cz}, xb{B.cx, B.cy, B.cz};
+      if (seg_far(A, B, (xb - xa) + min_image_shift(box, xa, xb), A.r + B.r + extra)) continue;
+      out[m++] = j;
+    }
+    near_cnt[i] = m;
+    ref2[i] = A.cx; ref2[n + i] = A.cy; ref2[2 * n + i] = A.cz;
+    ref2[3 * n + i] = A.ux; ref2[4 * n + i] = A.uy; ref2[5 * n + i] = A.uz;
+  }
+}
+
+__global__ void k_near_done(double near_skin, Ctl* ctl) {
+  if (ctl->err || !near_rebuild_due(ctl, near_skin)) return;
+  ctl->near_valid = 1;
+  ctl->near_disp = 0.0;
+  ctl->near_rebuilds += 1;
 }
 
 __global__ void k_cell_fill(int n, const int* cell_of, const int* cell_start, int* cell_fill,
@@ -197,6 +262,7 @@ __global__ void k_build_done(Ctl* ctl) {
   if (ctl->rebuild) {
     ctl->rebuilds += 1;
     ctl->rebuild = 0;
+    ctl->near_valid = 0;  // near lists are drawn from the lists
   }
   ctl->maxdisp = 0.0;
 }
@@ -295,7 +361,11 @@ __global__ void k_grid_ncells(DetDev* dd, const Ctl* ctl) {
   dd->ncells = dd->grid.ncells;
 }
 
+// Near lists are on unless near_skin_pct is negative (full lists).
+static bool check_near_lists(const rg_config& c) { return c.near_skin_pct >= 0; }
+
 cudaError_t detector_alloc(rg_system* s) {
+  ++s->buf_gen;
   Detector& d = s->det;
   const int n = s->n;
   const rg_config& c = s->cfg;
@@ -357,6 +427,13 @@ cudaError_t detector_alloc(rg_system* s) {
   if ((e = cudaMalloc(&d.hit_off, sizeof(int) * (n + 1)))) return e;
   if ((e = cudaMalloc(&d.hit_mask, sizeof(unsigned long long) * (size_t)n * d.mask_words))) return e;
   if ((e = cudaMemset(d.nbr_cnt, 0, sizeof(int) * n))) return e;
+  if (c.model != RG_MODEL_NSC && !d.all_pairs && check_near_lists(c)) {
+    // near lists of the multi-kernel detection (the soft / HM step)
+    d.near_skin = (c.near_skin_pct > 0 ? 0.01 * c.near_skin_pct : 0.05) * d.skin;
+    if ((e = cudaMalloc(&d.near_cnt, sizeof(int) * n))) return e;
+    if ((e = cudaMalloc(&d.near_nbr, sizeof(int) * (size_t)n * d.maxnb))) return e;
+    if ((e = cudaMalloc(&d.ref2, sizeof(double) * 6 * (size_t)n))) return e;
+  }
   if (c.model == RG_MODEL_NSC) {
     // all-pairs boxes rebuild the near list from every pair: a wider near
     // skin makes those rebuilds rare
@@ -379,6 +456,7 @@ void detector_free(rg_system* s) {
   cudaFree(d.cell_of); cudaFree(d.cell_cnt); cudaFree(d.cell_start); cudaFree(d.cell_fill);
   cudaFree(d.cell_rods); cudaFree(d.hit_cnt); cudaFree(d.hit_off); cudaFree(d.hit_mask);
   cudaFree(d.near); cudaFree(d.ref2); cudaFree(d.moved);
+  cudaFree(d.near_cnt); cudaFree(d.near_nbr);
   d = Detector();
 }
 
@@ -398,9 +476,10 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild) {
   DetDev* dd = det_dev(s);
   const int bs = 256;
   const int g = grid_for(n, bs);
+  const bool near = d.near_cnt != nullptr;
   RGL k_seg<<<g, bs, 0, st>>>(s->st, d.seg);
   if (check_rebuild && !d.all_pairs)
-    RGL k_disp_check<<<g, bs, 0, st>>>(s->st, d.seg, d.ref, s->box, d.skin, ctl);
+    RGL k_disp_check<<<g, bs, 0, st>>>(s->st, d.seg, d.ref, near ? d.ref2 : nullptr, s->box, d.skin, ctl);
   // --- rebuild: every kernel below returns at once unless ctl->rebuild ---
   if (!s->box.pbc) {
     cudaMemsetAsync(dd->mn, 0xff, sizeof(dd->mn), st);
@@ -412,7 +491,7 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild) {
   RGL k_zero_cells<<<grid_for((d.ncells + 1 > n ? d.ncells + 1 : n), bs), bs, 0, st>>>(d.cell_cnt, d.cell_fill, d.ncells,
                                                                                      d.nbr_cnt, n, ctl);
   RGL k_cell_count_dyn<<<g, bs, 0, st>>>(d.seg, n, &dd->grid, s->box.pbc, d.cell_of, d.cell_cnt, ctl);
-  s->scan.run(d.cell_cnt, d.cell_start, &dd->ncells, st);
+  s->scan.run(d.cell_cnt, d.cell_start, &dd->ncells, &ctl->err, st);
   RGL k_cell_fill<<<g, bs, 0, st>>>(n, d.cell_of, d.cell_start, d.cell_fill, d.cell_rods, ctl);
   int gb = d.ncells < s->sm_count * 8 ? d.ncells : s->sm_count * 8;
   RGL k_build_lists<<<gb, kTile, 0, st>>>(d.seg, n, &dd->grid, s->box, d.cell_start, d.cell_rods,
@@ -420,11 +499,21 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild) {
                                        d.nbr_cnt, d.nbr, d.maxnb, ctl);
   RGL k_save_ref<<<g, bs, 0, st>>>(d.seg, n, d.ref, d.nbr, d.nbr_cnt, d.maxnb, ctl);
   RGL k_build_done<<<1, 1, 0, st>>>(ctl);
+  // --- near lists (every kernel below returns at once unless they are due) ---
+  const int* lcnt = d.nbr_cnt;
+  const int* lnbr = d.nbr;
+  if (near) {
+    RGL k_near_build<<<g, bs, 0, st>>>(d.seg, n, s->st.inv_mass, s->box, d.margin + d.near_skin, d.near_skin,
+                                       d.nbr_cnt, d.nbr, d.maxnb, d.near_cnt, d.near_nbr, d.ref2, ctl);
+    RGL k_near_done<<<1, 1, 0, st>>>(d.near_skin, ctl);
+    lcnt = d.near_cnt;
+    lnbr = d.near_nbr;
+  }
   // --- narrow phase ---
-  RGL k_narrow_count<<<g, bs, 0, st>>>(d.seg, s->st, s->box, delta, d.nbr_cnt, d.nbr, d.maxnb,
+  RGL k_narrow_count<<<g, bs, 0, st>>>(d.seg, s->st, s->box, delta, lcnt, lnbr, d.maxnb,
                                    d.mask_words, d.hit_mask, d.hit_cnt, ctl);
-  s->scan.run(d.hit_cnt, d.hit_off, &dd->n, st);
-  RGL k_narrow_write<<<g, bs, 0, st>>>(d.seg, n, s->box, d.nbr_cnt, d.nbr, d.maxnb, d.mask_words,
+  s->scan.run(d.hit_cnt, d.hit_off, &dd->n, &ctl->err, st);
+  RGL k_narrow_write<<<g, bs, 0, st>>>(d.seg, n, s->box, lcnt, lnbr, d.maxnb, d.mask_words,
                                    d.hit_mask, d.hit_off, s->con, ctl);
 }
 

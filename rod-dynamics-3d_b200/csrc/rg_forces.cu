@@ -71,7 +71,7 @@ void csr_launch(rg_system* s) {
   cudaStream_t st = s->stream;
   RGL k_csr_zero<<<grid_for(s->n + 1, bs), bs, 0, st>>>(s->csr.cnt, s->csr.fill, s->n, s->d_ctl);
   RGL k_csr_count<<<grid_for(s->ccap, bs), bs, 0, st>>>(s->con.a, s->con.b, s->csr.cnt, s->d_ctl);
-  s->scan.run(s->csr.cnt, s->csr.off, detector_n_dev(s), st);
+  s->scan.run(s->csr.cnt, s->csr.off, detector_n_dev(s), &s->d_ctl->err, st);
   RGL k_csr_fill<<<grid_for(s->ccap, bs), bs, 0, st>>>(s->con.a, s->con.b, s->csr.off, s->csr.fill,
                                                    s->csr.ent, s->d_ctl);
   RGL k_csr_sort<<<grid_for(s->n, bs), bs, 0, st>>>(s->n, s->csr.off, s->csr.ent, s->d_ctl);
@@ -464,8 +464,8 @@ void force_eval_launch(rg_system* s) {
   // history merge
   RGL k_hist_keep_init<<<grid_for(H.cap, bs), bs, 0, st>>>(H.frame[cur], H.kept, hm ? 1 : 0, s->d_ctl);
   RGL k_hist_keep_clear<<<gc, bs, 0, st>>>(H.found, H.touched, H.kept, s->d_ctl);
-  s->scan.run(H.touched, H.touched_off, &s->d_ctl->contacts, st);
-  s->scan.run(H.kept, H.kept_off, &s->d_ctl->hist_n, st);
+  s->scan.run(H.touched, H.touched_off, &s->d_ctl->contacts, &s->d_ctl->err, st);
+  s->scan.run(H.kept, H.kept_off, &s->d_ctl->hist_n, &s->d_ctl->err, st);
   RGL k_hist_merge<<<gc, bs, 0, st>>>(s->con.a, s->con.b, H.touched, H.touched_off, H.newval, H.key[cur],
                                   H.val[cur], H.frame[cur], H.kept, H.kept_off, H.key[nxt], H.val[nxt],
                                   H.frame[nxt], H.cap, s->ccap, s->d_ctl);

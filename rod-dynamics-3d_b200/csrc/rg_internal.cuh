@@ -12,12 +12,14 @@ namespace rg {
 
 // Exclusive scan of int32 counts: out[0..n] with out[n] = total, n read
 // from the device (n_dev) so launches do not depend on host-known sizes.
+// One pass (decoupled look-back); a wait that runs out sets ERR_TIMEOUT in
+// *err.
 struct Scan {
   int cap = 0;
-  int* d_blocks = nullptr;  // per-block totals
+  void* d_blocks = nullptr;  // tile counter and tile status words
   cudaError_t alloc(int cap_);
   void free_();
-  void run(const int* in, int* out, const int* n_dev, cudaStream_t s) const;
+  void run(const int* in, int* out, const int* n_dev, int* err, cudaStream_t s) const;
 };
 
 // Device-resident control words of one system (one cudaMalloc).
@@ -82,6 +84,11 @@ struct Detector {
   int2* near = nullptr;           // n * maxnb
   double* ref2 = nullptr;         // 6n
   double near_skin = 0;
+  // near lists of the multi-kernel detection (soft / HM models): per rod,
+  // the ascending list entries within reach + near_skin (same layout as
+  // nbr); null when the full lists are used (NSC models, all-pairs boxes)
+  int* near_cnt = nullptr;        // n
+  int* near_nbr = nullptr;        // n * maxnb
   // 1: rod moved (position projection or periodic wrap) since the
   // position-level detection of the step; cleared by the position update
   unsigned char* moved = nullptr;  // n
@@ -211,6 +218,14 @@ struct rg_system {
   int team_blocks = 0;        // blocks of the NSC team (0: automatic)
   cudaGraphExec_t graph = nullptr;
   int graph_kind = -1;
+  // one velocity-Verlet step (soft / HM) captured as a CUDA graph; valid
+  // while the buffers it names are the current ones (buf_gen) and the
+  // history table starts in the same ping-pong buffer (vgraph_cur)
+  cudaGraphExec_t vgraph = nullptr;
+  long long vgraph_gen = -1;
+  int vgraph_cur = -1;
+  long long vgraph_kernels = 0;  // kernel nodes of the graph
+  long long buf_gen = 0;         // bumped by every (re)allocation of device buffers
 
   // pinned staging for host <-> device state copies (19 n doubles)
   double* h_stage = nullptr;
