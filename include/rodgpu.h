@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define RG_ABI_VERSION 1
+#define RG_ABI_VERSION 2
 
 typedef enum rg_status {
   RG_OK = 0,
@@ -135,7 +135,17 @@ typedef struct rg_config {
    * their waits run out after spin_limit polls and the call returns
    * RG_ERR_TIMEOUT (no fault, no hang: the wait is the bounded one above). */
   int32_t test_absent_blocks;
-  int32_t reserved[1];
+  /* Cylindrical tube boundary (SceneCfg::cylinder, config.hpp:150-154):
+   * an infinite tube of radius cylinder_radius about cylinder_axis through
+   * the origin.  NSC: wall manifolds for the sample points of each capsule
+   * (collideCapsuleInsideCylinder, collision.cpp:197-241; main.cpp:
+   * 4431-4447) and spin about the rod axis projected out after the position
+   * update (:4486-4494).  Soft model: a penalty spring with smooth Coulomb
+   * friction at both force evaluations (:4661-4690, :4756-4787).  The
+   * Hertz-Mindlin model has no wall term, as in the reference. */
+  int32_t cylinder_enabled;
+  double cylinder_radius;
+  double cylinder_axis[3];
 } rg_config;
 
 /* Per-call statistics (the profile-CSV columns of main.cpp:3276-3355). */

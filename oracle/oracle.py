@@ -64,6 +64,8 @@ def oracle_lib():
         L.orc_compute_forces.argtypes = [P, dp, dp, dp]
         L.orc_get_contact_network.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.c_size_t,
                                               ctypes.POINTER(ctypes.c_size_t)]
+        L.orc_get_wall_contacts.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.POINTER(_i), ctypes.c_size_t,
+                                            ctypes.POINTER(ctypes.c_size_t)]
         L.orc_get_history.argtypes = [P, ctypes.POINTER(_i), dp, ctypes.POINTER(ctypes.c_int64),
                                       ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L.orc_color.argtypes = [P, ctypes.POINTER(_i), ctypes.c_size_t, ctypes.POINTER(_i),
@@ -196,6 +198,16 @@ class Oracle:
         self.L.orc_get_impulses(self._h, _p(pairs, _i), _p(lam), _p(col, _i), cap, ctypes.byref(n))
         m = n.value
         return pairs[:m], lam[:m], col[:m]
+
+    def wall_contacts(self):
+        n = ctypes.c_size_t()
+        self.L.orc_get_wall_contacts(self._h, None, None, None, 0, ctypes.byref(n))
+        cap = max(1, n.value)
+        body = np.zeros(cap, np.int32)
+        rows = np.zeros((cap, 10))
+        col = np.zeros(cap, np.int32)
+        self.L.orc_get_wall_contacts(self._h, _p(body, _i), _p(rows), _p(col, _i), cap, ctypes.byref(n))
+        return body[:n.value], rows[:n.value], col[:n.value]
 
     def contact_network(self):
         n = ctypes.c_size_t()

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "config/config.hpp"
+#include "physics/collision.hpp"
 #include "physics/contact_detector.hpp"
 #include "physics/hertz_mindlin.hpp"
 #include "physics/integrator.hpp"
@@ -126,11 +127,42 @@ static void hm_capsule_forces(ref_system& S) {
   }
 }
 
+// Cylinder wall of the soft branch, as App::physicsStep applies it after each
+// computeForces (main.cpp:4661-4690, :4756-4787).
+static void soft_wall(ref_system& S) {
+  const rg_config& c = S.cfg;
+  if (!c.cylinder_enabled) return;
+  const float cylR = float(c.cylinder_radius);
+  const glm::vec3 cylAxis = glm::normalize(gv(c.cylinder_axis));
+  const float k_wall = float(c.soft_k_scaler), c_wall = float(c.soft_damping), mu_wall = float(c.soft_mu);
+  const float nu_wall = std::max((float)c.soft_nu, 1e-10f);
+  for (auto& rb : S.rods) {
+    if (rb.invMass <= 0.0f) continue;
+    const float maxD = cylR - rb.cap.r;
+    glm::vec3 p_perp = rb.x - glm::dot(rb.x, cylAxis) * cylAxis;
+    float d_perp = glm::length(p_perp);
+    float pen = d_perp - maxD;
+    if (pen <= 0.0f) continue;
+    glm::vec3 n = (d_perp > 1e-8f) ? p_perp / d_perp
+        : glm::normalize(glm::cross(cylAxis, (std::abs(cylAxis.x) < 0.9f) ? glm::vec3(1, 0, 0) : glm::vec3(0, 1, 0)));
+    float v_n = glm::dot(rb.v, n);
+    float Fn_mag = k_wall * pen + c_wall * std::max(v_n, 0.0f);
+    rb.f -= Fn_mag * n;
+    glm::vec3 v_t = rb.v - v_n * n;
+    float v_t_len = glm::length(v_t);
+    if (v_t_len > 1e-12f) {
+      float smooth = std::tanh(v_t_len / nu_wall);
+      rb.f -= (mu_wall * Fn_mag * smooth / v_t_len) * v_t;
+    }
+  }
+}
+
 static void force_eval(ref_system& S) {
   if (S.cfg.model == RG_MODEL_HARMONIC) {
     S.soft.detectContacts(S.rods);
     S.last_contacts = S.soft.getNumContacts();
     S.soft.computeForces(S.rods, S.cfg.dt, S.gravity);
+    soft_wall(S);
   } else if (S.cfg.model == RG_MODEL_HERTZ_MINDLIN) {
     hm_capsule_forces(S);
   }
@@ -152,6 +184,18 @@ static void nsc_step(ref_system& S) {
     }
   }
   S.nsc.detectAndBuildManifolds(rods);
+  // cylinder wall contacts (main.cpp:4431-4447)
+  if (S.cfg.cylinder_enabled) {
+    const float cylR = float(S.cfg.cylinder_radius);
+    const glm::vec3 cylAxis = glm::normalize(gv(S.cfg.cylinder_axis));
+    std::vector<Contact> cyl;
+    for (int i = 0; i < (int)rods.size(); ++i) {
+      if (rods[i].invMass <= 0.0f) continue;
+      cyl.clear();
+      collideCapsuleInsideCylinder(rods[i], cylR, cylAxis, cyl);
+      for (const auto& c : cyl) S.nsc.addWallContact(i, c, rods, rods[i].restitution);
+    }
+  }
   S.last_contacts = S.nsc.getNumContacts();
   S.nsc.solveVelocities(rods, dt);
   // main.cpp:4469-4483
@@ -167,6 +211,12 @@ static void nsc_step(ref_system& S) {
     float wLen = glm::length(rb.w);
     if (wLen > g_w_max) rb.w *= g_w_max / wLen;
   }
+  // spin about the rod axis projected out inside the tube (main.cpp:4486-4494)
+  if (S.cfg.cylinder_enabled)
+    for (auto& rb : rods) {
+      glm::vec3 u = glm::normalize(rb.axisY());
+      rb.w -= glm::dot(rb.w, u) * u;
+    }
   S.nsc.projectPositions(rods);
   if (g_pbc_enabled) {
     for (auto& rb : rods) {

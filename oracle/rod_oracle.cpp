@@ -125,6 +125,7 @@ struct Manifold {  // NscManifold (include/physics/nsc_contact.hpp:37-63)
   double invMA, invMB;
   double ln = 0, lt1 = 0, lt2 = 0;
   int color = 0;
+  bool wall = false;  // cylinder wall contact of body a (b == a), isWall
 };
 
 inline uint64_t pair_key(int a, int b) {
@@ -573,11 +574,46 @@ void hm_forces(orc_system& S, const std::vector<Contact>& cs) {
 }
 
 // One force evaluation at the current state: detect + computeForces.
+// Cylinder wall of the soft model: penalty spring on the centre's radial
+// overshoot plus smooth Coulomb friction, forces only (main.cpp:4661-4690 at
+// phase t, :4756-4787 at phase t + dt).
+void soft_wall_forces(orc_system& S) {
+  const rg_config& c = S.cfg;
+  if (!c.cylinder_enabled) return;
+  V3 ax = v3(c.cylinder_axis[0], c.cylinder_axis[1], c.cylinder_axis[2]);
+  ax = ax / length(ax);
+  const double k = c.soft_k_scaler, cd = c.soft_damping, mu = c.soft_mu;
+  const double nu = std::max(c.soft_nu, 1e-10);
+  for (int i = 0; i < S.n; ++i) {
+    const Body& B = S.body[i];
+    if (!(B.inv_mass > 0.0)) continue;
+    const double maxd = c.cylinder_radius - B.r;
+    V3 pp = S.x[i] - ax * dot(S.x[i], ax);
+    double d = length(pp);
+    double pen = d - maxd;
+    if (pen <= 0.0) continue;
+    V3 n;
+    if (d > 1e-8) {
+      n = pp / d;
+    } else {
+      V3 cr = cross(ax, std::fabs(ax.x) < 0.9 ? v3(1, 0, 0) : v3(0, 1, 0));
+      n = cr / length(cr);
+    }
+    double vn = dot(S.v[i], n);
+    double fn = k * pen + cd * std::max(vn, 0.0);
+    S.f[i] -= n * fn;
+    V3 vt = S.v[i] - n * vn;
+    double vtl = length(vt);
+    if (vtl > 1e-12) S.f[i] -= vt * (mu * fn * std::tanh(vtl / nu) / vtl);
+  }
+}
+
 void force_eval(orc_system& S) {
   if (S.cfg.model == RG_MODEL_HARMONIC) {
     auto cs = detect(S, S.cfg.soft_delta);
     S.last_contacts = (int64_t)cs.size();
     soft_forces(S, cs);
+    soft_wall_forces(S);
   } else if (S.cfg.model == RG_MODEL_HERTZ_MINDLIN) {
     S.hm_frame++;  // frame_counter_ advances per detectContacts (:31)
     auto cs = detect(S, 0.0);
@@ -796,9 +832,76 @@ void build_manifolds(orc_system& S, const std::vector<Contact>& cs) {
   }
 }
 
+// Wall manifolds of the cylindrical tube (collideCapsuleInsideCylinder,
+// collision.cpp:197-241, for each dynamic capsule, main.cpp:4431-4447;
+// NscContactSolver::addWallContact, nsc_contact.cpp:190-235): for the two
+// end points and the centre of the axis, a contact where the capsule surface
+// passes the tube wall; appended after the pair manifolds, in body order.
+void add_wall_manifolds(orc_system& S) {
+  const rg_config& c = S.cfg;
+  if (!c.cylinder_enabled) return;
+  V3 ax = v3(c.cylinder_axis[0], c.cylinder_axis[1], c.cylinder_axis[2]);
+  ax = ax / length(ax);
+  const double R = c.cylinder_radius;
+  for (int i = 0; i < S.n; ++i) {
+    const Body& B = S.body[i];
+    if (!(B.inv_mass > 0.0)) continue;
+    V3 u = axis_y(S.q[i]);
+    u = u / length(u);
+    const V3 pts[3] = {S.x[i] - u * B.h, S.x[i], S.x[i] + u * B.h};
+    for (const V3& p : pts) {
+      V3 pp = p - ax * dot(p, ax);
+      double d = length(pp);
+      double pen = d + B.r - R;
+      if (pen <= 0.0) continue;
+      Manifold m;
+      m.a = m.b = i;
+      m.wall = true;
+      if (d > 1e-8) {
+        m.n = pp / d;
+      } else {
+        V3 arb = std::fabs(ax.x) < 0.9 ? v3(1, 0, 0) : v3(0, 1, 0);
+        V3 cr = cross(ax, arb);
+        m.n = cr / length(cr);
+      }
+      V3 point = p + m.n * (R - d);
+      m.phi = -pen;
+      tangent_basis(m.n, m.t1, m.t2);
+      m.ra = point - S.x[i];
+      m.rb = v3(0, 0, 0);
+      // computeDiagWall (nsc_contact.cpp:144-150)
+      auto gw = [&](V3 dir) {
+        V3 rd = cross(m.ra, dir);
+        return std::max(B.inv_mass + dot(rd, iinv_apply(S, i, rd)) + c.nsc_cfm, 1e-12);
+      };
+      m.g_n = gw(m.n);
+      m.g_t1 = gw(m.t1);
+      m.g_t2 = gw(m.t2);
+      m.invMA = B.inv_mass;
+      m.invMB = 0.0;
+      m.IA_n = iinv_apply(S, i, cross(m.ra, m.n));
+      m.IA_t1 = iinv_apply(S, i, cross(m.ra, m.t1));
+      m.IA_t2 = iinv_apply(S, i, cross(m.ra, m.t2));
+      m.IB_n = m.IB_t1 = m.IB_t2 = v3(0, 0, 0);
+      m.v_rel_pre = -(S.v[i] + cross(S.w[i], m.ra));
+      m.v_n_pre = dot(m.n, m.v_rel_pre);
+      m.restitution = B.restitution;
+      S.manifolds.push_back(m);
+    }
+  }
+}
+
+// Relative contact velocity v_B - v_A; the wall is at rest (b unused).
+inline V3 rel_vel(const orc_system& S, const Manifold& m) {
+  V3 va = S.v[m.a] + cross(S.w[m.a], m.ra);
+  if (m.wall) return -va;
+  return (S.v[m.b] + cross(S.w[m.b], m.rb)) - va;
+}
+
 void apply_impulse(orc_system& S, const Manifold& m, V3 d, V3 IA, V3 IB, double l) {
   S.v[m.a] -= d * (l * m.invMA);
   S.w[m.a] -= IA * l;
+  if (m.wall) return;
   S.v[m.b] += d * (l * m.invMB);
   S.w[m.b] += IB * l;
 }
@@ -825,7 +928,7 @@ void solve_velocities(orc_system& S, const std::vector<int>& ord) {
     double res = 0;
     for (int idx : ord) {
       Manifold& m = S.manifolds[idx];
-      V3 vrel = (S.v[m.b] + cross(S.w[m.b], m.rb)) - (S.v[m.a] + cross(S.w[m.a], m.ra));
+      V3 vrel = rel_vel(S, m);
       double bn = m.phi < 0.0 ? beta * m.phi / dt : 0.0;
       double brest = m.v_n_pre < 0.0 ? m.restitution * m.v_n_pre : 0.0;
       double wn = dot(m.n, vrel) + bn + brest + cfm * m.ln;
@@ -838,10 +941,12 @@ void solve_velocities(orc_system& S, const std::vector<int>& ord) {
         S.v[m.a] -= dvA;
         S.w[m.a] -= m.IA_n * dn;
         vrel += dvA + cross(m.IA_n * dn, m.ra);
-        V3 dvB = m.n * (dn * m.invMB);
-        S.v[m.b] += dvB;
-        S.w[m.b] += m.IB_n * dn;
-        vrel += dvB + cross(m.IB_n * dn, m.rb);
+        if (!m.wall) {
+          V3 dvB = m.n * (dn * m.invMB);
+          S.v[m.b] += dvB;
+          S.w[m.b] += m.IB_n * dn;
+          vrel += dvB + cross(m.IB_n * dn, m.rb);
+        }
       }
       double mf = mu * m.ln;
       double lim1 = std::sqrt(std::max(0.0, mf * mf - m.lt2 * m.lt2));
@@ -855,10 +960,12 @@ void solve_velocities(orc_system& S, const std::vector<int>& ord) {
         S.v[m.a] -= dvA;
         S.w[m.a] -= m.IA_t1 * d1;
         vrel += dvA + cross(m.IA_t1 * d1, m.ra);
-        V3 dvB = m.t1 * (d1 * m.invMB);
-        S.v[m.b] += dvB;
-        S.w[m.b] += m.IB_t1 * d1;
-        vrel += dvB + cross(m.IB_t1 * d1, m.rb);
+        if (!m.wall) {
+          V3 dvB = m.t1 * (d1 * m.invMB);
+          S.v[m.b] += dvB;
+          S.w[m.b] += m.IB_t1 * d1;
+          vrel += dvB + cross(m.IB_t1 * d1, m.rb);
+        }
       }
       double lim2 = std::sqrt(std::max(0.0, mf * mf - m.lt1 * m.lt1));
       double w2 = dot(m.t2, vrel) + cfm * m.lt2;
@@ -869,8 +976,10 @@ void solve_velocities(orc_system& S, const std::vector<int>& ord) {
       if (d2 != 0.0) {
         S.v[m.a] -= m.t2 * (d2 * m.invMA);
         S.w[m.a] -= m.IA_t2 * d2;
-        S.v[m.b] += m.t2 * (d2 * m.invMB);
-        S.w[m.b] += m.IB_t2 * d2;
+        if (!m.wall) {
+          S.v[m.b] += m.t2 * (d2 * m.invMB);
+          S.w[m.b] += m.IB_t2 * d2;
+        }
       }
       res = std::max(res, std::fabs(dn) + std::fabs(d1) + std::fabs(d2));
     }
@@ -882,7 +991,10 @@ void solve_velocities(orc_system& S, const std::vector<int>& ord) {
   S.last_sweeps = sweeps;
   S.warm.clear();
   if (c.nsc_warm_start == RG_WARM_CACHE) {
-    for (const Manifold& m : S.manifolds) S.warm[pair_key(m.a, m.b)] = v3(m.ln, m.lt1, m.lt2);
+    // wall manifolds start cold every step (addWallContact, nsc_contact.cpp:
+    // 226-228): their (a, a) entries would never be read, so none is kept
+    for (const Manifold& m : S.manifolds)
+      if (!m.wall) S.warm[pair_key(m.a, m.b)] = v3(m.ln, m.lt1, m.lt2);
   }
 }
 
@@ -1007,20 +1119,22 @@ void nsc_step(orc_system& S) {
     V3 gyro = cross(S.w[i], Iw_w);
     S.w[i] += iinv_apply(S, i, S.tau[i] - gyro) * dt;
   }
-  // 2) detection + manifolds
+  // 2) detection + manifolds (pairs, then cylinder walls, main.cpp:4431-4447)
   auto cs = detect(S, 0.0);
-  S.last_contacts = (int64_t)cs.size();
   build_manifolds(S, cs);
-  std::vector<int> ca(cs.size()), cb(cs.size()), col;
-  for (size_t i = 0; i < cs.size(); ++i) { ca[i] = cs[i].a; cb[i] = cs[i].b; }
+  add_wall_manifolds(S);
+  const size_t M = S.manifolds.size();
+  S.last_contacts = (int64_t)M;  // getNumContacts counts the wall manifolds
+  std::vector<int> ca(M), cb(M), col;
+  for (size_t i = 0; i < M; ++i) { ca[i] = S.manifolds[i].a; cb[i] = S.manifolds[i].b; }
   S.last_colors = jp_color(S, ca, cb, col);
-  for (size_t i = 0; i < cs.size(); ++i) S.manifolds[i].color = col[i];
+  for (size_t i = 0; i < M; ++i) S.manifolds[i].color = col[i];
   int64_t coll = 0;
   for (const Manifold& m : S.manifolds)
     if (m.v_n_pre < -1e-6) ++coll;
   S.last_collisions = coll;
   // 3) velocity PSOR
-  solve_velocities(S, visit_order((int)cs.size(), col, colored));
+  solve_velocities(S, visit_order((int)M, col, colored));
   // impulse sums of the profile CSV (main.cpp:3339-3343); collisions above
   // are NscContactSolver::countImpacts (nsc_contact.hpp:112-117)
   S.jn_sum = 0; S.jt_sum = 0;
@@ -1041,6 +1155,14 @@ void nsc_step(orc_system& S) {
     double wl = length(S.w[i]);
     if (wl > c.w_max) S.w[i] = S.w[i] * (c.w_max / wl);
   }
+  // 4b) inside the tube, spin about the rod axis is projected out
+  // (main.cpp:4486-4494)
+  if (c.cylinder_enabled)
+    for (int i = 0; i < S.n; ++i) {
+      V3 u = axis_y(S.q[i]);
+      u = u / length(u);
+      S.w[i] = S.w[i] - u * dot(S.w[i], u);
+    }
   // 5) position projection
   project_positions(S, colored);
   // 6) PBC wrap (main.cpp:4508-4517)
@@ -1185,18 +1307,49 @@ int orc_detect(orc_system* S, double delta, int32_t* pairs, double* geom, double
   return cs.size() > cap ? RG_ERR_CAPACITY : RG_OK;
 }
 
+// Pair manifolds of the last velocity solve (the wall manifolds follow them
+// and are left out, as from the warm cache).
+static size_t pair_manifolds(const orc_system* S) {
+  size_t k = 0;
+  while (k < S->manifolds.size() && !S->manifolds[k].wall) ++k;
+  return k;
+}
+
 int orc_get_impulses(const orc_system* S, int32_t* pairs, double* lambda, int32_t* color,
                      size_t cap, size_t* n) {
   if (!S || !n) return RG_ERR_ARG;
-  *n = S->manifolds.size();
-  size_t m = std::min(cap, S->manifolds.size());
+  const size_t P = pair_manifolds(S);
+  *n = P;
+  size_t m = std::min(cap, P);
   for (size_t i = 0; i < m; ++i) {
     const Manifold& mf = S->manifolds[i];
     if (pairs) { pairs[2 * i] = mf.a; pairs[2 * i + 1] = mf.b; }
     if (lambda) { lambda[3 * i] = mf.ln; lambda[3 * i + 1] = mf.lt1; lambda[3 * i + 2] = mf.lt2; }
     if (color) color[i] = mf.color;
   }
-  return S->manifolds.size() > cap ? RG_ERR_CAPACITY : RG_OK;
+  return P > cap ? RG_ERR_CAPACITY : RG_OK;
+}
+
+// The wall manifolds of the last velocity solve: body, contact point
+// x_a + r_a, normal, phi, impulses, colour.
+int orc_get_wall_contacts(const orc_system* S, int32_t* body, double* rows, int32_t* color, size_t cap,
+                          size_t* n) {
+  if (!S || !n) return RG_ERR_ARG;
+  const size_t P = pair_manifolds(S), W = S->manifolds.size() - P;
+  *n = W;
+  for (size_t i = 0; i < W && i < cap; ++i) {
+    const Manifold& m = S->manifolds[P + i];
+    if (body) body[i] = m.a;
+    if (rows) {
+      double* o = rows + 10 * i;
+      V3 pt = S->x[m.a] + m.ra;
+      o[0] = pt.x; o[1] = pt.y; o[2] = pt.z;
+      o[3] = m.n.x; o[4] = m.n.y; o[5] = m.n.z;
+      o[6] = m.phi; o[7] = m.ln; o[8] = m.lt1; o[9] = m.lt2;
+    }
+    if (color) color[i] = m.color;
+  }
+  return W > cap ? RG_ERR_CAPACITY : RG_OK;
 }
 
 // Network rows of the last velocity solve (App::logNetworkFrame NSC branch,
@@ -1204,7 +1357,7 @@ int orc_get_impulses(const orc_system* S, int32_t* pairs, double* lambda, int32_
 // current state; phi, impulses and v_n_pre from the manifold.
 int orc_get_contact_network(const orc_system* S, int32_t* pairs, double* rows, size_t cap, size_t* n) {
   if (!S || !n) return RG_ERR_ARG;
-  const size_t m = S->manifolds.size();
+  const size_t m = pair_manifolds(S);  // rod-rod pairs only (walls skipped, main.cpp:3668)
   *n = m;
   for (size_t i = 0; i < m && i < cap; ++i) {
     const Manifold& M = S->manifolds[i];

@@ -33,4 +33,6 @@ extern "C" void rg_config_default(rg_config* c) {
   c->psor_order = RG_ORDER_COLORED;
   c->skin = 0.0; c->max_neighbors = 0;
   c->spin_limit = 0; c->test_absent_blocks = 0;
+  c->cylinder_enabled = 0; c->cylinder_radius = 0.3;  // CylinderCfg (config.hpp:150-154)
+  c->cylinder_axis[0] = 0; c->cylinder_axis[1] = 1; c->cylinder_axis[2] = 0;
 }

@@ -33,7 +33,8 @@ class RgConfig(ctypes.Structure):
         ("nsc_position_iters", _i), ("nsc_position_psor_iters", _i), ("nsc_warm_start", _i),
         ("psor_order", _i), ("skin", _d), ("max_neighbors", _i), ("team_blocks", _i),
         ("nsc_mlp_scope", _i), ("nsc_mlp_min_sweeps", _i), ("near_skin_pct", _i),
-        ("spin_limit", _i), ("test_absent_blocks", _i), ("reserved", _i * 1),
+        ("spin_limit", _i), ("test_absent_blocks", _i), ("cylinder_enabled", _i), ("cylinder_radius", _d),
+        ("cylinder_axis", _d * 3),
     ]
 
 
@@ -67,7 +68,7 @@ def apply_config(c, **kw):
             v = FRICTION[v]
         if k == "nsc_warm_start" and isinstance(v, str):
             v = WARM[v]
-        if k in ("gravity", "pbc_min", "pbc_max"):
+        if k in ("gravity", "pbc_min", "pbc_max", "cylinder_axis"):
             arr = getattr(c, k)
             for j in range(3):
                 arr[j] = float(v[j])

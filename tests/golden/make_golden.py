@@ -15,9 +15,12 @@ stores inputs and outputs as .npz next to this script:
   hm_5steps.npz     five Verlet steps of Hertz-Mindlin on capsules (the
                     harness's FP32 restatement; the reference's HM is
                     sphere-only)
+  nsc_tube_5steps.npz, soft_tube_5steps.npz
+                    five steps of rods in a cylindrical tube (wall
+                    manifolds, spin projection; the soft wall spring)
 
 Usage (in a tree where the reference is mounted):
-  python tests/golden/make_golden.py
+  python tests/golden/make_golden.py [case ...]
 """
 import os
 import sys
@@ -32,7 +35,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 import oracle  # noqa: E402
 import rodgpu  # noqa: E402
-from helpers import packed_scene  # noqa: E402
+from helpers import packed_scene, tube_config, tube_scene  # noqa: E402
 from rodgpu import scene  # noqa: E402
 
 CASES = {
@@ -47,10 +50,19 @@ CASES = {
     "hm_5steps": dict(n=300, d=0.1, phi=0.10, seed=8, steps=5, model="hertz-mindlin",
                       cfg=dict(dt=1e-4, hm_youngs_modulus=1e5, hm_poisson_ratio=0.3, hm_restitution=0.5,
                                hm_friction=0.5)),
+    # rods in a cylindrical tube (radius 0.3 about +y): wall manifolds and the
+    # spin projection of the NSC step, the soft wall spring of the Verlet step
+    "nsc_tube_5steps": dict(n=80, tube=True, seed=9, steps=5, model="nsc",
+                            cfg=dict(dt=5e-4, nsc_mu=0.3, nsc_tol=1e-6, nsc_velocity_iters=500, psor_order=1)),
+    "soft_tube_5steps": dict(n=40, tube=True, seed=10, steps=5, model="harmonic",
+                             tube_kw=dict(tilt=0.3, spacing=1.6, overshoot=0.02),
+                             cfg=dict(dt=1e-4, soft_delta=0.005, soft_k_scaler=1000.0, soft_damping=0.5)),
 }
 
 
 def case_config(c, sc):
+    if c.get("tube"):
+        return tube_config(sc, model=c["model"], **c.get("cfg", {}))
     kw = dict(gravity=(0.0, 0.0, 0.0), lin_damp=0.0, ang_damp=0.0, model=c["model"])
     kw.update(scene.pbc_kwargs(sc))
     kw.update(c.get("cfg", {}))
@@ -58,7 +70,10 @@ def case_config(c, sc):
 
 
 def inputs(c):
-    sc = packed_scene(c["n"], d=c["d"], phi=c["phi"], seed=c["seed"], squeeze=0.9)
+    if c.get("tube"):
+        sc = tube_scene(c["n"], seed=c["seed"], **c.get("tube_kw", {}))
+    else:
+        sc = packed_scene(c["n"], d=c["d"], phi=c["phi"], seed=c["seed"], squeeze=0.9)
     cfg = case_config(c, sc)
     return sc, cfg
 
@@ -89,10 +104,12 @@ def soft_inputs(c, margin=5e-5):
     raise RuntimeError("no seed keeps the soft contacts clear of d = h - delta")
 
 
-def main():
+def main(names=None):
     oracle.build(ref=True)
     for name, c in CASES.items():
-        if c["model"] == "harmonic" and "steps" in c:
+        if names and name not in names:
+            continue
+        if c["model"] == "harmonic" and "steps" in c and not c.get("tube"):
             sc, cfg, seed = soft_inputs(c)
             print(name, "seed", seed)
         else:
@@ -102,6 +119,8 @@ def main():
         r.set_state(sc["x"], sc["q"], sc["v"], sc["w"])
         out = dict(x=sc["x"], q=sc["q"], v=sc["v"], w=sc["w"], radius=sc["radius"],
                    half_height=sc["half_height"], restitution=sc["restitution"], lo=sc["lo"], side=sc["side"])
+        if c.get("tube"):
+            out.update(box_min=np.array(sc["box_min"]), box_max=np.array(sc["box_max"]), tube=sc["tube"])
         m, inertia = r.mass()
         out.update(mass=m, inertia=inertia)
         if name.startswith("detect"):
@@ -121,4 +140,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])  # optional case names (default: every case)

@@ -30,7 +30,7 @@ def test_library_exports_all_declared_symbols():
 
 def test_config_layout_and_defaults():
     L = rodgpu.lib()
-    assert L.rg_abi_version() == 1
+    assert L.rg_abi_version() == 2
     c = rodgpu.default_config()
     # NscContactCfg / SoftContactCfg defaults (include/config/config.hpp:6-88)
     assert c.nsc_velocity_iters == 40 and abs(c.nsc_beta - 0.2) < 1e-15

@@ -50,7 +50,8 @@ def test_pairs_match_reference(name):
     assert np.max(np.abs(geom[:, 9] - f["dist"])) < 1e-6  # reference distances are FP32
 
 
-@pytest.mark.parametrize("name", ["nsc_1step", "nsc_5steps", "soft_5steps", "hm_5steps"])
+@pytest.mark.parametrize("name", ["nsc_1step", "nsc_5steps", "soft_5steps", "hm_5steps", "nsc_tube_5steps",
+                                  "soft_tube_5steps"])
 def test_steps_match_reference(name):
     f, o, cfg = _fixture(name)
     o.step(int(f["steps"]))
@@ -61,10 +62,18 @@ def test_steps_match_reference(name):
         ref = f[k + "_out"]
         assert np.max(np.abs(s[k] - ref)) < 2e-4 * np.max(np.abs(ref)), k
     if "imp_lam" in f.files:
-        pairs, lam, _ = o.impulses()
-        assert np.array_equal(pairs, f["imp_pairs"])
+        # the reference lists wall manifolds (body a against the tube, shown
+        # as (a, a)) after the pair manifolds; the oracle reports them apart
+        wall = f["imp_pairs"][:, 0] == f["imp_pairs"][:, 1]
         scale = max(np.max(np.abs(f["imp_lam"])), 1e-12)
-        assert np.max(np.abs(lam - f["imp_lam"])) <= 1e-3 * scale + 1e-12
+        pairs, lam, _ = o.impulses()
+        assert np.array_equal(pairs, f["imp_pairs"][~wall])
+        assert np.max(np.abs(lam - f["imp_lam"][~wall]), initial=0.0) <= 1e-3 * scale + 1e-12
+        body, rows, _ = o.wall_contacts()
+        assert np.array_equal(body, f["imp_pairs"][wall, 0])
+        assert np.max(np.abs(rows[:, 7:10] - f["imp_lam"][wall]), initial=0.0) <= 1e-3 * scale + 1e-12
+        if name.startswith("nsc_tube"):
+            assert wall.sum() > 10 and (~wall).sum() > 0
 
 
 def test_known_nsc_elastic_exchange():
