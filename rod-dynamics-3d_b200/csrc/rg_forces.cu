@@ -410,6 +410,42 @@ __global__ void k_body_reduce(State st, const int* off, const int* ent, const do
 }
 
 // Deterministic potential-energy sum: fixed-shape two-level reduction.
+// Cylinder wall of the soft model (main.cpp:4661-4690 at phase t, :4756-4787
+// at phase t + dt): a penalty spring on the centre's radial overshoot past
+// R - r plus smooth Coulomb friction (tanh of |v_t| / nu); force only.
+__global__ void k_soft_wall(State st, rg_config cfg, const Ctl* ctl) {
+  if (ctl->err) return;
+  d3 ax{cfg.cylinder_axis[0], cfg.cylinder_axis[1], cfg.cylinder_axis[2]};
+  ax = ax / len(ax);
+  const double k = cfg.soft_k_scaler, cd = cfg.soft_damping, mu = cfg.soft_mu;
+  const double nu = smax(cfg.soft_nu, 1e-10);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
+    if (!(st.inv_mass[i] > 0.0)) continue;
+    const double maxd = cfg.cylinder_radius - st.r[i];
+    const d3 x = st.x.ld(i);
+    const d3 pp = x - ax * dot(x, ax);
+    const double d = len(pp);
+    const double pen = d - maxd;
+    if (pen <= 0.0) continue;
+    d3 n;
+    if (d > 1e-8) {
+      n = pp / d;
+    } else {
+      const d3 cr = cross(ax, fabs(ax.x) < 0.9 ? mk3(1, 0, 0) : mk3(0, 1, 0));
+      n = cr / len(cr);
+    }
+    const d3 v = st.v.ld(i);
+    const double vn = dot(v, n);
+    const double fn = k * pen + cd * smax(vn, 0.0);
+    d3 f = st.f.ld(i);
+    f = f - n * fn;
+    const d3 vt = v - n * vn;
+    const double vtl = len(vt);
+    if (vtl > 1e-12) f = f - vt * (mu * fn * tanh(vtl / nu) / vtl);
+    st.f.st(i, f);
+  }
+}
+
 constexpr int kPeBlocks = 64;
 __global__ void k_pe_partial(const double* pe, double* part, const Ctl* ctl) {
   if (ctl->err) return;
@@ -474,6 +510,7 @@ void force_eval_launch(rg_system* s) {
   // reduction into bodies
   RGL k_body_reduce<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, s->csr.off, s->csr.ent, s->d_cf, s->ccap,
                                                    s->d_ctl);
+  if (!hm && c.cylinder_enabled) RGL k_soft_wall<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, c, s->d_ctl);
   double* part = s->d_cf + 13 * (size_t)s->ccap;
   RGL k_pe_partial<<<kPeBlocks, 256, 0, st>>>(io.pe, part, s->d_ctl);
   RGL k_pe_final<<<1, 64, 0, st>>>(part, s->d_ctl);

@@ -939,7 +939,7 @@ __device__ __noinline__ int small_color(const NscView& V, int C, SmallSmem& S) {
 }
 
 // Colouring, manifold rows, PSOR and the warm cache for C <= kSmallC.
-__device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, PhaseClock& pc) {
+__device__ __noinline__ bool small_solve(const NscView& V, int C, int Cp, SmallSmem& S, PhaseClock& pc) {
   Ctl* ctl = V.ctl;
   const rg_config& cfg = V.cfg;
   const int t = threadIdx.x;
@@ -978,7 +978,7 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
                              kSmallC);
     coll = br & 1;
     S.cached[t] = (unsigned char)(br >> 1);
-    if (V.feat_on) {
+    if (V.feat_on && c < Cp) {  // wall rows (after the pairs) have no graph degree
       if (S.dyn[S.la[c]]) atomicAdd(&deg[S.la[c]], 1);
       if (S.dyn[S.lb[c]]) atomicAdd(&deg[S.lb[c]], 1);
     }
@@ -994,7 +994,7 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
     if (mlp_gate) {
       // the contacts the learned start is for (every contact, or those new
       // since the last step); the network runs only on tiles that hold one
-      const bool want = t < C && (V.mlp_all || !S.cached[t]);
+      const bool want = t < C && S.order[t] < Cp && (V.mlp_all || !S.cached[t]);  // never a wall row
       if (t < kSmallC / 16) S.mtile[t] = 0;
       __syncthreads();
       if (want) S.mtile[t >> 4] = 1;
@@ -1082,12 +1082,14 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
   double jn = 0, jt = 0;
   if (p < C) {
     double l0 = S.lam[p], l1 = S.lam[kSmallC + p], l2 = S.lam[2 * kSmallC + p];
-    V.wkey[c] = ((unsigned long long)(unsigned)V.con.a[c] << 32) | (unsigned)V.con.b[c];
-    V.wlam[c] = l0;
-    V.wlam[V.wcap + c] = l1;
-    V.wlam[2 * V.wcap + c] = l2;
-    reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = S.color[c];
-    if (V.xrow) export_row(V.xrow, V.wcap, c, R, p);
+    if (c < Cp) {  // wall rows start cold every step: they stay out of the cache
+      V.wkey[c] = ((unsigned long long)(unsigned)V.con.a[c] << 32) | (unsigned)V.con.b[c];
+      V.wlam[c] = l0;
+      V.wlam[V.wcap + c] = l1;
+      V.wlam[2 * V.wcap + c] = l2;
+      reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = S.color[c];
+      if (V.xrow) export_row(V.xrow, V.wcap, c, R, p);
+    }
     jn = fabs(l0);  // profile-CSV sums of main.cpp:3339-3343
     jt = fabs(l1) + fabs(l2);
   }
@@ -1098,7 +1100,7 @@ __device__ __noinline__ bool small_solve(const NscView& V, int C, SmallSmem& S, 
     atomicAdd(&ctl->jt_sum, jt);
   }
   if (t == 0) {
-    *V.wn = C;
+    *V.wn = Cp;
     ctl->vel_contacts = C;
     ctl->residual = res;
     ctl->sweeps_last = sweeps;
@@ -1227,6 +1229,87 @@ __device__ __noinline__ bool small_project(const NscView& V, int C, SmallSmem& S
 }
 
 // ---------------------------------------------------------------------------
+// Cylinder walls of the velocity solve: for every dynamic capsule, contacts
+// where its surface passes the tube wall at the two end points or the centre
+// of its axis (collideCapsuleInsideCylinder, collision.cpp:197-241), in body
+// order then sample order, appended after the Cp pair contacts as rows with
+// b == a (main.cpp:4431-4447).  The team's first block lists them (block
+// scan per round of rods); returns the total contact count.
+// ---------------------------------------------------------------------------
+__device__ inline int wall_hits(const NscView& V, int i, d3 ax, double R, d3* pt, d3* nrm, double* pen) {
+  const State& st = V.st;
+  if (!(st.inv_mass[i] > 0.0)) return 0;
+  const double h = st.h[i], r = st.r[i];
+  const d3 x = st.x.ld(i);
+  d3 u = axis_y(st.q.ld(i));
+  u = u / len(u);
+  const d3 smp[3] = {x - u * h, x, x + u * h};
+  int k = 0;
+  for (int j = 0; j < 3; ++j) {
+    const d3 p = smp[j];
+    const d3 pp = p - ax * dot(p, ax);
+    const double d = len(pp);
+    const double pe = d + r - R;
+    if (pe <= 0.0) continue;
+    d3 nv;
+    if (d > 1e-8) {
+      nv = pp / d;
+    } else {
+      const d3 cr = cross(ax, fabs(ax.x) < 0.9 ? mk3(1, 0, 0) : mk3(0, 1, 0));
+      nv = cr / len(cr);
+    }
+    if (pt) {
+      pt[k] = p + nv * (R - d);
+      nrm[k] = nv;
+      pen[k] = pe;
+    }
+    ++k;
+  }
+  return k;
+}
+
+__device__ __noinline__ int wall_phase(const Team& T, const NscView& V, int Cp, SmemNsc& sm) {
+  Ctl* ctl = V.ctl;
+  const int n = V.st.n;
+  const rg_config& cfg = V.cfg;
+  if (T.rank() == 0) {
+    d3 ax{cfg.cylinder_axis[0], cfg.cylinder_axis[1], cfg.cylinder_axis[2]};
+    ax = ax / len(ax);
+    const double R = cfg.cylinder_radius;
+    int run = Cp;
+    for (int base = 0; base < n; base += blockDim.x) {
+      const int i = base + threadIdx.x;
+      d3 pt[3], nv[3];
+      double pe[3];
+      const int k = i < n ? wall_hits(V, i, ax, R, pt, nv, pe) : 0;
+      int tot;
+      const int ex = block_excl_scan(k, sm.scan_w, tot);
+      for (int j = 0; j < k; ++j) {
+        const int c = run + ex + j;
+        if (c >= V.ccap) break;
+        V.con.a[c] = i;
+        V.con.b[c] = i;
+        V.con.type[c] = 3;  // wall
+        V.con.comp(0)[c] = pt[j].x; V.con.comp(1)[c] = pt[j].y; V.con.comp(2)[c] = pt[j].z;
+        V.con.comp(3)[c] = pt[j].x; V.con.comp(4)[c] = pt[j].y; V.con.comp(5)[c] = pt[j].z;
+        V.con.comp(6)[c] = nv[j].x; V.con.comp(7)[c] = nv[j].y; V.con.comp(8)[c] = nv[j].z;
+        V.con.comp(9)[c] = 0.0; V.con.comp(10)[c] = 0.0; V.con.comp(11)[c] = 0.0;
+        V.con.comp(12)[c] = -pe[j];  // phi = comp12 - comp13 = -penetration
+        V.con.comp(13)[c] = 0.0;
+      }
+      run += tot;
+    }
+    if (threadIdx.x == 0) {
+      if (run > V.ccap) atomicOr(&ctl->err, ERR_CONTACT_CAP);
+      ctl->contacts = run;
+    }
+  }
+  if (!team_sync(T)) return -1;
+  const int C = *(volatile int*)&ctl->contacts;
+  return C > V.ccap ? -1 : C;
+}
+
+// ---------------------------------------------------------------------------
 // One NSC step of one system by one team.
 // ---------------------------------------------------------------------------
 __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem& S) {
@@ -1265,8 +1348,10 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     if (!team_sync(T)) return false;
   }
   pc.mark(0);
-  // 2) detection, colouring, manifold rows
-  int C = detect_phase(T, V, 0.0, sm, false);
+  // 2) detection (pairs, then cylinder walls), colouring, manifold rows
+  const int Cp = detect_phase(T, V, 0.0, sm, false);
+  if (Cp < 0) return false;
+  const int C = cfg.cylinder_enabled ? wall_phase(T, V, Cp, sm) : Cp;
   if (C < 0) return false;
   pc.mark(1);
   const bool small = C <= kSmallC;
@@ -1274,7 +1359,7 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     // colouring, rows, PSOR and warm cache in one block, on chip
     bool ok = true;
     const unsigned long long ts = (rank == 0 && threadIdx.x == 0) ? gtimer() : 0ull;
-    if (rank == 0) ok = small_solve(V, C, S, pc);
+    if (rank == 0) ok = small_solve(V, C, Cp, S, pc);
     if (rank == 0 && threadIdx.x == 0) ctl->serial_ns += (long long)(gtimer() - ts);
     if (!ok) atomicOr(&ctl->err, ERR_COLOR);
     pc.mark(10);
@@ -1299,7 +1384,7 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     for (int p = tid; p < C; p += TS) {
       const int c = V.order[p];
       coll += build_row(st, V.con, cfg, c, p, R, V.wkey, V.wlam, W, V.wcap, V.feat_on ? V.feat : nullptr, V.ccap) & 1;
-      if (V.feat_on) {
+      if (V.feat_on && c < Cp) {  // wall rows have no graph degree
         if (im[V.con.a[c]] > 0.0) atomicAdd(&deg[V.con.a[c]], 1);
         if (im[V.con.b[c]] > 0.0) atomicAdd(&deg[V.con.b[c]], 1);
       }
@@ -1331,7 +1416,8 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
         const int lane = threadIdx.x & 31, gw = tid >> 5, nw = TS >> 5;
         for (int row0 = gw * 16; row0 < C; row0 += nw * 16) {
           const int p = row0 + (lane & 15);
-          const bool want = lane < 16 && p < C && (V.mlp_all || !warm_cached(V, V.order[p], W));
+          const bool want = lane < 16 && p < C && V.order[p] < Cp &&  // never a wall row
+                            (V.mlp_all || !warm_cached(V, V.order[p], W));
           if (!__ballot_sync(0xffffffffu, want)) continue;  // no row of this tile needs the network
           unsigned a[8][4];
           mlp_layer1(ms.w1, kW1Ld, q, V.feat, V.ccap, row0, C, lane, a);
@@ -1358,12 +1444,14 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     for (int p = tid; !small && p < C; p += TS) {
       int c = V.order[p];
       double l0 = R.lam[p], l1 = R.lam[R.ccap + p], l2 = R.lam[2 * R.ccap + p];
-      V.wkey[c] = ((unsigned long long)(unsigned)V.con.a[c] << 32) | (unsigned)V.con.b[c];
-      V.wlam[c] = l0;
-      V.wlam[V.wcap + c] = l1;
-      V.wlam[2 * V.wcap + c] = l2;
-      reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = V.color[c];
-      if (V.xrow) export_row(V.xrow, V.wcap, c, R, p);
+      if (c < Cp) {  // wall rows start cold every step: they stay out of the cache
+        V.wkey[c] = ((unsigned long long)(unsigned)V.con.a[c] << 32) | (unsigned)V.con.b[c];
+        V.wlam[c] = l0;
+        V.wlam[V.wcap + c] = l1;
+        V.wlam[2 * V.wcap + c] = l2;
+        reinterpret_cast<int*>(V.wlam + 3 * (size_t)V.wcap)[c] = V.color[c];
+        if (V.xrow) export_row(V.xrow, V.wcap, c, R, p);
+      }
       jn += fabs(l0);  // profile-CSV sums of main.cpp:3339-3343
       jt += fabs(l1) + fabs(l2);
     }
@@ -1374,7 +1462,7 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
       atomicAdd(&ctl->jt_sum, jt);
     }
     if (tid == 0 && !small) {
-      *V.wn = C;
+      *V.wn = Cp;
       ctl->vel_contacts = C;
     }
     int rec_base = 0;
@@ -1400,9 +1488,11 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
       const double* ref = V.ref;
       Seg* seg = V.seg;
       unsigned char* moved = V.moved;
+      const bool spin = cfg.cylinder_enabled != 0;
       const Box box = V.box;
       for (int i = tid; i < n; i += TS)
-        bad |= position_update_fused(SB, i, dt, ld, ad, w_max, ref, ref2, box, invL, seg, dmax, dnear, moved);
+        bad |= position_update_fused(SB, i, dt, ld, ad, w_max, ref, ref2, box, invL, seg, dmax, dnear, moved,
+                                     spin);
     }
     if (bad) atomicOr(&ctl->err, ERR_NONFINITE);
     double bm = block_reduce_max(dmax, sm.red_d);

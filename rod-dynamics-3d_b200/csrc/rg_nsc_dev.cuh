@@ -58,6 +58,61 @@ __device__ inline int lower_bound_key(const unsigned long long* k, int n, unsign
   return lo;
 }
 
+// Wall row of contact c (body a against the tube, stored with b == a): the
+// manifold of NscContactSolver::addWallContact (nsc_contact.cpp:190-235):
+// r_b = 0, no mass or inertia on the wall side, computeDiagWall
+// (:144-150), v_rel = -(v_a + w_a x r_a), the body's own restitution, and a
+// cold start (wall manifolds are never warm-started).  Returns the impact
+// bit, with bit 1 set so the learned start leaves the row alone.
+__device__ inline int build_wall_row(const State& st, const Contacts& con, const rg_config& cfg, int c, int p,
+                                     const RowIO& R, double beta, float* feat, int fld) {
+  const int a = con.a[c];
+  d3 pa{con.comp(0)[c], con.comp(1)[c], con.comp(2)[c]};
+  d3 n{con.comp(6)[c], con.comp(7)[c], con.comp(8)[c]};
+  double phi = con.comp(12)[c] - con.comp(13)[c];
+  d3 ref = fabs(n.x) < 0.9 ? mk3(1, 0, 0) : mk3(0, 1, 0);
+  d3 cr = cross(n, ref);
+  d3 t1 = cr / len(cr);
+  d3 t2 = cross(n, t1);
+  d3 ra = pa - st.x.ld(a);
+  const d3 zero{0, 0, 0};
+  R.w3(R_N, p, n); R.w3(R_T1, p, t1); R.w3(R_T2, p, t2);
+  R.w3(R_RA, p, ra); R.w3(R_RB, p, zero);
+  auto gw = [&](d3 d) {
+    d3 rd = cross(ra, d);
+    return smax(st.inv_mass[a] + dot(rd, iinv_apply(st, a, rd)) + cfg.nsc_cfm, 1e-12);
+  };
+  R.r(R_GN, p) = cfg.nsc_omega / gw(n);
+  R.r(R_GT1, p) = cfg.nsc_omega / gw(t1);
+  R.r(R_GT2, p) = cfg.nsc_omega / gw(t2);
+  R.r(R_IMA, p) = st.inv_mass[a];
+  R.r(R_IMB, p) = 0.0;
+  R.w3(R_IAN, p, iinv_apply(st, a, cross(ra, n)));
+  R.w3(R_IAT1, p, iinv_apply(st, a, cross(ra, t1)));
+  R.w3(R_IAT2, p, iinv_apply(st, a, cross(ra, t2)));
+  R.w3(R_IBN, p, zero); R.w3(R_IBT1, p, zero); R.w3(R_IBT2, p, zero);
+  d3 vrel = -(st.v.ld(a) + cross(st.w.ld(a), ra));
+  double vnp = dot(n, vrel);
+  double e = st.rest[a];
+  R.r(R_BN, p) = phi < 0.0 ? beta * phi / cfg.dt : 0.0;
+  R.r(R_BREST, p) = vnp < 0.0 ? e * vnp : 0.0;
+  R.r(R_PHI, p) = phi;
+  R.r(R_VNPRE, p) = vnp;
+  R.lam[p] = 0.0;
+  R.lam[R.ccap + p] = 0.0;
+  R.lam[2 * R.ccap + p] = 0.0;
+  if (feat) {
+    feat[p] = (float)phi;
+    feat[fld + p] = (float)vnp;
+    feat[2 * fld + p] = (float)dot(t1, vrel);
+    feat[3 * fld + p] = (float)dot(t2, vrel);
+    feat[4 * fld + p] = 0.0f;
+    feat[5 * fld + p] = 0.0f;
+    feat[6 * fld + p] = 0.0f;
+  }
+  return (vnp < -1e-6 ? 1 : 0) | 2;
+}
+
 // Manifold row of contact c into slot p; returns 1 for an impact
 // (v_n_pre < -1e-6, NscContactSolver::countImpacts).  When feat is given,
 // the learned warm start's features 0-6 of slot p go to feat[k * fld + p]
@@ -67,6 +122,7 @@ __device__ inline int build_row(const State& st, const Contacts& con, const rg_c
                                 int wcap, float* feat = nullptr, int fld = 0) {
   const double beta = cfg.nsc_position_stabilization ? cfg.nsc_beta * 0.01 : cfg.nsc_beta;
   const int a = con.a[c], b = con.b[c];
+  if (a == b) return build_wall_row(st, con, cfg, c, p, R, beta, feat, fld);
   d3 pa{con.comp(0)[c], con.comp(1)[c], con.comp(2)[c]};
   d3 pb{con.comp(3)[c], con.comp(4)[c], con.comp(5)[c]};
   d3 n{con.comp(6)[c], con.comp(7)[c], con.comp(8)[c]};
@@ -153,10 +209,12 @@ struct Vel {
   Vec3A v, w;
 };
 
+// a == b: a wall row (the wall takes no impulse).
 __device__ inline void apply_imp(const Vel& V, int a, int b, d3 d, d3 IA, d3 IB, double ima, double imb,
                                  double l) {
   V.v.st(a, V.v.ld(a) - d * (l * ima));
   V.w.st(a, V.w.ld(a) - IA * l);
+  if (a == b) return;
   V.v.st(b, V.v.ld(b) + d * (l * imb));
   V.w.st(b, V.w.ld(b) + IB * l);
 }
@@ -181,8 +239,12 @@ __device__ inline double psor_row(const RowIO& R, const Vel& V, int p, int a, in
   d3 IBn = R.r3(R_IBN, p), IBt1 = R.r3(R_IBT1, p), IBt2 = R.r3(R_IBT2, p);
   double ima = R.r(R_IMA, p), imb = R.r(R_IMB, p);
   double ln = R.lam[p], lt1 = R.lam[R.ccap + p], lt2 = R.lam[2 * R.ccap + p];
-  d3 vA = V.v.ld(a), wA = V.w.ld(a), vB = V.v.ld(b), wB = V.w.ld(b);
-  d3 vrel = (vB + cross(wB, rb)) - (vA + cross(wA, ra));
+  // a == b: a wall row; the wall is at rest and takes no impulse (its
+  // B-side terms are zero, v_rel = -(v_a + w_a x r_a))
+  const bool wall = a == b;
+  const d3 zero{0, 0, 0};
+  d3 vA = V.v.ld(a), wA = V.w.ld(a), vB = wall ? zero : V.v.ld(b), wB = wall ? zero : V.w.ld(b);
+  d3 vrel = wall ? -(vA + cross(wA, ra)) : (vB + cross(wB, rb)) - (vA + cross(wA, ra));
   double wn = dot(n, vrel) + R.r(R_BN, p) + R.r(R_BREST, p) + cfm * ln;
   double dn_ = -R.r(R_GN, p) * wn;
   double old = ln;
@@ -229,7 +291,7 @@ __device__ inline double psor_row(const RowIO& R, const Vel& V, int p, int a, in
   }
   if (dn != 0.0 || d1 != 0.0 || d2 != 0.0) {
     V.v.st(a, vA); V.w.st(a, wA);
-    V.v.st(b, vB); V.w.st(b, wB);
+    if (!wall) { V.v.st(b, vB); V.w.st(b, wB); }
     R.lam[p] = ln; R.lam[R.ccap + p] = lt1; R.lam[2 * R.ccap + p] = lt2;
   }
   return fabs(dn) + fabs(d1) + fabs(d2);
@@ -335,7 +397,7 @@ __device__ inline void free_flight_fused(const StateBase& S, int i, d3 g, double
 __device__ inline int position_update_fused(const StateBase& S, int i, double dt, double ld, double ad,
                                             double w_max, const double* ref, const double* ref2, const Box& box,
                                             const double* invL, Seg* seg_out, double& dmax, double& dnear,
-                                            unsigned char* moved) {
+                                            unsigned char* moved, bool spin_project) {
   const int n = S.n;
   d3 v = S.ld3(7, i), w = S.ld3(10, i);
   d3 x = S.ld3(0, i);
@@ -354,6 +416,11 @@ __device__ inline int position_update_fused(const StateBase& S, int i, double dt
   w = w * ad;
   double wl = len(w);
   if (wl > w_max) w = w * (w_max / wl);
+  if (spin_project) {  // inside a tube: no spin about the rod axis (main.cpp:4486-4494)
+    d3 u = axis_y(q);
+    u = u / len(u);
+    w = w - u * dot(w, u);
+  }
   S.st3(0, i, x);
   S.c(3)[i] = q.w; S.c(4)[i] = q.x; S.c(5)[i] = q.y; S.c(6)[i] = q.z;
   S.st3(7, i, v);
