@@ -478,8 +478,9 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild) {
   const int g = grid_for(n, bs);
   const bool near = d.near_cnt != nullptr;
   RGL k_seg<<<g, bs, 0, st>>>(s->st, d.seg);
-  if (check_rebuild && !d.all_pairs)
+  if (check_rebuild && !d.all_pairs) {
     RGL k_disp_check<<<g, bs, 0, st>>>(s->st, d.seg, d.ref, near ? d.ref2 : nullptr, s->box, d.skin, ctl);
+  }
   // --- rebuild: every kernel below returns at once unless ctl->rebuild ---
   if (!s->box.pbc) {
     cudaMemsetAsync(dd->mn, 0xff, sizeof(dd->mn), st);

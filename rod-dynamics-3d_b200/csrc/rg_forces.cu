@@ -510,7 +510,9 @@ void force_eval_launch(rg_system* s) {
   // reduction into bodies
   RGL k_body_reduce<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, s->csr.off, s->csr.ent, s->d_cf, s->ccap,
                                                    s->d_ctl);
-  if (!hm && c.cylinder_enabled) RGL k_soft_wall<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, c, s->d_ctl);
+  if (!hm && c.cylinder_enabled) {
+    RGL k_soft_wall<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, c, s->d_ctl);
+  }
   double* part = s->d_cf + 13 * (size_t)s->ccap;
   RGL k_pe_partial<<<kPeBlocks, 256, 0, st>>>(io.pe, part, s->d_ctl);
   RGL k_pe_final<<<1, 64, 0, st>>>(part, s->d_ctl);

@@ -244,7 +244,9 @@ struct rg_system {
 namespace rg {
 // Kernel launches issued by this library (all systems), for run statistics.
 extern long long g_launches;
-#define RGL ++::rg::g_launches;
+// Counts the launch written after it; one expression (comma operator), so
+// `if (c) RGL k<<<...>>>(...)` guards the count and the launch together.
+#define RGL ++::rg::g_launches,
 
 enum Stage { ST_INTEGRATE = 0, ST_DETECT, ST_COLOR, ST_MANIFOLDS, ST_PSOR, ST_PROJECT, ST_FORCES, ST_OTHER };
 

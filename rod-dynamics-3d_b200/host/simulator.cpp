@@ -10,7 +10,8 @@
 // Scene keys read (src/config/config.cpp, include/config/config.hpp):
 //   physics: dt, gravity, lin_damp, ang_damp, w_max, contact_model,
 //            soft_contact{...}, hertz_mindlin{...}, nsc{...}
-//   scene:   periodic{enabled,min,max}, bodies[{pos, rot_quat (wxyz array,
+//   scene:   periodic{enabled,min,max}, cylinder{enabled,axis,radius},
+//            bodies[{pos, rot_quat (wxyz array,
 //            or object, rot_quat_order "xyzw"), rot_axis+rot_deg, shape,
 //            length, diameter|radius, density, restitution, is_static,
 //            v_lin, v_ang}], populate{count, seed, length, radius, density,
@@ -187,6 +188,16 @@ Simulator::Simulator(const std::string& scene_path, const std::string& init_csv_
     vec3_of(pb["min"], mn);
     vec3_of(pb["max"], mx);
     for (int k = 0; k < 3; ++k) { cfg_.pbc_min[k] = mn[k]; cfg_.pbc_max[k] = mx[k]; }
+  }
+
+  // ---- cylindrical tube boundary (config.cpp:517-525) ----
+  const Value& cy = sc["cylinder"];
+  if (cy["enabled"].boolean(false)) {
+    cfg_.cylinder_enabled = 1;
+    cfg_.cylinder_radius = cy["radius"].number(cfg_.cylinder_radius);
+    vec3_of(cy["axis"], cfg_.cylinder_axis);
+    if (cfg_.model == RG_MODEL_HERTZ_MINDLIN && !quiet_)
+      std::fprintf(stderr, "[rod_dynamics_py] scene.cylinder has no effect with hertz-mindlin (as in the reference)\n");
   }
 
   // ---- bodies: endpoint CSV, populate, or the explicit list ----
