@@ -283,6 +283,67 @@ def secondary_gpu_baseline(rodgpu, args, sizes=(10000, 50000, 100000)):
     return out
 
 
+def learned_line(rodgpu, args, train_runs=12, eval_runs=5, n=50000, steps=200, warm=100, chunk=12):
+    """The learned-warm-start configuration: N = 50,000 rods (L = 1,
+    d = 0.05, phi 0.10 - the isotropic RSA limit near phi*AR ~ 2.4 rules
+    out the stated 0.20 - device packings), mu ~ U[0.1, 0.8] per run.  The
+    network is trained by the library's kernels on the records of
+    train_runs plain-PSOR runs (steps recorded after `warm` unrecorded
+    steps, generated `chunk` runs at a time and merged through the record
+    file format), then each of eval_runs held-out seeds runs warm + steps
+    steps from the cache start and from the learned start (default scope
+    and gate).  Reported: PSOR sweeps, device time and steps stopped at the
+    sweep cap, in total and per held-out run."""
+    import tempfile
+    from rodgpu import records, scene
+    t0 = time.perf_counter()
+    parts = []
+    with tempfile.TemporaryDirectory() as tmp:
+        for c0 in range(0, train_runs, chunk):
+            path = os.path.join(tmp, f"records_{c0}.npz")
+            records.generate(min(chunk, train_runs - c0), steps, n=n, ar=20, phi=0.10, mu_range=(0.1, 0.8),
+                             seed=1000 + c0, warmup=warm, path=path)
+            parts.append(records.load(path))
+    ds = records.merge(parts)
+    t_rec = time.perf_counter() - t0
+    trainer = rodgpu.System(rodgpu.default_config(n_bodies=16, model="nsc"))
+    t0 = time.perf_counter()
+    loss = trainer.mlp_train(ds["features"], ds["targets"], epochs=20, batch=4096, lr=1e-3, seed=3)
+    t_train = time.perf_counter() - t0
+    params = trainer.mlp_get_params()
+    trainer.close()
+    per_run = []
+    for k in range(eval_runs):
+        rng = np.random.default_rng(50000 + k)
+        mu = float(rng.uniform(0.1, 0.8))
+        sc = scene.make_rods_device(n, 1.0, 0.05, phi=0.10, seed=70000 + k, max_attempts=20000)
+        row = {"mu": round(mu, 3)}
+        for mode in ("cache", "mlp"):
+            kw = dict(model="nsc", dt=5e-4, nsc_mu=mu, nsc_omega=1.0, nsc_tol=1e-6, nsc_velocity_iters=500,
+                      gravity=(0.0, 0.0, 0.0), lin_damp=0.0, ang_damp=0.0, nsc_warm_start=mode)
+            kw.update(scene.pbc_kwargs(sc))
+            s = load_system(rodgpu, rodgpu.default_config(n_bodies=sc["n"], **kw), sc)
+            if mode == "mlp":
+                s.mlp_set_params(params)
+            s.step(warm)
+            st = s.step(steps)
+            row[mode] = {"sweeps": int(st["psor_sweeps"]), "ms": round(st["device_ms"], 2),
+                         "capped_steps": int(st["not_converged"])}
+            s.close()
+        per_run.append(row)
+    tot = {m: {"sweeps": sum(r[m]["sweeps"] for r in per_run), "ms": round(sum(r[m]["ms"] for r in per_run), 2),
+               "capped_steps": sum(r[m]["capped_steps"] for r in per_run)} for m in ("cache", "mlp")}
+    ratio_sw = [r["mlp"]["sweeps"] / max(r["cache"]["sweeps"], 1) for r in per_run]
+    ratio_ms = [r["mlp"]["ms"] / max(r["cache"]["ms"], 1e-9) for r in per_run]
+    return {"rods": n, "train": {"runs": train_runs, "steps": steps, "warmup": warm, "records": int(len(ds["features"])),
+                                 "final_loss": round(loss, 4), "record_s": round(t_rec, 1), "train_s": round(t_train, 1)},
+            "held_out": {"runs": eval_runs, "steps": steps, "after_warmup": warm, "total": tot, "per_run": per_run,
+                         "sweeps_ratio_mean": round(float(np.mean(ratio_sw)), 3),
+                         "sweeps_ratio_range": [round(min(ratio_sw), 3), round(max(ratio_sw), 3)],
+                         "time_ratio_mean": round(float(np.mean(ratio_ms)), 3),
+                         "time_ratio_range": [round(min(ratio_ms), 3), round(max(ratio_ms), 3)]}}
+
+
 def train_network(rodgpu, args):
     """Records converged impulses of plain PSOR on separate seeded systems
     and trains the network with the library's kernels."""
@@ -401,6 +462,8 @@ def run_ours(args, rank, world):
         second = secondary_gpu_baseline(rodgpu, args)
     except Exception as e:  # noqa: BLE001
         second = {"unavailable": str(e)}
+    learned_n50k = {} if args.no_learned else learned_line(rodgpu, args, train_runs=args.learned_train_runs,
+                                                           eval_runs=args.learned_eval_runs)
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": "rod-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
@@ -424,6 +487,7 @@ def run_ours(args, rank, world):
         "roofline": roof,
         "hertz_mindlin": hm,
         "secondary_gpu_baseline": second,
+        "learned_warm_start_n50k": learned_n50k,
         "clocks": clk.summary(),
     }
     return out
@@ -480,6 +544,16 @@ def run_single(args, rank, world):
     import rodgpu
     import torch
     dev = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "learned_n50k":
+        r = learned_line(rodgpu, args, train_runs=args.learned_train_runs, eval_runs=args.learned_eval_runs)
+        tot = r["held_out"]["total"]
+        n_rs = r["rods"] * r["held_out"]["runs"] * r["held_out"]["steps"]
+        return {"metric": METRIC, "value": round(n_rs / (tot["mlp"]["ms"] / 1000.0), 1), "unit": "rod-steps/s",
+                "n_gpus": world, "steps": r["held_out"]["steps"], "warmup": r["held_out"]["after_warmup"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded device RSA packings)",
+                "config": {"workload": "learned_n50k: N=50000, AR 20, phi 0.10, mu U[0.1,0.8]"},
+                "plain_value": round(n_rs / (tot["cache"]["ms"] / 1000.0), 1), "detail": r}
     if args.workload in HM_LINES:
         with ClockSampler(dev) as clk:
             r = hm_line(rodgpu, args, args.workload, args.n)
@@ -606,6 +680,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-hm", action="store_true", help="skip the Hertz-Mindlin workloads")
     ap.add_argument("--hm-steps", type=int, default=0, help="timed steps of a Hertz-Mindlin workload (0: its own)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the N=50,000 learned-warm-start line")
+    ap.add_argument("--learned-train-runs", type=int, default=12)
+    ap.add_argument("--learned-eval-runs", type=int, default=5)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -387,7 +387,11 @@ __device__ __noinline__ int detect_near(const Team& T, const NscView& V, double 
   const int bsum = block_reduce_sum_i(mine, sm.red_i);
   if (threadIdx.x == 0) V.blk[rank] = bsum;
   if (!team_sync(T)) return -1;
-  if (rank == 0 && threadIdx.x == 0) ctl->maxdisp = 0.0;  // every block has read it
+  // every block has read maxdisp.  After a position-level pass it stays:
+  // the next free flight refreshes only the rods moved since, and the
+  // unmoved rods' bounds are the ones it holds (unless the lists were just
+  // rebuilt, when every bound restarts at zero).
+  if (rank == 0 && threadIdx.x == 0 && (!position_level || lists_rebuilt)) ctl->maxdisp = 0.0;
   block_prefix(V.blk, T.nb, rank, prefix, total, sm);
   if (total > V.ccap) {
     if (rank == 0 && threadIdx.x == 0) atomicOr(&ctl->err, ERR_CONTACT_CAP);
@@ -453,7 +457,8 @@ __device__ __noinline__ int detect_phase(const Team& T, const NscView& V, double
   int run = block_reduce_sum_i(mine, sm.red_i);
   if (threadIdx.x == 0) V.blk[rank] = run;
   if (!team_sync(T)) return -1;
-  if (rank == 0 && threadIdx.x == 0) ctl->maxdisp = 0.0;  // every block has read it
+  // every block has read maxdisp (kept after a position-level pass, as above)
+  if (rank == 0 && threadIdx.x == 0 && (!position_level || need)) ctl->maxdisp = 0.0;
   int prefix, total;
   block_prefix(V.blk, T.nb, rank, prefix, total, sm);
   if (total > V.ccap) {
@@ -1312,7 +1317,7 @@ __device__ __noinline__ int wall_phase(const Team& T, const NscView& V, int Cp, 
 // ---------------------------------------------------------------------------
 // One NSC step of one system by one team.
 // ---------------------------------------------------------------------------
-__device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem& S) {
+__device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem& S, bool first) {
   Ctl* ctl = V.ctl;
   const State& st = V.st;
   const rg_config& cfg = V.cfg;
@@ -1338,7 +1343,17 @@ __device__ bool nsc_step(const Team& T, const NscView& V, SmemNsc& sm, SmallSmem
     const double* ref = V.ref;
     Seg* seg = V.seg;
     const Box box = V.box;
-    for (int i = tid; i < n; i += TS) free_flight_fused(SB, i, g, dt, ref, ref2, box, invL, seg, dmax, dnear);
+    // Only the position update, the projection and the wrap move rods, and
+    // the last two flag what they move: other rods keep the segment record
+    // and displacement bounds of the position update (still folded into
+    // ctl->maxdisp / near_disp), and need their velocities only.  The first
+    // step of a launch refreshes every rod (the state may have been set
+    // from the host).
+    const unsigned char* moved = first ? nullptr : V.moved;
+    for (int i = tid; i < n; i += TS) {
+      if (moved && !moved[i]) free_flight_velocity(SB, i, g, dt);
+      else free_flight_fused(SB, i, g, dt, ref, ref2, box, invL, seg, dmax, dnear);
+    }
     double bm = block_reduce_max(dmax, sm.red_d);
     if (threadIdx.x == 0) atomic_max_nonneg(&ctl->maxdisp, bm);
     if (V.near) {
@@ -1569,7 +1584,7 @@ __global__ void __launch_bounds__(kBlock, 1) k_nsc_run(const NscView* views, con
              V.cfg.test_absent_blocks > 0 ? (unsigned)V.cfg.test_absent_blocks : 0u};
       const bool timer = threadIdx.x == 0 && (int)blockIdx.x == td.b0;
       const unsigned long long t0 = timer ? gtimer() : 0ull;
-      any |= nsc_step(T, V, sm, S);
+      any |= nsc_step(T, V, sm, S, s == 0);
       if (timer) V.ctl->member_ns += (long long)(gtimer() - t0);  // one writer per system
     }
     if (!any) break;

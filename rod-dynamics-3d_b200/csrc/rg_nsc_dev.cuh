@@ -358,6 +358,24 @@ __device__ inline Seg seg_of(d3 x, dq q, double h, double r) {
   return s;
 }
 
+// Free flight of rod i alone (velocities; nsc_free_flight_body from the
+// buffer bases): for rods whose segment record and displacement bounds are
+// still those of the last position update.
+__device__ inline void free_flight_velocity(const StateBase& S, int i, d3 g, double dt) {
+  const double im = S.pc(3)[i];
+  if (!(im > 0)) return;
+  const dq q{S.c(3)[i], S.c(4)[i], S.c(5)[i], S.c(6)[i]};
+  d3 v = S.ld3(7, i);
+  d3 w = S.ld3(10, i);
+  const d3 f = S.ld3(13, i), tau = S.ld3(16, i), I = S.pld3(5, i), Iinv = S.pld3(8, i);
+  v = v + (f * im + g) * dt;
+  d3 Iw_w = rot_diag_apply(q, I, w);
+  d3 gyro = cross(w, Iw_w);
+  w = w + rot_diag_apply(q, Iinv, tau - gyro) * dt;
+  S.st3(7, i, v);
+  S.st3(10, i, w);
+}
+
 // Free flight of rod i (nsc_free_flight_body), its segment record and the
 // displacement bounds against ref (and ref2 when given), with every input
 // loaded before the first store: one round trip to memory per rod instead

@@ -111,9 +111,9 @@ def test_learned_warm_start_saves_sweeps(trained):
             tot += r["psor_sweeps"]
         sweeps[warm] = tot
     print("sweeps per 81 steps:", sweeps, "records:", nrec, "train loss:", loss)
-    # the network beats a cold start and does not lose to the cache
+    # the network beats a cold start (its gain over the cache start is
+    # tested at scale on held-out systems below)
     assert sweeps["mlp"] < sweeps["none"]
-    assert sweeps["mlp"] <= 1.05 * sweeps["cache"]
     # PSOR ran to the same residual from either start.  Frictional contact
     # solutions are not unique, so velocities may differ between starts;
     # contact impulses are internal, so linear momentum is the same, and
@@ -164,6 +164,42 @@ def test_sweep_gated_learned_start(trained):
     g.mlp_set_params(params)
     r = g.step(40)
     assert r["not_converged"] == 0 and r["max_residual"] < 1e-6
+
+
+def test_learned_start_beats_cache_on_held_out_systems(tmp_path):
+    """The learned warm start trained on plain-PSOR records (8 seeded runs of
+    20,000 rods, aspect ratio 20, mu ~ U[0.1, 0.8], written to and read back
+    from the record file format) against the cache start on 4 other seeds:
+    it must need clearly fewer PSOR sweeps for the same residual tolerance.
+    (In this regime most sweeps come from steps that stall near the
+    tolerance from the cache start; the learned start lets more of them
+    converge.)"""
+    from rodgpu import records
+    path = tmp_path / "records.npz"
+    records.generate(8, 100, n=20000, ar=20, phi=0.10, mu_range=(0.1, 0.8), seed=11, warmup=50, path=path)
+    ds = records.load(path)
+    assert len(ds["features"]) > 50000 and len(ds["runs"]) == 8
+    trainer = rodgpu.System(rodgpu.default_config(n_bodies=16, model="nsc"))
+    trainer.mlp_train(ds["features"], ds["targets"], epochs=20, batch=4096, lr=1e-3, seed=3)
+    params = trainer.mlp_get_params()
+    sweeps = {"cache": 0, "mlp": 0}
+    capped = {"cache": 0, "mlp": 0}
+    for k in range(4):
+        rng = np.random.default_rng(1000 + k)
+        mu = float(rng.uniform(0.1, 0.8))
+        sc = scene.make_rods_device(20000, 1.0, 0.05, phi=0.10, seed=9000 + k, max_attempts=20000)
+        for warm in ("cache", "mlp"):
+            g = _nsc_system(sc, warm, nsc_mu=mu, nsc_mlp_min_sweeps=3)
+            if warm == "mlp":
+                g.mlp_set_params(params)
+            g.step(50)
+            r = g.step(100)
+            sweeps[warm] += r["psor_sweeps"]
+            capped[warm] += r["not_converged"]
+            g.close()
+    print("held-out sweeps:", sweeps, "steps at the sweep cap:", capped)
+    assert sweeps["mlp"] < 0.8 * sweeps["cache"]
+    assert capped["mlp"] <= capped["cache"]
 
 
 def test_mlp_warm_start_requires_network():
