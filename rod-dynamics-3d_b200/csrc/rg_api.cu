@@ -443,9 +443,9 @@ int rg_create(const rg_config* cfg, rg_system** out) {
   // identity orientations
   std::vector<double> one(s->n, 1.0);
   cudaMemcpy(s->st.q.w, one.data(), sizeof(double) * s->n, cudaMemcpyHostToDevice);
-  // persistent kernels run one 256-thread block per SM (co-residency is
+  // persistent kernels run as many blocks per SM as fit (co-residency is
   // guaranteed by the cooperative launch attribute)
-  s->coop_blocks = s->sm_count;
+  s->coop_blocks = s->sm_count * nsc_blocks_per_sm();
   s->team_blocks = cfg->team_blocks;  // NSC team size; 0 = automatic
   *out = s;
   return RG_OK;

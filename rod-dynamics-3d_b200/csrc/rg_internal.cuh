@@ -310,6 +310,7 @@ void wrap_launch(rg_system* s);
 // rg_nsc.cu
 void nsc_run_launch(rg_system* s, int nsteps);
 int nsc_team_blocks(const rg_system* s);
+int nsc_blocks_per_sm();
 size_t nsc_view_bytes();
 size_t nsc_team_bytes();
 // rg_mlp.cu

@@ -790,8 +790,11 @@ __device__ __noinline__ bool project_phase(const Team& T, const NscView& V, int 
 // phases synchronise with __syncthreads.  Same arithmetic, same order as the
 // team path and the oracle.
 // ---------------------------------------------------------------------------
-constexpr int kSmallC = kTile;       // one contact per thread
-constexpr int kSmallB = 2 * kTile;   // local body slots
+#ifndef RG_SMALL_C
+#define RG_SMALL_C kTile
+#endif
+constexpr int kSmallC = RG_SMALL_C;      // one contact per thread
+constexpr int kSmallB = 2 * kSmallC;     // local body slots
 
 struct SmallSmem {
   double row[kRowComps * kSmallC];   // manifold rows (or projection rows)
@@ -811,9 +814,15 @@ struct SmallSmem {
   int mtile[kSmallC / 16];           // 16-contact tiles that need the network
   unsigned char cached[kSmallC];     // 1: the slot's contact is in the warm cache
   // one hidden layer of the network (the rest is staged in pmax/cmask)
+#ifndef RG_NO_MLP_STAGE
   alignas(16) __nv_bfloat16 wh[kStageWh];
+#else
+  alignas(16) __nv_bfloat16 wh[8];  // build without in-step inference staging
+#endif
 };
+#ifndef RG_NO_MLP_STAGE
 static_assert(sizeof(unsigned long long) * 3 * kSmallB >= kStageSmallBytes, "MLP staging space");
+#endif
 static_assert(sizeof(SmallSmem) >= kBuildQOff + 2 * sizeof(unsigned) * kBuildQ,
               "list-build tiles and queues share the small-solve memory");
 
@@ -1560,7 +1569,10 @@ constexpr int kBlock = RG_NSC_BLOCK;  // threads per block of the persistent ste
 // of the team's systems, one system after the other within a step.  A
 // system whose step failed (error bits set) returns at once from its later
 // steps; the others carry on.
-__global__ void __launch_bounds__(kBlock, 1) k_nsc_run(const NscView* views, const TeamDesc* teams, int nteams,
+#ifndef RG_NSC_MIN_BLOCKS
+#define RG_NSC_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kBlock, RG_NSC_MIN_BLOCKS) k_nsc_run(const NscView* views, const TeamDesc* teams, int nteams,
                                                    const int* members, int nsteps) {
   __shared__ SmemNsc sm;
   extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -1700,6 +1712,23 @@ void nsc_batch_launch(const NscView* views, const TeamDesc* teams, int nteams, c
 }
 
 int nsc_block_threads() { return kBlock; }
+
+// Co-resident blocks of the persistent kernel per SM (its registers and
+// shared memory decide; the cooperative launch needs them all resident).
+int nsc_blocks_per_sm() {
+  static int per_sm = -1;
+  if (per_sm < 0) {
+    nsc_set_smem();
+    int k = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, k_nsc_run, kBlock, sizeof(SmallSmem)) != cudaSuccess ||
+        k < 1) {
+      cudaGetLastError();
+      k = 1;
+    }
+    per_sm = k;
+  }
+  return per_sm;
+}
 size_t nsc_block_smem() { return sizeof(SmallSmem) + sizeof(SmemNsc); }
 
 size_t nsc_view_bytes() { return sizeof(NscView); }
