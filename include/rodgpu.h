@@ -204,7 +204,12 @@ int rg_set_bodies(rg_system* sys, const double* radius, const double* half_heigh
                   const double* restitution);
 
 /* State, structure of arrays: x[3N], q[4N] (w,x,y,z), v[3N], w[3N].
- * Forces f[3N], tau[3N] may be NULL on set (zeroed) or on get (skipped). */
+ * Forces f[3N], tau[3N] may be NULL on set (zeroed) or on get (skipped).
+ * Soft / Hertz-Mindlin models: both force evaluations of a step start from
+ * zero forces (the reference clears them in integrateSecondHalf,
+ * src/physics/integrator.cpp:156-158); after a step f and tau hold the
+ * forces at t + dt that its second half kick used, after rg_compute_forces
+ * the forces it returned. */
 int rg_set_state(rg_system* sys, const double* x, const double* q,
                  const double* v, const double* w,
                  const double* f, const double* tau);

@@ -688,15 +688,17 @@ void second_half(orc_system& S) {
     if (c.ang_damp > 0.0) S.w[i] = S.w[i] * ea;
     double wl = length(S.w[i]);
     if (wl > c.w_max) S.w[i] = S.w[i] * (c.w_max / wl);
-    S.f[i] = v3(0, 0, 0);
-    S.tau[i] = v3(0, 0, 0);
   }
 }
 
 // Velocity-Verlet step of App::physicsStep for the soft and HM branches
-// (main.cpp:4529-4609 and :4610-4810) with random forces, walls and sleep
-// disabled.
+// (main.cpp:4529-4609 and :4610-4810) with random forces and sleep disabled.
+// Both evaluations start from zero forces: integrateSecondHalf clears them
+// for the next frame (integrator.cpp:156-158) and the step clears them
+// before the second evaluation.  The forces at t + dt are left in f and tau
+// (the library's state after a step reports them).
 void verlet_step(orc_system& S) {
+  for (int i = 0; i < S.n; ++i) { S.f[i] = v3(0, 0, 0); S.tau[i] = v3(0, 0, 0); }
   force_eval(S);
   half_pos(S);
   for (int i = 0; i < S.n; ++i) { S.f[i] = v3(0, 0, 0); S.tau[i] = v3(0, 0, 0); }

@@ -75,7 +75,7 @@ void free_contact_buffers(rg_system* s) {
   s->csr = BodyCSR();
   History& H = s->hist;
   for (int k = 0; k < 2; ++k) { cudaFree(H.key[k]); cudaFree(H.val[k]); cudaFree(H.frame[k]); }
-  cudaFree(H.found); cudaFree(H.touched); cudaFree(H.touched_off); cudaFree(H.kept);
+  cudaFree(H.touched); cudaFree(H.touched_off); cudaFree(H.kept);
   cudaFree(H.kept_off); cudaFree(H.newval);
   H = History();
   Nsc& N = s->nsc;
@@ -111,7 +111,6 @@ cudaError_t alloc_contact_buffers(rg_system* s, int ccap, int hcap) {
     if ((e = cudaMalloc(&H.val[k], sizeof(double) * 3 * (size_t)hcap))) return e;
     if ((e = cudaMalloc(&H.frame[k], sizeof(long long) * hcap))) return e;
   }
-  if ((e = cudaMalloc(&H.found, sizeof(int) * ccap))) return e;
   if ((e = cudaMalloc(&H.touched, sizeof(int) * (ccap + 1)))) return e;
   if ((e = cudaMalloc(&H.touched_off, sizeof(int) * (ccap + 1)))) return e;
   if ((e = cudaMalloc(&H.kept, sizeof(int) * (hcap + 1)))) return e;
@@ -572,14 +571,14 @@ int rg_get_state(const rg_system* s, double* x, double* q, double* v, double* w,
 namespace rg {
 
 // One velocity-Verlet step (main.cpp:4610-4810): forces at t, half kick and
-// drift, forces at t + dt, second half kick.
+// drift, forces at t + dt, second half kick.  Each evaluation starts from
+// zero forces (integrateSecondHalf clears them for the next frame,
+// integrator.cpp:156-158, and the step clears them again before the second
+// evaluation); the per-body sums are fused into the two kick kernels.
 static void verlet_step(rg_system* s) {
-  force_eval_launch(s);      // forces at t (reuses fresh contacts)
-  half_pos_launch(s);
-  clear_forces_launch(s);
+  force_eval_launch(s, EvalTail::kHalfPos);  // forces at t (reuses fresh contacts), kick and drift
   s->contacts_fresh = false;
-  force_eval_launch(s);      // forces at t + dt
-  second_half_launch(s);
+  force_eval_launch(s, EvalTail::kSecondHalf, true);  // forces at t + dt, second kick
   s->contacts_fresh = true;  // positions unchanged until the next drift
 }
 

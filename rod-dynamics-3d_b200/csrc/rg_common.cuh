@@ -217,6 +217,66 @@ __device__ inline int contact_type(double s, double t) {
   return 2;
 }
 
+// ---- programmatic dependent launch -------------------------------------------
+// A kernel launched with programmatic stream serialization (launch_dep) may
+// be scheduled while the kernel before it in the stream drains; this wait
+// returns once that kernel has completed and its writes are visible.  Every
+// kernel launched through launch_dep calls it before touching memory (for a
+// kernel launched without the attribute it returns at once).
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// ---- per-body force terms of the soft / Hertz-Mindlin models ------------------
+// f += Σ, tau += Σ of a body's contact addends in contact order (the
+// reference's sequential accumulation, f[a] -= F; f[b] += F over the contact
+// list).  off/ent: the body -> contact CSR (ent = 2c for side a, 2c + 1 for
+// side b); cf: 12 addend arrays of ccap (f_a, tau_a, f_b, tau_b).
+__device__ inline void body_sum(const int* off, const int* ent, const double* cf, int ccap, int i, d3& f,
+                                d3& t) {
+  const int s = off[i], e = off[i + 1];
+  for (int k = s; k < e; ++k) {
+    const int v = ent[k];
+    const int c = v >> 1;
+    const int base = (v & 1) ? 6 : 0;
+    f.x = f.x + cf[(size_t)(base + 0) * ccap + c];
+    f.y = f.y + cf[(size_t)(base + 1) * ccap + c];
+    f.z = f.z + cf[(size_t)(base + 2) * ccap + c];
+    t.x = t.x + cf[(size_t)(base + 3) * ccap + c];
+    t.y = t.y + cf[(size_t)(base + 4) * ccap + c];
+    t.z = t.z + cf[(size_t)(base + 5) * ccap + c];
+  }
+}
+
+// Cylinder wall of the soft model on one dynamic body (main.cpp:4661-4690 at
+// phase t, :4756-4787 at phase t + dt): a penalty spring on the centre's
+// radial overshoot past R - r plus smooth Coulomb friction (tanh of |v_t| /
+// nu), added to f.  ax: the unit cylinder axis (soft_wall_axis).
+__device__ inline d3 soft_wall_axis(const rg_config& c) {
+  const d3 ax{c.cylinder_axis[0], c.cylinder_axis[1], c.cylinder_axis[2]};
+  return ax / len(ax);
+}
+__device__ inline void soft_wall_apply(const rg_config& cfg, d3 ax, double r, d3 x, d3 v, d3& f) {
+  const double k = cfg.soft_k_scaler, cd = cfg.soft_damping, mu = cfg.soft_mu;
+  const double nu = smax(cfg.soft_nu, 1e-10);
+  const double maxd = cfg.cylinder_radius - r;
+  const d3 pp = x - ax * dot(x, ax);
+  const double d = len(pp);
+  const double pen = d - maxd;
+  if (pen <= 0.0) return;
+  d3 n;
+  if (d > 1e-8) {
+    n = pp / d;
+  } else {
+    const d3 cr = cross(ax, fabs(ax.x) < 0.9 ? mk3(1, 0, 0) : mk3(0, 1, 0));
+    n = cr / len(cr);
+  }
+  const double vn = dot(v, n);
+  const double fn = k * pen + cd * smax(vn, 0.0);
+  f = f - n * fn;
+  const d3 vt = v - n * vn;
+  const double vtl = len(vt);
+  if (vtl > 1e-12) f = f - vt * (mu * fn * tanh(vtl / nu) / vtl);
+}
+
 // ---- reductions --------------------------------------------------------------
 __device__ inline double warp_max(double v) {
 #pragma unroll

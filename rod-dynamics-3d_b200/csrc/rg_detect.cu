@@ -26,71 +26,125 @@ long long g_launches = 0;
 // Exclusive scan in one pass: decoupled look-back (Merrill & Garland, "Single-
 // pass Parallel Prefix Scan with Decoupled Look-back", 2016).  Blocks take
 // tiles in increasing order from a counter; a tile publishes its aggregate,
-// adds the published values of its predecessors until it meets an inclusive
-// prefix, then publishes its own inclusive prefix and writes its outputs.
-// A tile only waits on tiles taken before it by running blocks, and every
-// wait is bounded (ERR_TIMEOUT after kScanSpin polls).  n is read on the
-// device; the tile status words are cleared by a memset before each scan.
+// then one warp adds the published values of its predecessors, 32 status
+// words at a time, until it meets an inclusive prefix; the tile publishes its
+// own inclusive prefix and writes its outputs.  A tile only waits on tiles
+// taken before it by running blocks, and every wait is bounded (ERR_TIMEOUT
+// after kScanSpin polls).  n is read on the device; the tile status words
+// are cleared by a memset before each scan.  Each thread scans kScanItems
+// consecutive values, loaded and stored as int4 when the arrays allow it.
 // ---------------------------------------------------------------------------
-constexpr int kScanBS = 1024;
-constexpr int kScanItems = 2;
+constexpr int kScanBS = 512;
+constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanBS * kScanItems;
 constexpr long long kScanSpin = 1 << 24;
 constexpr unsigned long long kTileAgg = 1ull << 62, kTileInc = 2ull << 62;
 
-__global__ void k_scan_lookback(const int* in, int* out, const int* n_dev, unsigned long long* status, int* err) {
+__device__ inline unsigned long long scan_status_load(unsigned long long* w) {
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*w);
+  return r.load(cuda::memory_order_acquire);
+}
+__device__ inline void scan_status_store(unsigned long long* w, unsigned long long v) {
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*w);
+  r.store(v, cuda::memory_order_release);
+}
+
+// Exclusive prefix of tile t (t > 0) from its predecessors' status words
+// (status[p] for tile p), by warp 0; valid in every lane.  Returns false
+// when a wait ran out (ERR_TIMEOUT set).
+__device__ inline bool scan_lookback(unsigned long long* status, int t, int* err, int& prefix) {
+  const int lane = threadIdx.x & 31;
+  prefix = 0;
+  for (int p = t - 1;; p -= 32) {
+    const int idx = p - lane;  // lane k reads tile p - k
+    unsigned long long w = idx >= 0 ? scan_status_load(&status[idx]) : kTileInc;
+    long long it = 0;
+    while (!__all_sync(0xffffffffu, (w >> 62) != 0)) {
+      if (++it > kScanSpin) {
+        if (lane == 0) atomicOr(err, ERR_TIMEOUT);
+        return false;
+      }
+      if (it > 32) __nanosleep(32);
+      if ((w >> 62) == 0) w = scan_status_load(&status[idx]);
+    }
+    // the nearest inclusive prefix (lowest lane) ends the walk
+    const unsigned inc = __ballot_sync(0xffffffffu, (w & kTileInc) != 0);
+    const int stop = inc ? __ffs(inc) - 1 : 32;
+    const int v = (lane <= stop && idx >= 0) ? (int)(unsigned)(w & 0xffffffffull) : 0;
+    prefix += warp_sum_i(v);
+    if (inc) return true;
+  }
+}
+
+// words: [0] tile counter, [1 + t] status of tile t.
+__global__ void __launch_bounds__(kScanBS) k_scan_lookback(const int* in, int* out, const int* n_dev,
+                                                           unsigned long long* words, int* err) {
   __shared__ int shw[32];
-  __shared__ int sh_tile, sh_excl;
-  int* tile_ctr = reinterpret_cast<int*>(status);  // word 0; tile t's status is status[t + 1]
+  __shared__ int sh_tile, sh_excl, sh_ok;
+  int* tile_ctr = reinterpret_cast<int*>(&words[0]);
+  unsigned long long* status = words + 1;
   const int n = *n_dev;
   const int ntile = (n + kScanTile - 1) / kScanTile;
   if (ntile == 0) {
     if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = 0;
     return;
   }
+  const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
   for (;;) {
     if (threadIdx.x == 0) sh_tile = atomicAdd(tile_ctr, 1);
     __syncthreads();
     const int t = sh_tile;
     if (t >= ntile) return;
     const int base = t * kScanTile + threadIdx.x * kScanItems;
-    const int v0 = base < n ? in[base] : 0;
-    const int v1 = base + 1 < n ? in[base + 1] : 0;
+    int v[kScanItems];
+    if (vec && base + kScanItems <= n) {
+      const int4 a = *reinterpret_cast<const int4*>(in + base);
+      const int4 b = *reinterpret_cast<const int4*>(in + base + 4);
+      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < kScanItems; ++k) v[k] = base + k < n ? in[base + k] : 0;
+    }
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) sum += v[k];
     int tot;
-    const int ex = block_excl_scan(v0 + v1, shw, tot);
-    if (threadIdx.x == 0) {
-      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> mine(status[t + 1]);
+    const int ex = block_excl_scan(sum, shw, tot);
+    if (threadIdx.x < 32) {
       int prefix = 0;
+      bool ok = true;
       if (t == 0) {
-        mine.store(kTileInc | (unsigned)tot, cuda::memory_order_release);
+        if (threadIdx.x == 0) scan_status_store(&status[0], kTileInc | (unsigned)tot);
       } else {
-        mine.store(kTileAgg | (unsigned)tot, cuda::memory_order_release);
-        for (int p = t - 1; p >= 0;) {
-          cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> prev(status[p + 1]);
-          unsigned long long w = prev.load(cuda::memory_order_acquire);
-          long long it = 0;
-          while ((w >> 62) == 0) {
-            if (++it > kScanSpin) {
-              atomicOr(err, ERR_TIMEOUT);
-              break;
-            }
-            if (it > 32) __nanosleep(32);
-            w = prev.load(cuda::memory_order_acquire);
-          }
-          if ((w >> 62) == 0) break;  // gave up: the call fails with ERR_TIMEOUT
-          prefix += (int)(unsigned)(w & 0xffffffffull);
-          if (w & kTileInc) break;
-          --p;
-        }
-        mine.store(kTileInc | (unsigned)(prefix + tot), cuda::memory_order_release);
+        if (threadIdx.x == 0) scan_status_store(&status[t], kTileAgg | (unsigned)tot);
+        ok = scan_lookback(status, t, err, prefix);
+        // gave up: the call fails with ERR_TIMEOUT; later tiles see an aggregate
+        if (ok && threadIdx.x == 0) scan_status_store(&status[t], kTileInc | (unsigned)(prefix + tot));
       }
-      sh_excl = prefix;
-      if (t == ntile - 1) out[n] = prefix + tot;
+      if (threadIdx.x == 0) {
+        sh_excl = prefix;
+        sh_ok = ok;
+        if (t == ntile - 1) out[n] = prefix + tot;
+      }
     }
     __syncthreads();
-    const int add = sh_excl;
-    if (base < n) out[base] = add + ex;
-    if (base + 1 < n) out[base + 1] = add + ex + v0;
+    if (!sh_ok) return;
+    int run = sh_excl + ex;
+    int o[kScanItems];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      o[k] = run;
+      run += v[k];
+    }
+    if (vec && base + kScanItems <= n) {
+      *reinterpret_cast<int4*>(out + base) = make_int4(o[0], o[1], o[2], o[3]);
+      *reinterpret_cast<int4*>(out + base + 4) = make_int4(o[4], o[5], o[6], o[7]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kScanItems; ++k)
+        if (base + k < n) out[base + k] = o[k];
+    }
     __syncthreads();  // sh_tile / sh_excl are reused by the next tile
   }
 }
@@ -106,7 +160,7 @@ void Scan::free_() {
 }
 void Scan::run(const int* in, int* out, const int* n_dev, int* err, cudaStream_t s) const {
   const int tiles = (cap + kScanTile - 1) / kScanTile + 1;
-  int g = tiles < 148 * 2 ? tiles : 148 * 2;
+  int g = tiles < 148 * 4 ? tiles : 148 * 4;
   if (g < 1) g = 1;
   unsigned long long* status = reinterpret_cast<unsigned long long*>(d_blocks);
   cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (tiles + 1), s);
@@ -302,7 +356,12 @@ __global__ void k_cell_count_dyn(const Seg* seg, int n, const GridDev* gd, int p
 // ---------------------------------------------------------------------------
 // Narrow phase over the lists: count -> scan -> write (sorted by (a,b)).
 // ---------------------------------------------------------------------------
-__global__ void k_narrow_count(const Seg* seg, State st, Box box, double delta, const int* nbr_cnt,
+// Resident 256-thread blocks per SM k_narrow_count is compiled for (one rod
+// per thread, latency-bound on the neighbour gathers: more resident warps).
+#ifndef RG_NARROW_MIN_BLOCKS
+#define RG_NARROW_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(256, RG_NARROW_MIN_BLOCKS) k_narrow_count(const Seg* seg, State st, Box box, double delta, const int* nbr_cnt,
                                const int* nbr, int maxnb, int words, unsigned long long* mask,
                                int* hit_cnt, const Ctl* ctl) {
   if (ctl->err) return;
@@ -468,7 +527,7 @@ void force_rebuild(rg_system* s) {
 // Full detection at the current state with activation margin `delta`:
 // segment records, (optional) displacement check and list rebuild, narrow
 // phase.  Result: s->con sorted by (a,b) and ctl->contacts.
-void detect_launch(rg_system* s, double delta, bool check_rebuild) {
+void detect_launch(rg_system* s, double delta, bool check_rebuild, bool seg_ready) {
   Detector& d = s->det;
   const int n = s->n;
   cudaStream_t st = s->stream;
@@ -477,9 +536,11 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild) {
   const int bs = 256;
   const int g = grid_for(n, bs);
   const bool near = d.near_cnt != nullptr;
-  RGL k_seg<<<g, bs, 0, st>>>(s->st, d.seg);
-  if (check_rebuild && !d.all_pairs) {
-    RGL k_disp_check<<<g, bs, 0, st>>>(s->st, d.seg, d.ref, near ? d.ref2 : nullptr, s->box, d.skin, ctl);
+  if (!seg_ready) {
+    RGL k_seg<<<g, bs, 0, st>>>(s->st, d.seg);
+    if (check_rebuild && !d.all_pairs) {
+      RGL k_disp_check<<<g, bs, 0, st>>>(s->st, d.seg, d.ref, near ? d.ref2 : nullptr, s->box, d.skin, ctl);
+    }
   }
   // --- rebuild: every kernel below returns at once unless ctl->rebuild ---
   if (!s->box.pbc) {

@@ -93,39 +93,18 @@ __device__ inline int lower_bound_u64(const unsigned long long* k, int n, unsign
   return lo;
 }
 
-__global__ void k_eval_begin(Ctl* ctl) {
-  if (ctl->err) return;
-  ctl->frame += 1;
-}
-
-__global__ void k_hist_lookup(const int* ca, const int* cb, const unsigned long long* hkey, int* found,
-                              const Ctl* ctl) {
-  if (ctl->err) return;
-  const int C = ctl->contacts, H = ctl->hist_n;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
-    unsigned long long k = pkey(ca[c], cb[c]);
-    int p = lower_bound_u64(hkey, H, k);
-    found[c] = (p < H && hkey[p] == k) ? p : -1;
-  }
-}
-
-// kept[e]: retained untouched entries (HM: 4-frame retention; Cundall: all).
+// kept[e]: entries retained if untouched (HM: 4-frame retention; Cundall:
+// all); the force kernel that follows clears the touched ones.  fr is the
+// frame this evaluation opens (the force kernel advances ctl->frame).
 __global__ void k_hist_keep_init(const long long* hframe, int* kept, int hm, const Ctl* ctl) {
   if (ctl->err) return;
   const int H = ctl->hist_n;
-  const long long fr = ctl->frame;
+  const long long fr = ctl->frame + 1;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < H; e += gridDim.x * blockDim.x) {
     long long lf = hframe[e];
     kept[e] = hm ? ((fr - lf > 4 || lf == 0) ? 0 : 1) : 1;
   }
 }
-__global__ void k_hist_keep_clear(const int* found, const int* touched, int* kept, const Ctl* ctl) {
-  if (ctl->err) return;
-  const int C = ctl->contacts;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x)
-    if (touched[c] && found[c] >= 0) kept[found[c]] = 0;
-}
-
 __global__ void k_hist_merge(const int* ca, const int* cb, const int* touched, const int* toff,
                              const double* newval, const unsigned long long* okey, const double* oval,
                              const long long* oframe, const int* kept, const int* koff,
@@ -184,7 +163,8 @@ struct ForceIO {
   int *ca, *cb;
   const double* g;  // contact component arrays (Contacts::comp)
   int ccap;
-  const int* found;
+  const unsigned long long* hkey;  // current table keys (sorted)
+  int* kept;           // per table entry: 1 = retained untouched (cleared here when touched)
   const double* hval;  // current table values (3 * hcap SoA)
   int hcap;
   double* newval;      // 3 * ccap
@@ -192,6 +172,19 @@ struct ForceIO {
   double* cf;          // 12 * ccap
   double* pe;          // ccap
 };
+
+// Index of the pair (a, b) in the history table (binary search over the
+// sorted keys), or -1.
+__device__ inline int hist_find(const ForceIO& io, int a, int b, int H) {
+  const unsigned long long k = pkey(a, b);
+  const int p = lower_bound_u64(io.hkey, H, k);
+  return (p < H && io.hkey[p] == k) ? p : -1;
+}
+// The force kernel of an evaluation advances the frame counter (the
+// reference's frame_counter_ per detectContacts, hertz_mindlin.cpp:31).
+__device__ inline void eval_begin(Ctl* ctl) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->frame += 1;
+}
 
 __device__ inline d3 ldc(const ForceIO& io, int k, int c) {
   return {io.g[(size_t)k * io.ccap + c], io.g[(size_t)(k + 1) * io.ccap + c],
@@ -205,13 +198,15 @@ __device__ inline void st_cf(const ForceIO& io, int c, d3 fa, d3 ta, d3 fb, d3 t
   io.cf[9 * cc + c] = tb.x; io.cf[10 * cc + c] = tb.y; io.cf[11 * cc + c] = tb.z;
 }
 
-__global__ void k_soft_forces(State st, rg_config cfg, ForceIO io, const Ctl* ctl) {
+__global__ void k_soft_forces(State st, rg_config cfg, ForceIO io, Ctl* ctl) {
   if (ctl->err) return;
-  const int C = ctl->contacts;
+  const int C = ctl->contacts, H = ctl->hist_n;
+  eval_begin(ctl);
   const double dt = cfg.dt;
   const double K1 = 15.0 / cfg.soft_delta;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
     const int a = io.ca[c], b = io.cb[c];
+    const int hf = hist_find(io, a, b, H);
     d3 pa = ldc(io, 0, c), pb = ldc(io, 3, c), nrm = ldc(io, 6, c), sh = ldc(io, 9, c);
     double dist = io.g[(size_t)12 * io.ccap + c], hs = io.g[(size_t)13 * io.ccap + c];
     // potentialGradient / potentialEnergy
@@ -252,7 +247,7 @@ __global__ void k_soft_forces(State st, rg_config cfg, ForceIO io, const Ctl* ct
       double vtm = len(vt);
       if (!(vtm < 1e-10)) {
         if (cfg.soft_friction_mode == RG_FRICTION_CUNDALL) {
-          int f = io.found[c];
+          const int f = hf;
           d3 old{0, 0, 0};
           if (f >= 0) old = mk3(io.hval[f], io.hval[io.hcap + f], io.hval[2 * io.hcap + f]);
           d3 ft = old - vt * (cfg.soft_kt * dt);
@@ -301,14 +296,16 @@ __global__ void k_soft_forces(State st, rg_config cfg, ForceIO io, const Ctl* ct
     d3 ta = fa + fra, tb = fb - fra;
     st_cf(io, c, ta, cross(ra, ta), tb, cross(rb, tb));
     io.touched[c] = touch;
+    if (touch && hf >= 0) io.kept[hf] = 0;  // the touched entry is rewritten, not retained
     io.newval[c] = nv.x; io.newval[io.ccap + c] = nv.y; io.newval[2 * io.ccap + c] = nv.z;
     io.pe[c] = cfg.soft_k_scaler * U;
   }
 }
 
-__global__ void k_hm_forces(State st, rg_config cfg, ForceIO io, const Ctl* ctl) {
+__global__ void k_hm_forces(State st, rg_config cfg, ForceIO io, Ctl* ctl) {
   if (ctl->err) return;
-  const int C = ctl->contacts;
+  const int C = ctl->contacts, H = ctl->hist_n;
+  eval_begin(ctl);
   const double dt = cfg.dt;
   const double nu = cfg.hm_poisson_ratio;
   const double Es = cfg.hm_youngs_modulus / (2.0 * (1.0 - nu * nu));
@@ -320,6 +317,7 @@ __global__ void k_hm_forces(State st, rg_config cfg, ForceIO io, const Ctl* ctl)
   }
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
     const int a = io.ca[c], b = io.cb[c];
+    const int hf = hist_find(io, a, b, H);
     d3 pa = ldc(io, 0, c), pb = ldc(io, 3, c), nrm = ldc(io, 6, c), sh = ldc(io, 9, c);
     double dist = io.g[(size_t)12 * io.ccap + c], hs = io.g[(size_t)13 * io.ccap + c];
     double ra_ = st.r[a], rb_ = st.r[b], ma = st.mass[a], mb = st.mass[b];
@@ -343,7 +341,7 @@ __global__ void k_hm_forces(State st, rg_config cfg, ForceIO io, const Ctl* ctl)
     double Fn = smax(0.0, Fel + (-Cn * vn));
     d3 fn = nrm * Fn;
     d3 ft{0, 0, 0};
-    int f = io.found[c];
+    const int f = hf;
     d3 xi{0, 0, 0};
     if (f >= 0) xi = mk3(io.hval[f], io.hval[io.hcap + f], io.hval[2 * io.hcap + f]);
     if (cfg.hm_enable_tangential) {
@@ -380,6 +378,7 @@ __global__ void k_hm_forces(State st, rg_config cfg, ForceIO io, const Ctl* ctl)
     d3 F = fn + ft;
     st_cf(io, c, -F, cross(ra, -F) + tra, F, cross(rb, F) + trb);
     io.touched[c] = 1;
+    if (hf >= 0) io.kept[hf] = 0;  // the touched entry is rewritten, not retained
     io.newval[c] = xi.x; io.newval[io.ccap + c] = xi.y; io.newval[2 * io.ccap + c] = xi.z;
     io.pe[c] = (8.0 / 15.0) * Es * sqrt(Rs) * pow(delta, 2.5);
   }
@@ -390,62 +389,27 @@ __global__ void k_body_reduce(State st, const int* off, const int* ent, const do
                               const Ctl* ctl) {
   if (ctl->err) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
-    int s = off[i], e = off[i + 1];
-    if (s == e) continue;
+    if (off[i] == off[i + 1]) continue;
     d3 f = st.f.ld(i), t = st.tau.ld(i);
-    for (int k = s; k < e; ++k) {
-      int v = ent[k];
-      int c = v >> 1;
-      int base = (v & 1) ? 6 : 0;
-      f.x = f.x + cf[(size_t)(base + 0) * ccap + c];
-      f.y = f.y + cf[(size_t)(base + 1) * ccap + c];
-      f.z = f.z + cf[(size_t)(base + 2) * ccap + c];
-      t.x = t.x + cf[(size_t)(base + 3) * ccap + c];
-      t.y = t.y + cf[(size_t)(base + 4) * ccap + c];
-      t.z = t.z + cf[(size_t)(base + 5) * ccap + c];
-    }
+    body_sum(off, ent, cf, ccap, i, f, t);
     st.f.st(i, f);
     st.tau.st(i, t);
   }
 }
 
-// Deterministic potential-energy sum: fixed-shape two-level reduction.
-// Cylinder wall of the soft model (main.cpp:4661-4690 at phase t, :4756-4787
-// at phase t + dt): a penalty spring on the centre's radial overshoot past
-// R - r plus smooth Coulomb friction (tanh of |v_t| / nu); force only.
+// Cylinder wall of the soft model on every dynamic body (soft_wall_apply).
 __global__ void k_soft_wall(State st, rg_config cfg, const Ctl* ctl) {
   if (ctl->err) return;
-  d3 ax{cfg.cylinder_axis[0], cfg.cylinder_axis[1], cfg.cylinder_axis[2]};
-  ax = ax / len(ax);
-  const double k = cfg.soft_k_scaler, cd = cfg.soft_damping, mu = cfg.soft_mu;
-  const double nu = smax(cfg.soft_nu, 1e-10);
+  const d3 ax = soft_wall_axis(cfg);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
     if (!(st.inv_mass[i] > 0.0)) continue;
-    const double maxd = cfg.cylinder_radius - st.r[i];
-    const d3 x = st.x.ld(i);
-    const d3 pp = x - ax * dot(x, ax);
-    const double d = len(pp);
-    const double pen = d - maxd;
-    if (pen <= 0.0) continue;
-    d3 n;
-    if (d > 1e-8) {
-      n = pp / d;
-    } else {
-      const d3 cr = cross(ax, fabs(ax.x) < 0.9 ? mk3(1, 0, 0) : mk3(0, 1, 0));
-      n = cr / len(cr);
-    }
-    const d3 v = st.v.ld(i);
-    const double vn = dot(v, n);
-    const double fn = k * pen + cd * smax(vn, 0.0);
     d3 f = st.f.ld(i);
-    f = f - n * fn;
-    const d3 vt = v - n * vn;
-    const double vtl = len(vt);
-    if (vtl > 1e-12) f = f - vt * (mu * fn * tanh(vtl / nu) / vtl);
+    soft_wall_apply(cfg, ax, st.r[i], st.x.ld(i), st.v.ld(i), f);
     st.f.st(i, f);
   }
 }
 
+// Deterministic potential-energy sum: fixed-shape two-level reduction.
 constexpr int kPeBlocks = 64;
 __global__ void k_pe_partial(const double* pe, double* part, const Ctl* ctl) {
   if (ctl->err) return;
@@ -472,34 +436,40 @@ __global__ void k_pe_final(const double* part, Ctl* ctl) {
   if (threadIdx.x == 0) ctl->pe = sm[0] + sm[1];
 }
 
-// One force evaluation (detect unless the contacts are fresh, forces, history
-// update, reduction into f and tau).
-void force_eval_launch(rg_system* s) {
+// One force evaluation: detect unless the contacts are fresh (seg_ready: the
+// segment records and displacement check were written by the drift kernel),
+// forces and history update, then the tail:
+//   kForces:     reduction into f and tau (+ soft wall) and the potential energy;
+//   kHalfPos:    reduction fused with the first half kick and drift (forces
+//                at t are consumed there, not stored);
+//   kSecondHalf: reduction fused with the second half kick, then the
+//                potential energy.
+void force_eval_launch(rg_system* s, EvalTail tail, bool seg_ready) {
   const rg_config& c = s->cfg;
   const bool hm = c.model == RG_MODEL_HERTZ_MINDLIN;
   cudaStream_t st = s->stream;
   const int bs = 256;
   if (!s->contacts_fresh) {
     ProfScope p(s, ST_DETECT);
-    detect_launch(s, hm ? 0.0 : c.soft_delta, true);
+    detect_launch(s, hm ? 0.0 : c.soft_delta, true, seg_ready);
     csr_launch(s);
   }
   ProfScope prof(s, ST_FORCES);
-  RGL k_eval_begin<<<1, 1, 0, st>>>(s->d_ctl);
   History& H = s->hist;
   const int cur = H.cur, nxt = 1 - H.cur;
   const int gc = grid_for(s->ccap, bs);
-  RGL k_hist_lookup<<<gc, bs, 0, st>>>(s->con.a, s->con.b, H.key[cur], H.found, s->d_ctl);
+  RGL k_hist_keep_init<<<grid_for(H.cap, bs), bs, 0, st>>>(H.frame[cur], H.kept, hm ? 1 : 0, s->d_ctl);
   ForceIO io;
   io.ca = s->con.a; io.cb = s->con.b; io.g = s->con.g; io.ccap = s->ccap;
-  io.found = H.found; io.hval = H.val[cur]; io.hcap = H.cap;
+  io.hkey = H.key[cur]; io.kept = H.kept; io.hval = H.val[cur]; io.hcap = H.cap;
   io.newval = H.newval; io.touched = H.touched; io.cf = s->d_cf;
   io.pe = s->d_cf + 12 * (size_t)s->ccap;
-  if (hm) k_hm_forces<<<gc, bs, 0, st>>>(s->st, c, io, s->d_ctl);
-  else k_soft_forces<<<gc, bs, 0, st>>>(s->st, c, io, s->d_ctl);
+  if (hm) {
+    RGL k_hm_forces<<<gc, bs, 0, st>>>(s->st, c, io, s->d_ctl);
+  } else {
+    RGL k_soft_forces<<<gc, bs, 0, st>>>(s->st, c, io, s->d_ctl);
+  }
   // history merge
-  RGL k_hist_keep_init<<<grid_for(H.cap, bs), bs, 0, st>>>(H.frame[cur], H.kept, hm ? 1 : 0, s->d_ctl);
-  RGL k_hist_keep_clear<<<gc, bs, 0, st>>>(H.found, H.touched, H.kept, s->d_ctl);
   s->scan.run(H.touched, H.touched_off, &s->d_ctl->contacts, &s->d_ctl->err, st);
   s->scan.run(H.kept, H.kept_off, &s->d_ctl->hist_n, &s->d_ctl->err, st);
   RGL k_hist_merge<<<gc, bs, 0, st>>>(s->con.a, s->con.b, H.touched, H.touched_off, H.newval, H.key[cur],
@@ -507,11 +477,19 @@ void force_eval_launch(rg_system* s) {
                                   H.frame[nxt], H.cap, s->ccap, s->d_ctl);
   RGL k_hist_finish<<<1, 1, 0, st>>>(H.touched_off, H.kept_off, s->d_ctl);
   H.cur = nxt;
-  // reduction into bodies
-  RGL k_body_reduce<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, s->csr.off, s->csr.ent, s->d_cf, s->ccap,
-                                                   s->d_ctl);
-  if (!hm && c.cylinder_enabled) {
-    RGL k_soft_wall<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, c, s->d_ctl);
+  const bool wall = !hm && c.cylinder_enabled;
+  if (tail == EvalTail::kHalfPos) {
+    reduce_drift_launch(s, wall);
+    return;
+  }
+  if (tail == EvalTail::kSecondHalf) {
+    reduce_kick_launch(s, wall);
+  } else {
+    RGL k_body_reduce<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, s->csr.off, s->csr.ent, s->d_cf, s->ccap,
+                                                     s->d_ctl);
+    if (wall) {
+      RGL k_soft_wall<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, c, s->d_ctl);
+    }
   }
   double* part = s->d_cf + 13 * (size_t)s->ccap;
   RGL k_pe_partial<<<kPeBlocks, 256, 0, st>>>(io.pe, part, s->d_ctl);

@@ -114,7 +114,6 @@ struct History {  // sorted by key (a<<32|b)
   double* val[2] = {nullptr, nullptr};       // 3 * cap each (SoA)
   long long* frame[2] = {nullptr, nullptr};
   int cur = 0;
-  int* found = nullptr;        // ccap: index into current table or -1
   int* touched = nullptr;      // ccap+1 flags -> scan
   int* touched_off = nullptr;  // ccap+1
   int* kept = nullptr;         // cap+1
@@ -295,14 +294,21 @@ inline void prof_resolve(rg_system* s) {
 // rg_detect.cu
 cudaError_t detector_alloc(rg_system* s);
 void detector_free(rg_system* s);
-void detect_launch(rg_system* s, double delta, bool check_rebuild);
+// seg_ready: the segment records and the displacement check of the current
+// positions were written by the drift kernel (reduce_drift_launch)
+void detect_launch(rg_system* s, double delta, bool check_rebuild, bool seg_ready = false);
 void force_rebuild(rg_system* s);
 // rg_forces.cu
-void force_eval_launch(rg_system* s);  // detect (unless fresh) + forces into f, tau
+enum class EvalTail { kForces, kHalfPos, kSecondHalf };
+// detect (unless fresh) + forces; the tail (force_eval_launch in rg_forces.cu)
+void force_eval_launch(rg_system* s, EvalTail tail = EvalTail::kForces, bool seg_ready = false);
+// forces at t reduced per body, first half kick and drift, segment records
+// and displacement check of the drifted positions (velocity Verlet)
+void reduce_drift_launch(rg_system* s, bool wall);
+// forces at t + dt reduced per body (kept in f, tau) and the second half kick
+void reduce_kick_launch(rg_system* s, bool wall);
 void csr_launch(rg_system* s);         // body CSR of the current contacts
 // rg_integrate.cu
-void half_pos_launch(rg_system* s);
-void second_half_launch(rg_system* s);
 void clear_forces_launch(rg_system* s);
 void nsc_free_flight_launch(rg_system* s);
 void nsc_position_update_launch(rg_system* s);
