@@ -30,9 +30,11 @@ long long g_launches = 0;
 // words at a time, until it meets an inclusive prefix; the tile publishes its
 // own inclusive prefix and writes its outputs.  A tile only waits on tiles
 // taken before it by running blocks, and every wait is bounded (ERR_TIMEOUT
-// after kScanSpin polls).  n is read on the device; the tile status words
-// are cleared by a memset before each scan.  Each thread scans kScanItems
-// consecutive values, loaded and stored as int4 when the arrays allow it.
+// after kScanSpin polls).  n is read on the device.  The last block to leave
+// clears the tile status words it used and both counters, so the next scan
+// finds them zeroed without a memset (the words are zeroed once at
+// allocation).  Each thread scans kScanItems consecutive values, loaded and
+// stored as int4 when the arrays allow it.
 // ---------------------------------------------------------------------------
 constexpr int kScanBS = 512;
 constexpr int kScanItems = 8;
@@ -76,25 +78,24 @@ __device__ inline bool scan_lookback(unsigned long long* status, int t, int* err
   }
 }
 
-// words: [0] tile counter, [1 + t] status of tile t.
+// words: [0] tile counter, [1] exit counter, [2 + t] status of tile t.
 __global__ void __launch_bounds__(kScanBS) k_scan_lookback(const int* in, int* out, const int* n_dev,
                                                            unsigned long long* words, int* err) {
+  griddep_wait();
   __shared__ int shw[32];
-  __shared__ int sh_tile, sh_excl, sh_ok;
+  __shared__ int sh_tile, sh_excl, sh_ok, sh_last;
   int* tile_ctr = reinterpret_cast<int*>(&words[0]);
-  unsigned long long* status = words + 1;
+  int* exit_ctr = reinterpret_cast<int*>(&words[1]);
+  unsigned long long* status = words + 2;
   const int n = *n_dev;
   const int ntile = (n + kScanTile - 1) / kScanTile;
-  if (ntile == 0) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = 0;
-    return;
-  }
+  if (ntile == 0 && blockIdx.x == 0 && threadIdx.x == 0) out[0] = 0;
   const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
-  for (;;) {
+  while (ntile > 0) {
     if (threadIdx.x == 0) sh_tile = atomicAdd(tile_ctr, 1);
     __syncthreads();
     const int t = sh_tile;
-    if (t >= ntile) return;
+    if (t >= ntile) break;
     const int base = t * kScanTile + threadIdx.x * kScanItems;
     int v[kScanItems];
     if (vec && base + kScanItems <= n) {
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(kScanBS) k_scan_lookback(const int* in, int* o
       }
     }
     __syncthreads();
-    if (!sh_ok) return;
+    if (!sh_ok) break;
     int run = sh_excl + ex;
     int o[kScanItems];
 #pragma unroll
@@ -147,12 +148,30 @@ __global__ void __launch_bounds__(kScanBS) k_scan_lookback(const int* in, int* o
     }
     __syncthreads();  // sh_tile / sh_excl are reused by the next tile
   }
+  // The last block out finds every tile finished and no look-back running:
+  // it clears the status words and the counters for the next scan.
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    sh_last = atomicAdd(exit_ctr, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!sh_last) return;
+  __threadfence();
+  for (int t = threadIdx.x; t < ntile; t += blockDim.x) status[t] = 0;
+  if (threadIdx.x == 0) {
+    *tile_ctr = 0;
+    *exit_ctr = 0;
+  }
 }
 
 cudaError_t Scan::alloc(int cap_) {
   cap = cap_;
   const int tiles = (cap + kScanTile - 1) / kScanTile + 1;
-  return cudaMalloc(&d_blocks, sizeof(unsigned long long) * (tiles + 1));
+  const size_t bytes = sizeof(unsigned long long) * (tiles + 2);
+  cudaError_t e = cudaMalloc(&d_blocks, bytes);
+  if (e == cudaSuccess) e = cudaMemset(d_blocks, 0, bytes);
+  return e;
 }
 void Scan::free_() {
   if (d_blocks) cudaFree(d_blocks);
@@ -162,15 +181,14 @@ void Scan::run(const int* in, int* out, const int* n_dev, int* err, cudaStream_t
   const int tiles = (cap + kScanTile - 1) / kScanTile + 1;
   int g = tiles < 148 * 4 ? tiles : 148 * 4;
   if (g < 1) g = 1;
-  unsigned long long* status = reinterpret_cast<unsigned long long*>(d_blocks);
-  cudaMemsetAsync(status, 0, sizeof(unsigned long long) * (tiles + 1), s);
-  RGL k_scan_lookback<<<g, kScanBS, 0, s>>>(in, out, n_dev, status, err);
+  RGL launch_dep(k_scan_lookback, g, kScanBS, s, in, out, n_dev, static_cast<unsigned long long*>(d_blocks), err);
 }
 
 // ---------------------------------------------------------------------------
 // Segment records, displacement check, cell grid.
 // ---------------------------------------------------------------------------
 __global__ void k_seg(State st, Seg* seg) {
+  griddep_wait();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
     dq q = st.q.ld(i);
     d3 u = axis_y(q);
@@ -186,6 +204,7 @@ __global__ void k_seg(State st, Seg* seg) {
 // bound since the last near-list build goes to ctl->near_disp.
 __global__ void k_disp_check(State st, const Seg* seg, const double* ref, const double* ref2, Box box,
                              double skin, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   __shared__ double sm[32], sm2[32];
   double m = 0.0, m2 = 0.0;
@@ -228,6 +247,7 @@ __device__ inline bool near_rebuild_due(const Ctl* ctl, double near_skin) {
 __global__ void k_near_build(const Seg* seg, int n, const double* inv_mass, Box box, double extra,
                              double near_skin, const int* nbr_cnt, const int* nbr, int maxnb, int* near_cnt,
                              int* near_nbr, double* ref2, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !near_rebuild_due(ctl, near_skin)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const Seg A = seg[i];
@@ -251,6 +271,7 @@ __global__ void k_near_build(const Seg* seg, int n, const double* inv_mass, Box 
 }
 
 __global__ void k_near_done(double near_skin, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !near_rebuild_due(ctl, near_skin)) return;
   ctl->near_valid = 1;
   ctl->near_disp = 0.0;
@@ -259,6 +280,7 @@ __global__ void k_near_done(double near_skin, Ctl* ctl) {
 
 __global__ void k_cell_fill(int n, const int* cell_of, const int* cell_start, int* cell_fill,
                             int* cell_rods, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !ctl->rebuild) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int c = cell_of[i];
@@ -268,6 +290,7 @@ __global__ void k_cell_fill(int n, const int* cell_of, const int* cell_start, in
 }
 
 __global__ void k_zero_cells(int* cnt, int* fill, int ncells, int* nbr_cnt, int n, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !ctl->rebuild) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= ncells || i < n; i += gridDim.x * blockDim.x) {
     if (i <= ncells) cnt[i] = 0;
@@ -282,6 +305,7 @@ __global__ void __launch_bounds__(kTile) k_build_lists(const Seg* seg, int n, co
                                                        double margin, double skin, double cut_center,
                                                        int all_pairs, int* nbr_cnt, int* nbr,
                                                        int maxnb, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !ctl->rebuild) return;
   const GridDev g = *gdev;
   __shared__ BuildSmem sm;
@@ -300,6 +324,7 @@ __global__ void __launch_bounds__(kTile) k_build_lists(const Seg* seg, int n, co
 }
 
 __global__ void k_save_ref(const Seg* seg, int n, double* ref, int* nbr, int* nbr_cnt, int maxnb, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !ctl->rebuild) return;
   int overflow = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -312,6 +337,7 @@ __global__ void k_save_ref(const Seg* seg, int n, double* ref, int* nbr, int* nb
 }
 
 __global__ void k_build_done(Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   if (ctl->rebuild) {
     ctl->rebuilds += 1;
@@ -323,6 +349,7 @@ __global__ void k_build_done(Ctl* ctl) {
 
 __global__ void k_bounds(const Seg* seg, int n, unsigned long long* mn, unsigned long long* mx,
                          const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !ctl->rebuild) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     Seg s = seg[i];
@@ -333,6 +360,7 @@ __global__ void k_bounds(const Seg* seg, int n, unsigned long long* mn, unsigned
 }
 __global__ void k_open_grid(const unsigned long long* mn, const unsigned long long* mx, double cut,
                             int maxdim, GridDev* g, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !ctl->rebuild) return;
   open_grid(mn, mx, cut, maxdim, g);
 }
@@ -340,6 +368,7 @@ __global__ void k_open_grid(const unsigned long long* mn, const unsigned long lo
 // Reads the device grid descriptor into each thread (open systems).
 __global__ void k_cell_count_dyn(const Seg* seg, int n, const GridDev* gd, int pbc, int* cell_of,
                                  int* cell_cnt, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !ctl->rebuild) return;
   GridDev g = *gd;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -364,6 +393,7 @@ __global__ void k_cell_count_dyn(const Seg* seg, int n, const GridDev* gd, int p
 __global__ void __launch_bounds__(256, RG_NARROW_MIN_BLOCKS) k_narrow_count(const Seg* seg, State st, Box box, double delta, const int* nbr_cnt,
                                const int* nbr, int maxnb, int words, unsigned long long* mask,
                                int* hit_cnt, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x)
     hit_cnt[i] = narrow_count_rod(i, seg, st.inv_mass, box, delta, nbr_cnt, nbr, maxnb, words, mask);
@@ -372,6 +402,7 @@ __global__ void __launch_bounds__(256, RG_NARROW_MIN_BLOCKS) k_narrow_count(cons
 __global__ void k_narrow_write(const Seg* seg, int n, Box box, const int* nbr_cnt, const int* nbr,
                                int maxnb, int words, const unsigned long long* mask, const int* hit_off,
                                Contacts con, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   int total = hit_off[n];
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -416,6 +447,7 @@ GridDev* detector_grid(rg_system* s) { return &det_dev(s)->grid; }
 unsigned long long* detector_bounds(rg_system* s) { return det_dev(s)->mn; }
 
 __global__ void k_grid_ncells(DetDev* dd, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err || !ctl->rebuild) return;
   dd->ncells = dd->grid.ncells;
 }
@@ -537,45 +569,45 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild, bool seg_read
   const int g = grid_for(n, bs);
   const bool near = d.near_cnt != nullptr;
   if (!seg_ready) {
-    RGL k_seg<<<g, bs, 0, st>>>(s->st, d.seg);
+    RGL launch_dep(k_seg, g, bs, st, s->st, d.seg);
     if (check_rebuild && !d.all_pairs) {
-      RGL k_disp_check<<<g, bs, 0, st>>>(s->st, d.seg, d.ref, near ? d.ref2 : nullptr, s->box, d.skin, ctl);
+      RGL launch_dep(k_disp_check, g, bs, st, s->st, d.seg, d.ref, near ? d.ref2 : nullptr, s->box, d.skin, ctl);
     }
   }
   // --- rebuild: every kernel below returns at once unless ctl->rebuild ---
   if (!s->box.pbc) {
     cudaMemsetAsync(dd->mn, 0xff, sizeof(dd->mn), st);
     cudaMemsetAsync(dd->mx, 0x00, sizeof(dd->mx), st);
-    RGL k_bounds<<<g, bs, 0, st>>>(d.seg, n, dd->mn, dd->mx, ctl);
-    RGL k_open_grid<<<1, 1, 0, st>>>(dd->mn, dd->mx, d.cut_center, 64, &dd->grid, ctl);
-    RGL k_grid_ncells<<<1, 1, 0, st>>>(dd, ctl);
+    RGL launch_dep(k_bounds, g, bs, st, d.seg, n, dd->mn, dd->mx, ctl);
+    RGL launch_dep(k_open_grid, 1, 1, st, dd->mn, dd->mx, d.cut_center, 64, &dd->grid, ctl);
+    RGL launch_dep(k_grid_ncells, 1, 1, st, dd, ctl);
   }
-  RGL k_zero_cells<<<grid_for((d.ncells + 1 > n ? d.ncells + 1 : n), bs), bs, 0, st>>>(d.cell_cnt, d.cell_fill, d.ncells,
+  RGL launch_dep(k_zero_cells, grid_for((d.ncells + 1 > n ? d.ncells + 1 : n), bs), bs, st, d.cell_cnt, d.cell_fill, d.ncells,
                                                                                      d.nbr_cnt, n, ctl);
-  RGL k_cell_count_dyn<<<g, bs, 0, st>>>(d.seg, n, &dd->grid, s->box.pbc, d.cell_of, d.cell_cnt, ctl);
+  RGL launch_dep(k_cell_count_dyn, g, bs, st, d.seg, n, &dd->grid, s->box.pbc, d.cell_of, d.cell_cnt, ctl);
   s->scan.run(d.cell_cnt, d.cell_start, &dd->ncells, &ctl->err, st);
-  RGL k_cell_fill<<<g, bs, 0, st>>>(n, d.cell_of, d.cell_start, d.cell_fill, d.cell_rods, ctl);
+  RGL launch_dep(k_cell_fill, g, bs, st, n, d.cell_of, d.cell_start, d.cell_fill, d.cell_rods, ctl);
   int gb = d.ncells < s->sm_count * 8 ? d.ncells : s->sm_count * 8;
-  RGL k_build_lists<<<gb, kTile, 0, st>>>(d.seg, n, &dd->grid, s->box, d.cell_start, d.cell_rods,
+  RGL launch_dep(k_build_lists, gb, kTile, st, d.seg, n, &dd->grid, s->box, d.cell_start, d.cell_rods,
                                        d.margin, d.skin, d.cut_center, d.all_pairs ? 1 : 0,
                                        d.nbr_cnt, d.nbr, d.maxnb, ctl);
-  RGL k_save_ref<<<g, bs, 0, st>>>(d.seg, n, d.ref, d.nbr, d.nbr_cnt, d.maxnb, ctl);
-  RGL k_build_done<<<1, 1, 0, st>>>(ctl);
+  RGL launch_dep(k_save_ref, g, bs, st, d.seg, n, d.ref, d.nbr, d.nbr_cnt, d.maxnb, ctl);
+  RGL launch_dep(k_build_done, 1, 1, st, ctl);
   // --- near lists (every kernel below returns at once unless they are due) ---
   const int* lcnt = d.nbr_cnt;
   const int* lnbr = d.nbr;
   if (near) {
-    RGL k_near_build<<<g, bs, 0, st>>>(d.seg, n, s->st.inv_mass, s->box, d.margin + d.near_skin, d.near_skin,
+    RGL launch_dep(k_near_build, g, bs, st, d.seg, n, s->st.inv_mass, s->box, d.margin + d.near_skin, d.near_skin,
                                        d.nbr_cnt, d.nbr, d.maxnb, d.near_cnt, d.near_nbr, d.ref2, ctl);
-    RGL k_near_done<<<1, 1, 0, st>>>(d.near_skin, ctl);
+    RGL launch_dep(k_near_done, 1, 1, st, d.near_skin, ctl);
     lcnt = d.near_cnt;
     lnbr = d.near_nbr;
   }
   // --- narrow phase ---
-  RGL k_narrow_count<<<g, bs, 0, st>>>(d.seg, s->st, s->box, delta, lcnt, lnbr, d.maxnb,
+  RGL launch_dep(k_narrow_count, g, bs, st, d.seg, s->st, s->box, delta, lcnt, lnbr, d.maxnb,
                                    d.mask_words, d.hit_mask, d.hit_cnt, ctl);
   s->scan.run(d.hit_cnt, d.hit_off, &dd->n, &ctl->err, st);
-  RGL k_narrow_write<<<g, bs, 0, st>>>(d.seg, n, s->box, lcnt, lnbr, d.maxnb, d.mask_words,
+  RGL launch_dep(k_narrow_write, g, bs, st, d.seg, n, s->box, lcnt, lnbr, d.maxnb, d.mask_words,
                                    d.hit_mask, d.hit_off, s->con, ctl);
 }
 

@@ -26,6 +26,7 @@ const int* detector_n_dev(rg_system* s);
 // Body CSR: cnt -> scan -> fill -> per-body insertion sort.
 // ---------------------------------------------------------------------------
 __global__ void k_csr_zero(int* cnt, int* fill, int n, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
     cnt[i] = 0;
@@ -33,6 +34,7 @@ __global__ void k_csr_zero(int* cnt, int* fill, int n, const Ctl* ctl) {
   }
 }
 __global__ void k_csr_count(const int* ca, const int* cb, int* cnt, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   const int C = ctl->contacts;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
@@ -42,6 +44,7 @@ __global__ void k_csr_count(const int* ca, const int* cb, int* cnt, const Ctl* c
 }
 __global__ void k_csr_fill(const int* ca, const int* cb, const int* off, int* fill, int* ent,
                            const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   const int C = ctl->contacts;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) {
@@ -51,6 +54,7 @@ __global__ void k_csr_fill(const int* ca, const int* cb, const int* off, int* fi
   }
 }
 __global__ void k_csr_sort(int n, const int* off, int* ent, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int s = off[i], e = off[i + 1];
@@ -69,12 +73,12 @@ __global__ void k_csr_sort(int n, const int* off, int* ent, const Ctl* ctl) {
 void csr_launch(rg_system* s) {
   const int bs = 256;
   cudaStream_t st = s->stream;
-  RGL k_csr_zero<<<grid_for(s->n + 1, bs), bs, 0, st>>>(s->csr.cnt, s->csr.fill, s->n, s->d_ctl);
-  RGL k_csr_count<<<grid_for(s->ccap, bs), bs, 0, st>>>(s->con.a, s->con.b, s->csr.cnt, s->d_ctl);
+  RGL launch_dep(k_csr_zero, grid_for(s->n + 1, bs), bs, st, s->csr.cnt, s->csr.fill, s->n, s->d_ctl);
+  RGL launch_dep(k_csr_count, grid_for(s->ccap, bs), bs, st, s->con.a, s->con.b, s->csr.cnt, s->d_ctl);
   s->scan.run(s->csr.cnt, s->csr.off, detector_n_dev(s), &s->d_ctl->err, st);
-  RGL k_csr_fill<<<grid_for(s->ccap, bs), bs, 0, st>>>(s->con.a, s->con.b, s->csr.off, s->csr.fill,
+  RGL launch_dep(k_csr_fill, grid_for(s->ccap, bs), bs, st, s->con.a, s->con.b, s->csr.off, s->csr.fill,
                                                    s->csr.ent, s->d_ctl);
-  RGL k_csr_sort<<<grid_for(s->n, bs), bs, 0, st>>>(s->n, s->csr.off, s->csr.ent, s->d_ctl);
+  RGL launch_dep(k_csr_sort, grid_for(s->n, bs), bs, st, s->n, s->csr.off, s->csr.ent, s->d_ctl);
 }
 
 // ---------------------------------------------------------------------------
@@ -97,6 +101,7 @@ __device__ inline int lower_bound_u64(const unsigned long long* k, int n, unsign
 // all); the force kernel that follows clears the touched ones.  fr is the
 // frame this evaluation opens (the force kernel advances ctl->frame).
 __global__ void k_hist_keep_init(const long long* hframe, int* kept, int hm, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   const int H = ctl->hist_n;
   const long long fr = ctl->frame + 1;
@@ -110,6 +115,7 @@ __global__ void k_hist_merge(const int* ca, const int* cb, const int* touched, c
                              const long long* oframe, const int* kept, const int* koff,
                              unsigned long long* nkey, double* nval, long long* nframe, int cap,
                              int ccap, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   const int C = ctl->contacts, H = ctl->hist_n;
   const int T = toff[C], K = koff[H];
@@ -149,6 +155,7 @@ __global__ void k_hist_merge(const int* ca, const int* cb, const int* touched, c
   }
 }
 __global__ void k_hist_finish(const int* toff, const int* koff, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   int T = toff[ctl->contacts], K = koff[ctl->hist_n];
   ctl->hist_n = T + K;
@@ -199,6 +206,7 @@ __device__ inline void st_cf(const ForceIO& io, int c, d3 fa, d3 ta, d3 fb, d3 t
 }
 
 __global__ void k_soft_forces(State st, rg_config cfg, ForceIO io, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   const int C = ctl->contacts, H = ctl->hist_n;
   eval_begin(ctl);
@@ -303,6 +311,7 @@ __global__ void k_soft_forces(State st, rg_config cfg, ForceIO io, Ctl* ctl) {
 }
 
 __global__ void k_hm_forces(State st, rg_config cfg, ForceIO io, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   const int C = ctl->contacts, H = ctl->hist_n;
   eval_begin(ctl);
@@ -387,6 +396,7 @@ __global__ void k_hm_forces(State st, rg_config cfg, ForceIO io, Ctl* ctl) {
 // f_i += Σ addends in contact order (the reference's sequential order).
 __global__ void k_body_reduce(State st, const int* off, const int* ent, const double* cf, int ccap,
                               const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
     if (off[i] == off[i + 1]) continue;
@@ -399,6 +409,7 @@ __global__ void k_body_reduce(State st, const int* off, const int* ent, const do
 
 // Cylinder wall of the soft model on every dynamic body (soft_wall_apply).
 __global__ void k_soft_wall(State st, rg_config cfg, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   const d3 ax = soft_wall_axis(cfg);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
@@ -412,6 +423,7 @@ __global__ void k_soft_wall(State st, rg_config cfg, const Ctl* ctl) {
 // Deterministic potential-energy sum: fixed-shape two-level reduction.
 constexpr int kPeBlocks = 64;
 __global__ void k_pe_partial(const double* pe, double* part, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   __shared__ double sm[32];
   const int C = ctl->contacts;
@@ -427,6 +439,7 @@ __global__ void k_pe_partial(const double* pe, double* part, const Ctl* ctl) {
   }
 }
 __global__ void k_pe_final(const double* part, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   double v = threadIdx.x < kPeBlocks ? part[threadIdx.x] : 0.0;
   v = warp_sum(v);
@@ -458,24 +471,24 @@ void force_eval_launch(rg_system* s, EvalTail tail, bool seg_ready) {
   History& H = s->hist;
   const int cur = H.cur, nxt = 1 - H.cur;
   const int gc = grid_for(s->ccap, bs);
-  RGL k_hist_keep_init<<<grid_for(H.cap, bs), bs, 0, st>>>(H.frame[cur], H.kept, hm ? 1 : 0, s->d_ctl);
+  RGL launch_dep(k_hist_keep_init, grid_for(H.cap, bs), bs, st, H.frame[cur], H.kept, hm ? 1 : 0, s->d_ctl);
   ForceIO io;
   io.ca = s->con.a; io.cb = s->con.b; io.g = s->con.g; io.ccap = s->ccap;
   io.hkey = H.key[cur]; io.kept = H.kept; io.hval = H.val[cur]; io.hcap = H.cap;
   io.newval = H.newval; io.touched = H.touched; io.cf = s->d_cf;
   io.pe = s->d_cf + 12 * (size_t)s->ccap;
   if (hm) {
-    RGL k_hm_forces<<<gc, bs, 0, st>>>(s->st, c, io, s->d_ctl);
+    RGL launch_dep(k_hm_forces, gc, bs, st, s->st, c, io, s->d_ctl);
   } else {
-    RGL k_soft_forces<<<gc, bs, 0, st>>>(s->st, c, io, s->d_ctl);
+    RGL launch_dep(k_soft_forces, gc, bs, st, s->st, c, io, s->d_ctl);
   }
   // history merge
   s->scan.run(H.touched, H.touched_off, &s->d_ctl->contacts, &s->d_ctl->err, st);
   s->scan.run(H.kept, H.kept_off, &s->d_ctl->hist_n, &s->d_ctl->err, st);
-  RGL k_hist_merge<<<gc, bs, 0, st>>>(s->con.a, s->con.b, H.touched, H.touched_off, H.newval, H.key[cur],
+  RGL launch_dep(k_hist_merge, gc, bs, st, s->con.a, s->con.b, H.touched, H.touched_off, H.newval, H.key[cur],
                                   H.val[cur], H.frame[cur], H.kept, H.kept_off, H.key[nxt], H.val[nxt],
                                   H.frame[nxt], H.cap, s->ccap, s->d_ctl);
-  RGL k_hist_finish<<<1, 1, 0, st>>>(H.touched_off, H.kept_off, s->d_ctl);
+  RGL launch_dep(k_hist_finish, 1, 1, st, H.touched_off, H.kept_off, s->d_ctl);
   H.cur = nxt;
   const bool wall = !hm && c.cylinder_enabled;
   if (tail == EvalTail::kHalfPos) {
@@ -485,15 +498,15 @@ void force_eval_launch(rg_system* s, EvalTail tail, bool seg_ready) {
   if (tail == EvalTail::kSecondHalf) {
     reduce_kick_launch(s, wall);
   } else {
-    RGL k_body_reduce<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, s->csr.off, s->csr.ent, s->d_cf, s->ccap,
+    RGL launch_dep(k_body_reduce, grid_for(s->n, bs), bs, st, s->st, s->csr.off, s->csr.ent, s->d_cf, s->ccap,
                                                      s->d_ctl);
     if (wall) {
-      RGL k_soft_wall<<<grid_for(s->n, bs), bs, 0, st>>>(s->st, c, s->d_ctl);
+      RGL launch_dep(k_soft_wall, grid_for(s->n, bs), bs, st, s->st, c, s->d_ctl);
     }
   }
   double* part = s->d_cf + 13 * (size_t)s->ccap;
-  RGL k_pe_partial<<<kPeBlocks, 256, 0, st>>>(io.pe, part, s->d_ctl);
-  RGL k_pe_final<<<1, 64, 0, st>>>(part, s->d_ctl);
+  RGL launch_dep(k_pe_partial, kPeBlocks, 256, st, io.pe, part, s->d_ctl);
+  RGL launch_dep(k_pe_final, 1, 64, st, part, s->d_ctl);
 }
 
 }  // namespace rg

@@ -51,6 +51,7 @@ struct DriftOut {
 __global__ void __launch_bounds__(256, RG_BODY_MIN_BLOCKS)
     k_reduce_drift(State st, Box box, rg_config cfg, const int* off, const int* ent, const double* cf,
                    int ccap, int wall, DriftOut o, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   __shared__ double sm[32], sm2[32];
   const d3 g{cfg.gravity[0], cfg.gravity[1], cfg.gravity[2]};
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(256, RG_BODY_MIN_BLOCKS)
 __global__ void __launch_bounds__(256, RG_BODY_MIN_BLOCKS)
     k_reduce_kick(State st, rg_config cfg, const int* off, const int* ent, const double* cf, int ccap,
                   int wall, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   const d3 g{cfg.gravity[0], cfg.gravity[1], cfg.gravity[2]};
   const double hdt = 0.5 * cfg.dt;
@@ -144,6 +146,7 @@ __global__ void __launch_bounds__(256, RG_BODY_MIN_BLOCKS)
 }
 
 __global__ void k_clear_forces(State st, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
     st.f.st(i, mk3(0, 0, 0));
@@ -152,6 +155,7 @@ __global__ void k_clear_forces(State st, const Ctl* ctl) {
 }
 
 __global__ void k_nsc_free_flight(State st, rg_config cfg, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   const d3 g{cfg.gravity[0], cfg.gravity[1], cfg.gravity[2]};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x)
@@ -159,6 +163,7 @@ __global__ void k_nsc_free_flight(State st, rg_config cfg, const Ctl* ctl) {
 }
 
 __global__ void k_nsc_position_update(State st, rg_config cfg, Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   int bad = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x)
@@ -167,6 +172,7 @@ __global__ void k_nsc_position_update(State st, rg_config cfg, Ctl* ctl) {
 }
 
 __global__ void k_wrap_clear(State st, Box box, const Ctl* ctl) {
+  griddep_wait();
   if (ctl->err) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x)
     wrap_clear_body(st, box, i);
@@ -181,24 +187,24 @@ void reduce_drift_launch(rg_system* s, bool wall) {
   o.ref = d.all_pairs ? nullptr : d.ref;
   o.ref2 = (d.all_pairs || !d.near_cnt) ? nullptr : d.ref2;
   o.skin = d.skin;
-  RGL k_reduce_drift<<<body_grid(s), 256, 0, s->stream>>>(s->st, s->box, s->cfg, s->csr.off, s->csr.ent,
+  RGL launch_dep(k_reduce_drift, body_grid(s), 256, s->stream, s->st, s->box, s->cfg, s->csr.off, s->csr.ent,
                                                           s->d_cf, s->ccap, wall ? 1 : 0, o, s->d_ctl);
 }
 void reduce_kick_launch(rg_system* s, bool wall) {
-  RGL k_reduce_kick<<<body_grid(s), 256, 0, s->stream>>>(s->st, s->cfg, s->csr.off, s->csr.ent, s->d_cf,
+  RGL launch_dep(k_reduce_kick, body_grid(s), 256, s->stream, s->st, s->cfg, s->csr.off, s->csr.ent, s->d_cf,
                                                          s->ccap, wall ? 1 : 0, s->d_ctl);
 }
 void clear_forces_launch(rg_system* s) {
-  RGL k_clear_forces<<<body_grid(s), 256, 0, s->stream>>>(s->st, s->d_ctl);
+  RGL launch_dep(k_clear_forces, body_grid(s), 256, s->stream, s->st, s->d_ctl);
 }
 void nsc_free_flight_launch(rg_system* s) {
-  RGL k_nsc_free_flight<<<body_grid(s), 256, 0, s->stream>>>(s->st, s->cfg, s->d_ctl);
+  RGL launch_dep(k_nsc_free_flight, body_grid(s), 256, s->stream, s->st, s->cfg, s->d_ctl);
 }
 void nsc_position_update_launch(rg_system* s) {
-  RGL k_nsc_position_update<<<body_grid(s), 256, 0, s->stream>>>(s->st, s->cfg, s->d_ctl);
+  RGL launch_dep(k_nsc_position_update, body_grid(s), 256, s->stream, s->st, s->cfg, s->d_ctl);
 }
 void wrap_launch(rg_system* s) {
-  RGL k_wrap_clear<<<body_grid(s), 256, 0, s->stream>>>(s->st, s->box, s->d_ctl);
+  RGL launch_dep(k_wrap_clear, body_grid(s), 256, s->stream, s->st, s->box, s->d_ctl);
 }
 
 }  // namespace rg

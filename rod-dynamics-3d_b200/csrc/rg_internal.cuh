@@ -247,6 +247,25 @@ extern long long g_launches;
 // `if (c) RGL k<<<...>>>(...)` guards the count and the launch together.
 #define RGL ++::rg::g_launches,
 
+// Launches k with programmatic stream serialization: the grid may be
+// scheduled while the previous kernel in the stream drains, which hides the
+// launch gap between the short dependent kernels of a step (inside a CUDA
+// graph as well).  k must call griddep_wait() before it touches memory.
+template <typename... K, typename... A>
+inline cudaError_t launch_dep(void (*k)(K...), unsigned grid, unsigned block, cudaStream_t st, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, static_cast<A&&>(args)...);
+}
+
 enum Stage { ST_INTEGRATE = 0, ST_DETECT, ST_COLOR, ST_MANIFOLDS, ST_PSOR, ST_PROJECT, ST_FORCES, ST_OTHER };
 
 inline int prof_event(rg_system* s) {
