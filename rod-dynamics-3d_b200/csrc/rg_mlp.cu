@@ -4,10 +4,11 @@
 // last-step impulses only (src/physics/nsc_contact.cpp:305-317, :646-654).
 // The network (rg_mlp_dev.cuh) is trained on records of converged impulses
 // that the plain PSOR path itself produces (rg_mlp_record), with this file's
-// own forward and backward kernels: a strided, shared-memory-tiled GEMM on
-// tensor cores (mma.sync m16n8k16, BF16 operands, FP32 accumulation), SiLU
-// and loss kernels, and Adam on FP32 master weights.  BF16 copies of the
-// weights feed both training and the in-step inference.
+// own kernels: one fused forward + loss + backward + weight-gradient kernel
+// per minibatch on tensor cores (mma.sync m16n8k16, BF16 operands, FP32
+// accumulation) and one kernel that sums the blocks' partial gradients and
+// applies Adam to the FP32 master weights.  BF16 copies of the weights feed
+// both training and the in-step inference.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -20,180 +21,460 @@
 namespace rg {
 
 // ---------------------------------------------------------------------------
-// GEMM: C[M x N] (FP32) = A[M x K] * B[K x N] (+ C), A and B BF16 with
-// arbitrary element strides: A(m,k) = A[m*sam + k*sak], B(k,n) = B[k*sbk + n*sbn].
-// Block 128 threads (4 warps) computes a 64 x 64 tile, K in steps of 32.
+// Training: one fused kernel per minibatch.  A block of kTrainWarps warps
+// takes tiles of kTrainRows rows (16 per warp) and runs, for its rows, the
+// forward pass (pre-activations Z kept in shared memory, activations in
+// registers: the accumulator fragment of a layer is the A fragment of the
+// next), the loss, the backward pass (dH = dZ W with W read transposed from
+// shared memory, dZ = dH * silu'(Z)) and the block's share of the weight
+// gradients dW = dZ^T H as block-level mma.sync products over the tile's
+// rows (H recomputed from Z).  Each block writes its partial gradient (and
+// loss) to its own slice of a partial buffer, summing over its tiles in a
+// fixed order; one reduction kernel then adds the slices in block order
+// (deterministic) and applies Adam and the BF16 weight copies.
 // ---------------------------------------------------------------------------
-constexpr int kGM = 64, kGN = 64, kGK = 32, kGPad = 8;
+constexpr int kTrainWarps = 4;
+constexpr int kTrainThreads = 32 * kTrainWarps;
+constexpr int kTrainRows = 16 * kTrainWarps;      // 64 rows per tile
+constexpr int kZLd = kMlpH + 8;                   // FP32 pre-activation rows (136)
+constexpr int kXLd = kW1Pad + 8;                  // BF16 input rows (24)
+constexpr int kDyLd = 16;                         // BF16 output-gradient rows
+constexpr int kGradParams = kOffInMean;           // trained parameters
+constexpr int kTrainMaxBlocks = 296;
 
-__global__ void __launch_bounds__(128) k_gemm_bf16(const __nv_bfloat16* A, long sam, long sak,
-                                                   const __nv_bfloat16* B, long sbk, long sbn, float* C,
-                                                   long ldc, int M, int N, int K, int accumulate) {
-  __shared__ __align__(16) __nv_bfloat16 As[kGM][kGK + kGPad];
-  __shared__ __align__(16) __nv_bfloat16 Bs[kGN][kGK + kGPad];  // [n][k]
-  const int m0 = blockIdx.y * kGM, n0 = blockIdx.x * kGN;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+// Shared-memory carve-up of the training kernel (byte offsets, 16-aligned).
+constexpr int kTsW2 = 0;
+constexpr int kTsW3 = kTsW2 + 2 * kStageWh;
+constexpr int kTsSmall = kTsW3 + 2 * kStageWh;                         // W1, W4, floats (MlpStage)
+constexpr int kTsX = kTsSmall + ((kStageSmallBytes + 15) / 16) * 16;
+constexpr int kTsZ = kTsX + 2 * kTrainRows * kXLd;                     // Z1, Z2, Z3
+constexpr int kTsDzA = kTsZ + 3 * 4 * kTrainRows * kZLd;
+constexpr int kTsDzB = kTsDzA + 2 * kTrainRows * kWhLd;
+constexpr int kTsDy = kTsDzB + 2 * kTrainRows * kWhLd;
+constexpr int kTsBias = kTsDy + 2 * kTrainRows * kDyLd;                // [warp][b1|b2|b3|b4(8)]
+constexpr int kTsLoss = kTsBias + 4 * kTrainWarps * (3 * kMlpH + 8);
+constexpr int kTrainSmem = kTsLoss + 16 * kTrainWarps;
+static_assert(kTrainSmem <= 227 * 1024, "training kernel shared memory");
+static_assert(kTsSmall % 16 == 0 && kTsX % 16 == 0 && kTsZ % 16 == 0 && kTsDzA % 16 == 0 && kTsDzB % 16 == 0 &&
+                  kTsDy % 16 == 0 && kTsBias % 16 == 0,
+              "16-byte aligned regions");
+
+struct TrainSmem {
+  __nv_bfloat16 *w2, *w3;  // [128][kWhLd]
+  MlpStage st;             // W1 [128][kW1Ld], W4 [8][kWhLd], biases and scales
+  __nv_bfloat16* x;        // [64][kXLd] normalised inputs (columns 8..15 zero)
+  float* z[3];             // [64][kZLd] pre-activations of layers 1..3
+  __nv_bfloat16 *dza, *dzb;  // [64][kWhLd] BF16 dZ of two layers
+  __nv_bfloat16* dy;       // [64][kDyLd] BF16 dY (columns 3..15 zero)
+  float* bias;             // [warp][3 * 128 + 8] bias-gradient partial sums
+  float* loss;             // [warp]
+};
+__device__ inline TrainSmem train_smem(unsigned char* b) {
+  TrainSmem s;
+  s.w2 = reinterpret_cast<__nv_bfloat16*>(b + kTsW2);
+  s.w3 = reinterpret_cast<__nv_bfloat16*>(b + kTsW3);
+  s.st = mlp_stage_at(b + kTsSmall);
+  s.x = reinterpret_cast<__nv_bfloat16*>(b + kTsX);
+  for (int l = 0; l < 3; ++l) s.z[l] = reinterpret_cast<float*>(b + kTsZ) + (size_t)l * kTrainRows * kZLd;
+  s.dza = reinterpret_cast<__nv_bfloat16*>(b + kTsDzA);
+  s.dzb = reinterpret_cast<__nv_bfloat16*>(b + kTsDzB);
+  s.dy = reinterpret_cast<__nv_bfloat16*>(b + kTsDy);
+  s.bias = reinterpret_cast<float*>(b + kTsBias);
+  s.loss = reinterpret_cast<float*>(b + kTsLoss);
+  return s;
+}
+
+__device__ inline unsigned short bf16_bits(__nv_bfloat16 v) { return *reinterpret_cast<unsigned short*>(&v); }
+// Two BF16 values from different rows packed into one fragment register.
+__device__ inline unsigned pack2(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  return (unsigned)bf16_bits(lo) | ((unsigned)bf16_bits(hi) << 16);
+}
+// B fragment of W^T for the backward product dH = dZ W (W row-major
+// [out][in] with leading dimension ldw): k = out (k-tile kt), n = in
+// (n-tile nt); elements of a register come from two rows of W.
+__device__ inline void load_bt(const __nv_bfloat16* W, int ldw, int nt, int kt, int lane, unsigned& b0,
+                               unsigned& b1) {
   const int g = lane >> 2, t = lane & 3;
-  float acc[2][4][4];
-  for (int i = 0; i < 2; ++i)
-    for (int j = 0; j < 4; ++j)
-      for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0f;
-  const __nv_bfloat16 zero = __float2bfloat16(0.0f);
-  for (int k0 = 0; k0 < K; k0 += kGK) {
-    for (int e = threadIdx.x; e < kGM * kGK; e += blockDim.x) {
-      int mm = e / kGK, kk = e % kGK;
-      int m = m0 + mm, k = k0 + kk;
-      As[mm][kk] = (m < M && k < K) ? A[m * sam + k * sak] : zero;
-    }
-    for (int e = threadIdx.x; e < kGN * kGK; e += blockDim.x) {
-      int nn = e / kGK, kk = e % kGK;
-      int n = n0 + nn, k = k0 + kk;
-      Bs[nn][kk] = (n < N && k < K) ? B[k * sbk + n * sbn] : zero;
-    }
-    __syncthreads();
+  const int n = nt * 8 + g, k = kt * 16 + 2 * t;
+  b0 = pack2(W[(size_t)k * ldw + n], W[(size_t)(k + 1) * ldw + n]);
+  b1 = pack2(W[(size_t)(k + 8) * ldw + n], W[(size_t)(k + 9) * ldw + n]);
+}
+__device__ inline float silu_grad(float z) {
+  const float s = 1.0f / (1.0f + __expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+// Accumulator fragments (16 n-tiles) -> A fragments of the next product.
+__device__ inline void acc_to_a(const float (&c)[16][4], unsigned (&a)[8][4], bool act) {
 #pragma unroll
-    for (int ks = 0; ks < kGK; ks += 16) {
-      unsigned a[2][4], b[4][2];
+  for (int kk = 0; kk < 8; ++kk) {
+    const float* p = c[2 * kk];
+    const float* q = c[2 * kk + 1];
+    if (act) {
+      a[kk][0] = pack_bf16(silu(p[0]), silu(p[1]));
+      a[kk][1] = pack_bf16(silu(p[2]), silu(p[3]));
+      a[kk][2] = pack_bf16(silu(q[0]), silu(q[1]));
+      a[kk][3] = pack_bf16(silu(q[2]), silu(q[3]));
+    } else {
+      a[kk][0] = pack_bf16(p[0], p[1]);
+      a[kk][1] = pack_bf16(p[2], p[3]);
+      a[kk][2] = pack_bf16(q[0], q[1]);
+      a[kk][3] = pack_bf16(q[2], q[3]);
+    }
+  }
+}
+// Stores a warp's 16 x 128 FP32 accumulator block at rows lr0.. of Z.
+__device__ inline void store_z(float* z, int lr0, const float (&c)[16][4], int lane) {
+  const int g = lane >> 2, t = lane & 3;
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int r = wm + i * 16 + g;
-        a[i][0] = *reinterpret_cast<const unsigned*>(&As[r][ks + 2 * t]);
-        a[i][1] = *reinterpret_cast<const unsigned*>(&As[r + 8][ks + 2 * t]);
-        a[i][2] = *reinterpret_cast<const unsigned*>(&As[r][ks + 2 * t + 8]);
-        a[i][3] = *reinterpret_cast<const unsigned*>(&As[r + 8][ks + 2 * t + 8]);
+  for (int nt = 0; nt < 16; ++nt) {
+    const int col = nt * 8 + 2 * t;
+    *reinterpret_cast<float2*>(&z[(size_t)(lr0 + g) * kZLd + col]) = make_float2(c[nt][0], c[nt][1]);
+    *reinterpret_cast<float2*>(&z[(size_t)(lr0 + g + 8) * kZLd + col]) = make_float2(c[nt][2], c[nt][3]);
+  }
+}
+
+__device__ inline float warp_sum_f(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// Partial gradient slice of a block: '=' on its first tile, '+=' after.
+__device__ inline void part_put(float* p, int i, float v, bool first) { p[i] = first ? v : p[i] + v; }
+
+// Block-level weight gradient dW[o][i] = Σ_r dZ[r][o] H[r][i] over the
+// tile's 64 rows: output rows o in m-tiles [0, mtiles) (warp w takes m-tiles
+// w, w + 4, ...), input columns [0, 8 * NTN).  dZ: BF16 rows of leading
+// dimension ldz.  H: the BF16 copy of silu(Z) (Z FP32 [64][kZLd]) or, when
+// zs is null, the BF16 inputs xs [64][kXLd].  Rows o < nrows and columns
+// i < ncols go to part[off + o * ncols + i].
+template <int NTN>
+__device__ inline void block_dw(const __nv_bfloat16* dz, int ldz, int mtiles, int nrows, const float* zs,
+                                const __nv_bfloat16* xs, int ncols, float* part, int off, bool first, int warp,
+                                int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  for (int mt = warp; mt < mtiles; mt += kTrainWarps) {
+    const int m0 = mt * 16;
+    float c[NTN][4];
+#pragma unroll
+    for (int j = 0; j < NTN; ++j) c[j][0] = c[j][1] = c[j][2] = c[j][3] = 0.0f;
+#pragma unroll
+    for (int ks = 0; ks < kTrainRows / 16; ++ks) {
+      const int r = ks * 16 + 2 * t;
+      const __nv_bfloat16* d0 = dz + (size_t)r * ldz + m0 + g;
+      const unsigned a0 = pack2(d0[0], d0[ldz]);
+      const unsigned a1 = pack2(d0[8], d0[ldz + 8]);
+      const unsigned a2 = pack2(d0[8 * ldz], d0[9 * ldz]);
+      const unsigned a3 = pack2(d0[8 * ldz + 8], d0[9 * ldz + 8]);
+#pragma unroll
+      for (int j = 0; j < NTN; ++j) {
+        const int n = j * 8 + g;
+        unsigned b0, b1;
+        if (zs) {
+          const float* z0 = zs + (size_t)r * kZLd + n;
+          b0 = pack_bf16(silu(z0[0]), silu(z0[kZLd]));
+          b1 = pack_bf16(silu(z0[8 * kZLd]), silu(z0[9 * kZLd]));
+        } else {
+          const __nv_bfloat16* x0 = xs + (size_t)r * kXLd + n;
+          b0 = pack2(x0[0], x0[kXLd]);
+          b1 = pack2(x0[8 * kXLd], x0[9 * kXLd]);
+        }
+        mma_bf16(c[j], a0, a1, a2, a3, b0, b1);
       }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int c = wn + j * 8 + g;
-        b[j][0] = *reinterpret_cast<const unsigned*>(&Bs[c][ks + 2 * t]);
-        b[j][1] = *reinterpret_cast<const unsigned*>(&Bs[c][ks + 2 * t + 8]);
-      }
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], a[i][0], a[i][1], a[i][2], a[i][3], b[j][0], b[j][1]);
     }
-    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NTN; ++j) {
+      const int col = j * 8 + 2 * t;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int o = m0 + g + (e >= 2 ? 8 : 0), i = col + (e & 1);
+        if (o < nrows && i < ncols) part_put(part, off + o * ncols + i, c[j][e], first);
+      }
+    }
+  }
+}
+
+// Column sums over a warp's 16 rows of a 16 x 128 FP32 fragment block,
+// added to sums[0..127] ('=' on the block's first tile); lanes with g = 0
+// write.
+__device__ inline void warp_colsum_acc(const float (&c)[16][4], float* sums, int lane, bool first) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc) {
+      float v = c[nt][cc] + c[nt][2 + cc];
+      v += __shfl_xor_sync(0xffffffffu, v, 4);
+      v += __shfl_xor_sync(0xffffffffu, v, 8);
+      v += __shfl_xor_sync(0xffffffffu, v, 16);
+      if (g == 0) {
+        float* s = &sums[nt * 8 + 2 * t + cc];
+        *s = first ? v : *s + v;
+      }
+    }
+  }
+}
+
+// dZ = dH * silu'(Z) in place on the accumulator block (Z rows lr0..), and
+// its BF16 copy into dzs.
+__device__ inline void dz_from_dh(float (&c)[16][4], const float* z, __nv_bfloat16* dzs, int lr0, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+    const int col = nt * 8 + 2 * t;
+    const float2 z0 = *reinterpret_cast<const float2*>(&z[(size_t)(lr0 + g) * kZLd + col]);
+    const float2 z1 = *reinterpret_cast<const float2*>(&z[(size_t)(lr0 + g + 8) * kZLd + col]);
+    c[nt][0] *= silu_grad(z0.x);
+    c[nt][1] *= silu_grad(z0.y);
+    c[nt][2] *= silu_grad(z1.x);
+    c[nt][3] *= silu_grad(z1.y);
+    *reinterpret_cast<unsigned*>(&dzs[(size_t)(lr0 + g) * kWhLd + col]) = pack_bf16(c[nt][0], c[nt][1]);
+    *reinterpret_cast<unsigned*>(&dzs[(size_t)(lr0 + g + 8) * kWhLd + col]) = pack_bf16(c[nt][2], c[nt][3]);
+  }
+}
+// dH = dZ W for a warp's 16 rows: dZ A fragments from dzs (BF16 rows lr0..),
+// W staged [out][kWhLd].
+__device__ inline void dh_product(const __nv_bfloat16* dzs, int lr0, const __nv_bfloat16* W, float (&c)[16][4],
+                                  int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0f;
+#pragma unroll
+  for (int kt = 0; kt < 8; ++kt) {
+    const __nv_bfloat16* r0 = dzs + (size_t)(lr0 + g) * kWhLd + kt * 16 + 2 * t;
+    const __nv_bfloat16* r1 = r0 + 8 * kWhLd;
+    const unsigned a0 = *reinterpret_cast<const unsigned*>(r0), a1 = *reinterpret_cast<const unsigned*>(r1);
+    const unsigned a2 = *reinterpret_cast<const unsigned*>(r0 + 8), a3 = *reinterpret_cast<const unsigned*>(r1 + 8);
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt) {
+      unsigned b0, b1;
+      load_bt(W, kWhLd, nt, kt, lane, b0, b1);
+      mma_bf16(c[nt], a0, a1, a2, a3, b0, b1);
+    }
+  }
+}
+// Forward through one hidden layer from A fragments a (16 x 128) with W
+// staged [out][kWhLd]: c = a W^T + bias (FP32).
+__device__ inline void fwd_product(const unsigned (&a)[8][4], const __nv_bfloat16* W, const float* bias,
+                                   float (&c)[16][4], int lane) {
+  const int t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+    const float bl = bias[nt * 8 + 2 * t], bh = bias[nt * 8 + 2 * t + 1];
+    c[nt][0] = bl; c[nt][1] = bh; c[nt][2] = bl; c[nt][3] = bh;
   }
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int kt = 0; kt < 8; ++kt) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int nt = 0; nt < 16; ++nt) {
+      unsigned b0, b1;
+      load_b(W, kWhLd, nt, kt, lane, b0, b1);
+      mma_bf16(c[nt], a[kt][0], a[kt][1], a[kt][2], a[kt][3], b0, b1);
+    }
+  }
+}
+
+// One minibatch: rows [0, n) of feat/tgt (row-major [n][8] / [n][3]),
+// gathered by idx when given.  Block b handles tiles b, b + gridDim.x, ...
+// and leaves its partial gradient in part[b * kGradParams ...] and its
+// partial loss (Σ squared error) in loss_part[b].
+__global__ void __launch_bounds__(kTrainThreads, 1)
+    k_mlp_train_fb(MlpDev M, const float* feat, const float* tgt, const int* idx, int n, float* part,
+                   float* loss_part) {
+  extern __shared__ __align__(16) unsigned char tsm[];
+  const TrainSmem S = train_smem(tsm);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  stage_bf16(S.w2, kWhLd, M.w2, kMlpH, kMlpH);
+  stage_bf16(S.w3, kWhLd, M.w3, kMlpH, kMlpH);
+  stage_small(S.st, M);
+  stage_wait();
+  __syncthreads();
+  const MlpSmall q = S.st.small();
+  float* mypart = part + (size_t)blockIdx.x * kGradParams;
+  const int ntiles = (n + kTrainRows - 1) / kTrainRows;
+  const float inv_n3 = 1.0f / (float)(n * kMlpOut);
+  const int lr0 = warp * 16;
+  float* bsum = S.bias + warp * (3 * kMlpH + 8);
+  float lsum = 0.0f;
+  bool first = true;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, first = false) {
+    const int row0 = tile * kTrainRows;
+    // ---- forward (per warp, rows lr0..lr0+15 of the tile) ----
+    unsigned x0, x1;
+    {
+      float v[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        int m = m0 + wm + i * 16 + g + (r >= 2 ? 8 : 0);
-        int n = n0 + wn + j * 8 + 2 * t + (r & 1);
-        if (m < M && n < N) {
-          float v = acc[i][j][r];
-          if (accumulate) v += C[m * ldc + n];
-          C[m * ldc + n] = v;
+      for (int rr = 0; rr < 2; ++rr) {
+        const int lr = lr0 + g + 8 * rr, r = row0 + lr;
+        const int rid = r < n ? (idx ? idx[r] : r) : 0;
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int k = 2 * t + cc;
+          v[rr * 2 + cc] = r < n ? (feat[(size_t)rid * kMlpIn + k] - q.in_mean[k]) * q.in_scale[k] : 0.0f;
+        }
+        *reinterpret_cast<unsigned*>(&S.x[(size_t)lr * kXLd + 2 * t]) = pack_bf16(v[rr * 2], v[rr * 2 + 1]);
+        *reinterpret_cast<unsigned*>(&S.x[(size_t)lr * kXLd + 8 + 2 * t]) = 0u;
+      }
+      x0 = pack_bf16(v[0], v[1]);
+      x1 = pack_bf16(v[2], v[3]);
+    }
+    unsigned a[8][4];
+    float c[16][4];
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt) {
+      const float bl = q.b1[nt * 8 + 2 * t], bh = q.b1[nt * 8 + 2 * t + 1];
+      c[nt][0] = bl; c[nt][1] = bh; c[nt][2] = bl; c[nt][3] = bh;
+      unsigned b0, b1;
+      load_b(S.st.w1, kW1Ld, nt, 0, lane, b0, b1);
+      mma_bf16(c[nt], x0, x1, 0u, 0u, b0, b1);
+    }
+    store_z(S.z[0], lr0, c, lane);
+    acc_to_a(c, a, true);
+    fwd_product(a, S.w2, q.b2, c, lane);
+    store_z(S.z[1], lr0, c, lane);
+    acc_to_a(c, a, true);
+    fwd_product(a, S.w3, q.b3, c, lane);
+    store_z(S.z[2], lr0, c, lane);
+    acc_to_a(c, a, true);
+    // output layer, loss and dY (outputs 2t, 2t + 1 of rows g, g + 8)
+    float dy[4];
+    {
+      float y[4];
+      const float bl = 2 * t < kMlpOut ? q.b4[2 * t] : 0.0f, bh = 2 * t + 1 < kMlpOut ? q.b4[2 * t + 1] : 0.0f;
+      y[0] = bl; y[1] = bh; y[2] = bl; y[3] = bh;
+#pragma unroll
+      for (int kt = 0; kt < 8; ++kt) {
+        unsigned b0, b1;
+        load_b(S.st.w4, kWhLd, 0, kt, lane, b0, b1);
+        mma_bf16(y, a[kt][0], a[kt][1], a[kt][2], a[kt][3], b0, b1);
+      }
+#pragma unroll
+      for (int rr = 0; rr < 2; ++rr) {
+        const int lr = lr0 + g + 8 * rr, r = row0 + lr;
+        const int rid = r < n ? (idx ? idx[r] : r) : 0;
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int o = 2 * t + cc;
+          float d = 0.0f;
+          if (o < kMlpOut && r < n) {
+            const float tn = (tgt[(size_t)rid * kMlpOut + o] - feat[(size_t)rid * kMlpIn + 4 + o]) / q.out_scale[o];
+            const float diff = y[rr * 2 + cc] - tn;
+            lsum += diff * diff;
+            d = 2.0f * diff * inv_n3;
+          }
+          dy[rr * 2 + cc] = d;
+        }
+        *reinterpret_cast<unsigned*>(&S.dy[(size_t)lr * kDyLd + 2 * t]) = pack_bf16(dy[rr * 2], dy[rr * 2 + 1]);
+        *reinterpret_cast<unsigned*>(&S.dy[(size_t)lr * kDyLd + 8 + 2 * t]) = 0u;
+      }
+    }
+    // ---- backward through the output layer: db4, dH3 = dY W4 ----
+    {
+#pragma unroll
+      for (int cc = 0; cc < 2; ++cc) {
+        float v = dy[cc] + dy[2 + cc];
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        v += __shfl_xor_sync(0xffffffffu, v, 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        if (g == 0) {
+          float* s = &bsum[3 * kMlpH + 2 * t + cc];
+          *s = first ? v : *s + v;
         }
       }
-}
-
-static void gemm(const __nv_bfloat16* A, long sam, long sak, const __nv_bfloat16* B, long sbk, long sbn, float* C,
-                 long ldc, int M, int N, int K, cudaStream_t st, int accumulate = 0) {
-  dim3 grid((N + kGN - 1) / kGN, (M + kGM - 1) / kGM);
-  RGL k_gemm_bf16<<<grid, 128, 0, st>>>(A, sam, sak, B, sbk, sbn, C, ldc, M, N, K, accumulate);
-}
-
-// ---------------------------------------------------------------------------
-// Elementwise kernels.
-// ---------------------------------------------------------------------------
-// X[b][0..15] = normalised features (8..15 zero), rows gathered by idx.
-__global__ void k_mlp_input(const float* feat, const int* idx, int n, const float* P, __nv_bfloat16* X) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * kW1Pad; e += gridDim.x * blockDim.x) {
-    int b = e / kW1Pad, k = e % kW1Pad;
+      const unsigned ya0 = pack_bf16(dy[0], dy[1]), ya1 = pack_bf16(dy[2], dy[3]);
+#pragma unroll
+      for (int nt = 0; nt < 16; ++nt) {
+        c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0f;
+        const int nn = nt * 8 + g;
+        const unsigned b0 = pack2(S.st.w4[(size_t)(2 * t) * kWhLd + nn], S.st.w4[(size_t)(2 * t + 1) * kWhLd + nn]);
+        mma_bf16(c[nt], ya0, ya1, 0u, 0u, b0, 0u);
+      }
+    }
+    // layer 3: dZ3 -> dza, db3; dH2 = dZ3 W3
+    dz_from_dh(c, S.z[2], S.dza, lr0, lane);
+    warp_colsum_acc(c, bsum + 2 * kMlpH, lane, first);
+    __syncwarp();
+    dh_product(S.dza, lr0, S.w3, c, lane);
+    // layer 2: dZ2 -> dzb, db2
+    dz_from_dh(c, S.z[1], S.dzb, lr0, lane);
+    warp_colsum_acc(c, bsum + kMlpH, lane, first);
+    __syncthreads();  // every warp's dZ3, dZ2 and dY are in shared memory
+    block_dw<16>(S.dza, kWhLd, kMlpH / 16, kMlpH, S.z[1], nullptr, kMlpH, mypart, kOffW3, first, warp, lane);
+    block_dw<16>(S.dy, kDyLd, 1, kMlpOut, S.z[2], nullptr, kMlpH, mypart, kOffW4, first, warp, lane);
+    __syncthreads();  // dza is free again
+    // layer 1: dH1 = dZ2 W2, dZ1 -> dza, db1
+    dh_product(S.dzb, lr0, S.w2, c, lane);
+    dz_from_dh(c, S.z[0], S.dza, lr0, lane);
+    warp_colsum_acc(c, bsum, lane, first);
+    __syncthreads();
+    block_dw<16>(S.dzb, kWhLd, kMlpH / 16, kMlpH, S.z[0], nullptr, kMlpH, mypart, kOffW2, first, warp, lane);
+    block_dw<2>(S.dza, kWhLd, kMlpH / 16, kMlpH, nullptr, S.x, kMlpIn, mypart, kOffW1, first, warp, lane);
+    __syncthreads();  // shared tiles are reused by the next tile
+  }
+  // bias gradients and loss: sum the warps' partial sums in warp order
+  lsum = warp_sum_f(lsum);
+  if (lane == 0) S.loss[warp] = lsum;
+  __syncthreads();
+  const bool any = blockIdx.x < ntiles;
+  for (int i = threadIdx.x; i < 3 * kMlpH + kMlpOut; i += blockDim.x) {
     float v = 0.0f;
-    if (k < kMlpIn) {
-      int r = idx ? idx[b] : b;
-      v = (feat[(size_t)r * kMlpIn + k] - P[kOffInMean + k]) * P[kOffInScale + k];
-    }
-    X[e] = __float2bfloat16(v);
+    if (any)
+      for (int w = 0; w < kTrainWarps; ++w) v += S.bias[w * (3 * kMlpH + 8) + i];
+    const int off = i < kMlpH ? kOffB1 + i : i < 2 * kMlpH ? kOffB2 + i - kMlpH
+                  : i < 3 * kMlpH ? kOffB3 + i - 2 * kMlpH : kOffB4 + i - 3 * kMlpH;
+    mypart[off] = v;
   }
-}
-// Z += bias; H = bf16(silu(Z)).
-__global__ void k_bias_silu(float* Z, const float* bias, int n, int w, __nv_bfloat16* H) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * w; e += gridDim.x * blockDim.x) {
-    float z = Z[e] + bias[e % w];
-    Z[e] = z;
-    H[e] = __float2bfloat16(silu(z));
-  }
-}
-// Output layer: Y = Z4 + b4 against the normalised impulse change
-// T = (λ - λ_prev) / s; dY = 2 (Y - T) / (n * 3); per-block loss sums.
-__global__ void k_out_loss(float* Z4, const float* P, const float* feat, const float* tgt, const int* idx, int n,
-                           float* dY, __nv_bfloat16* dYb, float* loss_part) {
-  __shared__ float sm[32];
-  float l = 0.0f;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * kW4Pad; e += gridDim.x * blockDim.x) {
-    int b = e / kW4Pad, o = e % kW4Pad;
-    float d = 0.0f;
-    if (o < kMlpOut) {
-      float y = Z4[e] + P[kOffB4 + o];
-      Z4[e] = y;
-      int r = idx ? idx[b] : b;
-      float tn = (tgt[(size_t)r * kMlpOut + o] - feat[(size_t)r * kMlpIn + 4 + o]) / P[kOffOutScale + o];
-      float diff = y - tn;
-      l += diff * diff;
-      d = 2.0f * diff / (float)(n * kMlpOut);
-    }
-    dY[e] = d;
-    dYb[e] = __float2bfloat16(d);
-  }
-  for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = l;
-  __syncthreads();
   if (threadIdx.x == 0) {
-    float s = 0.0f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sm[w];
-    loss_part[blockIdx.x] = s;
+    float l = 0.0f;
+    for (int w = 0; w < kTrainWarps; ++w) l += S.loss[w];
+    loss_part[blockIdx.x] = any ? l : 0.0f;
+  }
+  if (!any) {  // a block without a tile contributes zero weight gradients
+    for (int i = threadIdx.x; i < kGradParams; i += blockDim.x) {
+      const bool bias = (i >= kOffB1 && i < kOffW2) || (i >= kOffB2 && i < kOffW3) || (i >= kOffB3 && i < kOffW4) ||
+                        i >= kOffB4;
+      if (!bias) mypart[i] = 0.0f;
+    }
   }
 }
-// dZ = dH * silu'(Z), FP32 and BF16 copies.
-__global__ void k_silu_back(const float* dH, const float* Z, int n, float* dZ, __nv_bfloat16* dZb) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * kMlpH; e += gridDim.x * blockDim.x) {
-    float z = Z[e];
-    float s = 1.0f / (1.0f + __expf(-z));
-    float d = dH[e] * (s * (1.0f + z * (1.0f - s)));
-    dZ[e] = d;
-    dZb[e] = __float2bfloat16(d);
-  }
+
+// g_i = Σ_b part[b][i] in block order (deterministic), i < kGradParams.
+__device__ inline float grad_sum(const float* part, int nblk, int i) {
+  float g = 0.0f;
+  for (int b = 0; b < nblk; ++b) g += part[(size_t)b * kGradParams + i];
+  return g;
 }
-// db[c] = Σ_b dZ[b][c] for c < w_out (one block per column).
-__global__ void k_bias_grad(const float* dZ, int n, int w, int w_out, float* db) {
-  __shared__ float sm[32];
-  const int c = blockIdx.x;
-  if (c >= w_out) return;
-  float s = 0.0f;
-  for (int b = threadIdx.x; b < n; b += blockDim.x) s += dZ[(size_t)b * w + c];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float t = 0.0f;
-    for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) t += sm[w2];
-    db[c] = t;
-  }
+__global__ void k_mlp_grad_sum(const float* part, int nblk, float* G) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGradParams; i += gridDim.x * blockDim.x)
+    G[i] = grad_sum(part, nblk, i);
 }
-// Copies a padded gradient block ([rows][ldp]) into the parameter layout.
-__global__ void k_unpad(const float* src, int rows, int cols, int ldp, float* dst) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < rows * cols; e += gridDim.x * blockDim.x)
-    dst[e] = src[(e / cols) * ldp + (e % cols)];
-}
-// Adam on the network parameters [0, kOffInMean).
-__global__ void k_adam(float* P, const float* G, float* m, float* v, float lr, float b1, float b2, float eps,
-                       float bc1, float bc2) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kOffInMean; i += gridDim.x * blockDim.x) {
-    float g = G[i];
-    float mi = b1 * m[i] + (1.0f - b1) * g;
-    float vi = b2 * v[i] + (1.0f - b2) * g * g;
+// Adam on the trained parameters from the summed partial gradients, then
+// the BF16 weight copies the next minibatch and the in-step inference read
+// (their padding stays zero from the full copy).
+__global__ void k_mlp_adam(const float* part, int nblk, float* P, float* m, float* v, float lr, float b1, float b2,
+                           float eps, float bc1, float bc2, __nv_bfloat16* w1, __nv_bfloat16* w2,
+                           __nv_bfloat16* w3, __nv_bfloat16* w4) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGradParams; i += gridDim.x * blockDim.x) {
+    const float g = grad_sum(part, nblk, i);
+    const float mi = b1 * m[i] + (1.0f - b1) * g;
+    const float vi = b2 * v[i] + (1.0f - b2) * g * g;
     m[i] = mi;
     v[i] = vi;
-    P[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    const float p = P[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    P[i] = p;
+    const __nv_bfloat16 pb = __float2bfloat16(p);
+    if (i < kOffB1) {
+      w1[(i / kMlpIn) * kW1Pad + i % kMlpIn] = pb;
+    } else if (i >= kOffW2 && i < kOffB2) {
+      w2[i - kOffW2] = pb;
+    } else if (i >= kOffW3 && i < kOffB3) {
+      w3[i - kOffW3] = pb;
+    } else if (i >= kOffW4 && i < kOffB4) {
+      w4[i - kOffW4] = pb;
+    }
   }
 }
+
 // BF16 padded weight copies from the FP32 parameter vector.
 __global__ void k_weights_bf16(const float* P, __nv_bfloat16* w1, __nv_bfloat16* w2, __nv_bfloat16* w3,
                                __nv_bfloat16* w4) {
@@ -231,12 +512,11 @@ __global__ void k_mlp_infer(MlpDev M, const float* featT, int n, float* outT) {
 struct MlpHost {
   float* P = nullptr;              // FP32 parameters (kMlpParams)
   __nv_bfloat16* wb = nullptr;     // w1 | w2 | w3 | w4 (padded)
-  // training workspace (sized for cap rows)
-  int cap = 0;
-  __nv_bfloat16 *X = nullptr, *H1 = nullptr, *H2 = nullptr, *H3 = nullptr, *dZb = nullptr, *dYb = nullptr;
-  float *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *Z4 = nullptr, *dZ = nullptr, *dH = nullptr, *dY = nullptr;
-  float *G = nullptr, *Gpad = nullptr, *Am = nullptr, *Av = nullptr, *loss = nullptr;
-  int* idx = nullptr;
+  // training workspace
+  float *part = nullptr, *loss = nullptr;  // per-block partial gradients / losses
+  float *G = nullptr, *Am = nullptr, *Av = nullptr;
+  int* idx = nullptr;              // minibatch order of an epoch (n)
+  size_t nidx = 0;
   float *feat = nullptr, *tgt = nullptr;  // dataset on the device
   size_t nfeat = 0;
 };
@@ -276,90 +556,40 @@ static void refresh_bf16(rg_system* s) {
                                                  const_cast<__nv_bfloat16*>(M.w4));
 }
 
-static cudaError_t ensure_workspace(rg_system* s, int rows) {
+static cudaError_t ensure_workspace(rg_system* s) {
   MlpHost& H = host_of(s);
-  if (H.cap >= rows) return cudaSuccess;
-  cudaFree(H.X); cudaFree(H.H1); cudaFree(H.H2); cudaFree(H.H3); cudaFree(H.dZb); cudaFree(H.dYb);
-  cudaFree(H.Z1); cudaFree(H.Z2); cudaFree(H.Z3); cudaFree(H.Z4); cudaFree(H.dZ); cudaFree(H.dH);
-  cudaFree(H.dY); cudaFree(H.G); cudaFree(H.Gpad); cudaFree(H.Am); cudaFree(H.Av); cudaFree(H.loss);
-  cudaFree(H.idx);
-  H.cap = rows;
-  const size_t r = rows;
+  if (H.part) return cudaSuccess;
   cudaError_t e;
-  if ((e = cudaMalloc(&H.X, sizeof(__nv_bfloat16) * r * kW1Pad))) return e;
-  if ((e = cudaMalloc(&H.H1, sizeof(__nv_bfloat16) * r * kMlpH))) return e;
-  if ((e = cudaMalloc(&H.H2, sizeof(__nv_bfloat16) * r * kMlpH))) return e;
-  if ((e = cudaMalloc(&H.H3, sizeof(__nv_bfloat16) * r * kMlpH))) return e;
-  if ((e = cudaMalloc(&H.dZb, sizeof(__nv_bfloat16) * r * kMlpH))) return e;
-  if ((e = cudaMalloc(&H.dYb, sizeof(__nv_bfloat16) * r * kW4Pad))) return e;
-  if ((e = cudaMalloc(&H.Z1, sizeof(float) * r * kMlpH))) return e;
-  if ((e = cudaMalloc(&H.Z2, sizeof(float) * r * kMlpH))) return e;
-  if ((e = cudaMalloc(&H.Z3, sizeof(float) * r * kMlpH))) return e;
-  if ((e = cudaMalloc(&H.Z4, sizeof(float) * r * kW4Pad))) return e;
-  if ((e = cudaMalloc(&H.dZ, sizeof(float) * r * kMlpH))) return e;
-  if ((e = cudaMalloc(&H.dH, sizeof(float) * r * kMlpH))) return e;
-  if ((e = cudaMalloc(&H.dY, sizeof(float) * r * kW4Pad))) return e;
+  if ((e = cudaMalloc(&H.part, sizeof(float) * (size_t)kTrainMaxBlocks * kGradParams))) return e;
+  if ((e = cudaMalloc(&H.loss, sizeof(float) * kTrainMaxBlocks))) return e;
   if ((e = cudaMalloc(&H.G, sizeof(float) * kMlpParams))) return e;
-  if ((e = cudaMalloc(&H.Gpad, sizeof(float) * kMlpH * kMlpH))) return e;
   if ((e = cudaMalloc(&H.Am, sizeof(float) * kMlpParams))) return e;
   if ((e = cudaMalloc(&H.Av, sizeof(float) * kMlpParams))) return e;
-  if ((e = cudaMalloc(&H.loss, sizeof(float) * 256))) return e;
-  return cudaMalloc(&H.idx, sizeof(int) * r);
+  return cudaFuncSetAttribute(k_mlp_train_fb, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
 }
 
-// Forward + backward on rows (feat/tgt row-major, gathered by idx when
-// given); gradients into H.G, loss (mean squared error in normalised target
-// units) returned through the loss partials.
-static void forward_backward(rg_system* s, const float* feat, const float* tgt, const int* idx, int n) {
+// Forward + backward of rows [0, n) (feat/tgt row-major, gathered by idx
+// when given) into the per-block partial gradients and losses; returns the
+// number of blocks (partial slices) used.
+static int forward_backward(rg_system* s, const float* feat, const float* tgt, const int* idx, int n) {
   MlpHost& H = host_of(s);
-  MlpDev M = mlp_dev(s);
-  cudaStream_t st = s->stream;
-  const int eb = 256, eg = grid_for((long long)n * kMlpH, eb, 1024);
-  RGL k_mlp_input<<<grid_for((long long)n * kW1Pad, eb, 1024), eb, 0, st>>>(feat, idx, n, H.P, H.X);
-  // forward: Z = H_prev W^T (W row-major [out][in])
-  gemm(H.X, kW1Pad, 1, M.w1, 1, kW1Pad, H.Z1, kMlpH, n, kMlpH, kW1Pad, st);
-  RGL k_bias_silu<<<eg, eb, 0, st>>>(H.Z1, H.P + kOffB1, n, kMlpH, H.H1);
-  gemm(H.H1, kMlpH, 1, M.w2, 1, kMlpH, H.Z2, kMlpH, n, kMlpH, kMlpH, st);
-  RGL k_bias_silu<<<eg, eb, 0, st>>>(H.Z2, H.P + kOffB2, n, kMlpH, H.H2);
-  gemm(H.H2, kMlpH, 1, M.w3, 1, kMlpH, H.Z3, kMlpH, n, kMlpH, kMlpH, st);
-  RGL k_bias_silu<<<eg, eb, 0, st>>>(H.Z3, H.P + kOffB3, n, kMlpH, H.H3);
-  gemm(H.H3, kMlpH, 1, M.w4, 1, kMlpH, H.Z4, kW4Pad, n, kW4Pad, kMlpH, st);
-  RGL k_out_loss<<<128, 256, 0, st>>>(H.Z4, H.P, feat, tgt, idx, n, H.dY, H.dYb, H.loss);
-  // backward
-  cudaMemsetAsync(H.G, 0, sizeof(float) * kMlpParams, st);
-  // layer 4: dW4 = dY^T H3 ([8 x 128]), db4, dH3 = dY W4
-  gemm(H.dYb, 1, kW4Pad, H.H3, kMlpH, 1, H.Gpad, kMlpH, kW4Pad, kMlpH, n, st);
-  RGL k_unpad<<<4, 256, 0, st>>>(H.Gpad, kMlpOut, kMlpH, kMlpH, H.G + kOffW4);
-  RGL k_bias_grad<<<kW4Pad, 256, 0, st>>>(H.dY, n, kW4Pad, kMlpOut, H.G + kOffB4);
-  gemm(H.dYb, kW4Pad, 1, M.w4, kMlpH, 1, H.dH, kMlpH, n, kMlpH, kW4Pad, st);
-  // layer 3
-  RGL k_silu_back<<<eg, eb, 0, st>>>(H.dH, H.Z3, n, H.dZ, H.dZb);
-  gemm(H.dZb, 1, kMlpH, H.H2, kMlpH, 1, H.G + kOffW3, kMlpH, kMlpH, kMlpH, n, st);
-  RGL k_bias_grad<<<kMlpH, 256, 0, st>>>(H.dZ, n, kMlpH, kMlpH, H.G + kOffB3);
-  gemm(H.dZb, kMlpH, 1, M.w3, kMlpH, 1, H.dH, kMlpH, n, kMlpH, kMlpH, st);
-  // layer 2
-  RGL k_silu_back<<<eg, eb, 0, st>>>(H.dH, H.Z2, n, H.dZ, H.dZb);
-  gemm(H.dZb, 1, kMlpH, H.H1, kMlpH, 1, H.G + kOffW2, kMlpH, kMlpH, kMlpH, n, st);
-  RGL k_bias_grad<<<kMlpH, 256, 0, st>>>(H.dZ, n, kMlpH, kMlpH, H.G + kOffB2);
-  gemm(H.dZb, kMlpH, 1, M.w2, kMlpH, 1, H.dH, kMlpH, n, kMlpH, kMlpH, st);
-  // layer 1: dW1 = dZ1^T X ([128 x 16] -> first 8 columns)
-  RGL k_silu_back<<<eg, eb, 0, st>>>(H.dH, H.Z1, n, H.dZ, H.dZb);
-  gemm(H.dZb, 1, kMlpH, H.X, kW1Pad, 1, H.Gpad, kW1Pad, kMlpH, kW1Pad, n, st);
-  RGL k_unpad<<<8, 256, 0, st>>>(H.Gpad, kMlpH, kMlpIn, kW1Pad, H.G + kOffW1);
-  RGL k_bias_grad<<<kMlpH, 256, 0, st>>>(H.dZ, n, kMlpH, kMlpH, H.G + kOffB1);
+  const int tiles = (n + kTrainRows - 1) / kTrainRows;
+  const int nblk = tiles < kTrainMaxBlocks ? tiles : kTrainMaxBlocks;
+  RGL k_mlp_train_fb<<<nblk, kTrainThreads, kTrainSmem, s->stream>>>(mlp_dev(s), feat, tgt, idx, n, H.part,
+                                                                     H.loss);
+  return nblk;
 }
 
-static double read_loss(rg_system* s, int n) {
+static double read_loss(rg_system* s, int n, int nblk) {
   MlpHost& H = host_of(s);
-  float part[128];
-  cudaMemcpyAsync(part, H.loss, sizeof(part), cudaMemcpyDeviceToHost, s->stream);
+  std::vector<float> part(nblk);
+  cudaMemcpyAsync(part.data(), H.loss, sizeof(float) * nblk, cudaMemcpyDeviceToHost, s->stream);
   cudaStreamSynchronize(s->stream);
   double l = 0;
-  for (int i = 0; i < 128; ++i) l += part[i];
+  for (int i = 0; i < nblk; ++i) l += part[i];
   return l / ((double)n * kMlpOut);
 }
 
-// Normalisation from the data; He-uniform weights from the seed.
 static void init_params(std::vector<float>& P, const float* feat, const float* tgt, size_t n, uint64_t seed) {
   P.assign(kMlpParams, 0.0f);
   for (int k = 0; k < kMlpIn; ++k) {
@@ -397,9 +627,7 @@ void mlp_free(rg_system* s) {
   if (!s->mlp_host) return;
   MlpHost& H = host_of(s);
   cudaFree(H.P); cudaFree(H.wb);
-  cudaFree(H.X); cudaFree(H.H1); cudaFree(H.H2); cudaFree(H.H3); cudaFree(H.dZb); cudaFree(H.dYb);
-  cudaFree(H.Z1); cudaFree(H.Z2); cudaFree(H.Z3); cudaFree(H.Z4); cudaFree(H.dZ); cudaFree(H.dH);
-  cudaFree(H.dY); cudaFree(H.G); cudaFree(H.Gpad); cudaFree(H.Am); cudaFree(H.Av); cudaFree(H.loss);
+  cudaFree(H.part); cudaFree(H.loss); cudaFree(H.G); cudaFree(H.Am); cudaFree(H.Av);
   cudaFree(H.idx); cudaFree(H.feat); cudaFree(H.tgt);
   delete &H;
   s->mlp_host = nullptr;
@@ -464,13 +692,15 @@ int rg_mlp_grad(rg_system* s, const float* features, const float* targets, size_
   if (!s || !features || !targets || n == 0 || n > (1u << 24)) return RG_ERR_ARG;
   if (!s->mlp_host || !reinterpret_cast<MlpHost*>(s->mlp_host)->P) return RG_ERR_STATE;
   MlpHost& H = host_of(s);
-  if (ensure_workspace(s, (int)n)) return RG_ERR_CUDA;
+  if (ensure_workspace(s)) return RG_ERR_CUDA;
   float *df = nullptr, *dt = nullptr;
   if (cudaMalloc(&df, sizeof(float) * kMlpIn * n) || cudaMalloc(&dt, sizeof(float) * kMlpOut * n)) return RG_ERR_CUDA;
   cudaMemcpy(df, features, sizeof(float) * kMlpIn * n, cudaMemcpyHostToDevice);
   cudaMemcpy(dt, targets, sizeof(float) * kMlpOut * n, cudaMemcpyHostToDevice);
-  forward_backward(s, df, dt, nullptr, (int)n);
-  double l = read_loss(s, (int)n);
+  const int nblk = forward_backward(s, df, dt, nullptr, (int)n);
+  cudaMemsetAsync(H.G, 0, sizeof(float) * kMlpParams, s->stream);
+  RGL k_mlp_grad_sum<<<grid_for(kGradParams, 256), 256, 0, s->stream>>>(H.part, nblk, H.G);
+  double l = read_loss(s, (int)n, nblk);
   if (grad) cudaMemcpy(grad, H.G, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost);
   if (loss) *loss = (float)l;
   cudaFree(df);
@@ -488,7 +718,7 @@ int rg_mlp_train(rg_system* s, const float* features, const float* targets, size
   cudaMemcpy(H.P, P.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice);
   refresh_bf16(s);
   if (batch > (int)n) batch = (int)n;
-  if (ensure_workspace(s, batch)) return RG_ERR_CUDA;
+  if (ensure_workspace(s)) return RG_ERR_CUDA;
   if (H.nfeat < n) {
     cudaFree(H.feat);
     cudaFree(H.tgt);
@@ -500,25 +730,33 @@ int rg_mlp_train(rg_system* s, const float* features, const float* targets, size
   cudaMemcpy(H.tgt, targets, sizeof(float) * kMlpOut * n, cudaMemcpyHostToDevice);
   cudaMemset(H.Am, 0, sizeof(float) * kMlpParams);
   cudaMemset(H.Av, 0, sizeof(float) * kMlpParams);
+  if (H.nidx < n) {
+    cudaFree(H.idx);
+    if (cudaMalloc(&H.idx, sizeof(int) * n)) return RG_ERR_CUDA;
+    H.nidx = n;
+  }
   std::mt19937_64 rng(seed ^ 0xA5A5A5A5ull);
   std::vector<int> perm(n);
   for (size_t i = 0; i < n; ++i) perm[i] = (int)i;
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const MlpDev M = mlp_dev(s);
   long step = 0;
   double last = 0;
   for (int ep = 0; ep < epochs; ++ep) {
     std::shuffle(perm.begin(), perm.end(), rng);
+    // the epoch's order goes up once; each minibatch reads its slice
+    if (cudaMemcpyAsync(H.idx, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s->stream)) return RG_ERR_CUDA;
     double ep_loss = 0;
     int nb = 0;
     for (size_t b0 = 0; b0 + batch <= n; b0 += batch) {
-      cudaMemcpyAsync(H.idx, perm.data() + b0, sizeof(int) * batch, cudaMemcpyHostToDevice, s->stream);
-      forward_backward(s, H.feat, H.tgt, H.idx, batch);
+      const int nblk = forward_backward(s, H.feat, H.tgt, H.idx + b0, batch);
       ++step;
       float bc1 = 1.0f - std::pow(b1, (float)step), bc2 = 1.0f - std::pow(b2, (float)step);
-      RGL k_adam<<<64, 256, 0, s->stream>>>(H.P, H.G, H.Am, H.Av, lr, b1, b2, eps, bc1, bc2);
-      refresh_bf16(s);
+      RGL k_mlp_adam<<<grid_for(kGradParams, 256), 256, 0, s->stream>>>(
+          H.part, nblk, H.P, H.Am, H.Av, lr, b1, b2, eps, bc1, bc2, const_cast<__nv_bfloat16*>(M.w1),
+          const_cast<__nv_bfloat16*>(M.w2), const_cast<__nv_bfloat16*>(M.w3), const_cast<__nv_bfloat16*>(M.w4));
       if (ep == epochs - 1) {
-        ep_loss += read_loss(s, batch);
+        ep_loss += read_loss(s, batch, nblk);
         ++nb;
       }
     }
