@@ -8,10 +8,11 @@
 // (:1933-1995).  At 10^6 rods that serial loop dominates the set-up.
 //
 // Here every unplaced slot draws candidates in parallel, in rounds:
-//   1. try:     each unplaced slot draws up to D candidates (counter-based
-//               random numbers of (seed, slot, draw index)) and keeps the
-//               first one clear of every placed rod (27 cells of a grid of
-//               placed rods, cell >= L + d);
+//   1. try:     each unplaced slot has D candidate draws this round
+//               (counter-based random numbers of (seed, slot, draw index)),
+//               each tested by its own thread against every placed rod (27
+//               cells of a grid of placed rods, cell >= L + d); the first
+//               clear draw (lowest index) becomes the slot's candidate;
 //   2. resolve: survivors that overlap a survivor of a LOWER slot index are
 //               dropped (they retry next round), so accepted rods never
 //               overlap each other;
@@ -118,29 +119,53 @@ __device__ inline bool rsa_insert(const RsaGrid& G, d3 c, int i) {
   return false;
 }
 
-// 1. try: up to D draws per unplaced slot; the first draw clear of the
-// placed rods becomes the slot's candidate (candidate grid Gc).
-__global__ void k_rsa_try(int n, unsigned long long seed, RsaGrid G, RsaGrid Gc, const double* X, const double* U,
-                          double* CX, double* CU, const unsigned char* placed, long long* draws, int D,
-                          long long max_attempts, unsigned char* surv, double h, double d, double cut2,
-                          int* exhausted) {
+// 1. try.  a) the unplaced slots in a list (any order); every slot's
+// survivor flag cleared.
+__global__ void k_rsa_list(int n, const unsigned char* placed, unsigned char* surv, int* list, int* count,
+                           int* best) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     surv[i] = 0;
     if (placed[i]) continue;
-    long long k0 = draws[i];
+    best[i] = 0x7fffffff;
+    list[atomicAdd(count, 1)] = i;
+  }
+}
+// b) one thread per (listed slot, draw): a draw clear of the placed rods
+// lowers the slot's best draw index.
+__global__ void k_rsa_draws(unsigned long long seed, RsaGrid G, const double* X, const double* U, const int* list,
+                            const int* count, const long long* draws, int D, long long max_attempts, int* best,
+                            double h, double d, double cut2) {
+  const long long total = (long long)*count * D;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = list[t / D];
+    const long long k = draws[i] + t % D;
+    if (k >= max_attempts) continue;
+    d3 c, u;
+    rsa_draw(seed, i, k, G, c, u);
+    if (!rsa_hits(c, u, G, X, U, h, d, cut2, -1, -1)) atomicMin(&best[i], (int)k);
+  }
+}
+// c) per listed slot: the best draw becomes its candidate (recomputed from
+// its index) in the candidate grid Gc; the draw counter moves past it, or
+// past the round's D draws when none was clear.
+__global__ void k_rsa_pick(unsigned long long seed, RsaGrid G, RsaGrid Gc, const int* list, const int* count,
+                           long long* draws, int D, long long max_attempts, const int* best, double* CX,
+                           double* CU, unsigned char* surv, int* exhausted) {
+  const int m = *count;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const int i = list[j];
+    const long long k0 = draws[i];
     const long long k1 = min(k0 + (long long)D, max_attempts);
-    bool ok = false;
-    d3 c{}, u{};
-    long long k = k0;
-    for (; k < k1 && !ok; ++k) {
-      rsa_draw(seed, i, k, G, c, u);
-      ok = !rsa_hits(c, u, G, X, U, h, d, cut2, -1, -1);
-    }
-    draws[i] = k;
-    if (!ok) {
-      if (k >= max_attempts) atomicOr(exhausted, 1);  // this slot cannot be placed: the packing jams
+    const long long kb = best[i];
+    if (kb >= k1) {
+      draws[i] = k1;
+      if (k1 >= max_attempts) atomicOr(exhausted, 1);  // this slot cannot be placed: the packing jams
       continue;
     }
+    draws[i] = kb + 1;
+    d3 c, u;
+    rsa_draw(seed, i, kb, G, c, u);
     CX[3 * i] = c.x; CX[3 * i + 1] = c.y; CX[3 * i + 2] = c.z;
     CU[3 * i] = u.x; CU[3 * i + 1] = u.y; CU[3 * i + 2] = u.z;
     if (rsa_insert(Gc, c, i)) surv[i] = 1;  // a full candidate cell: retry next round
@@ -209,22 +234,23 @@ extern "C" int rg_scene_rsa_device(int n, double L, double d, double lo, double 
   // slots per cell: well above the mean; an overflow grows the grid
   const double per_cell = (double)n / (double)ncells;
   int cap = (int)std::ceil(2.0 * per_cell + 8.0 * std::sqrt(per_cell + 1.0) + 16.0);
-  DevBuf bX, bU, bCX, bCU, bPl, bSurv, bAcc, bDraw, bCnt, bCntC, bSlot, bSlotC, bFlags;
+  DevBuf bX, bU, bCX, bCU, bPl, bSurv, bAcc, bDraw, bCnt, bCntC, bSlot, bSlotC, bFlags, bList, bBest;
   cudaError_t e;
   if ((e = bX.alloc(sizeof(double) * 3 * (size_t)n)) || (e = bU.alloc(sizeof(double) * 3 * (size_t)n)) ||
       (e = bCX.alloc(sizeof(double) * 3 * (size_t)n)) || (e = bCU.alloc(sizeof(double) * 3 * (size_t)n)) ||
       (e = bPl.alloc((size_t)n)) || (e = bSurv.alloc((size_t)n)) || (e = bAcc.alloc((size_t)n)) ||
       (e = bDraw.alloc(sizeof(long long) * (size_t)n)) || (e = bCnt.alloc(sizeof(int) * ncells)) ||
-      (e = bCntC.alloc(sizeof(int) * ncells)) || (e = bFlags.alloc(sizeof(int) * 4))) {
+      (e = bCntC.alloc(sizeof(int) * ncells)) || (e = bFlags.alloc(sizeof(int) * 8)) ||
+      (e = bList.alloc(sizeof(int) * (size_t)n)) || (e = bBest.alloc(sizeof(int) * (size_t)n))) {
     cudaGetLastError();
     return RG_ERR_CUDA;
   }
   cudaMemset(bPl.p, 0, (size_t)n);
   cudaMemset(bDraw.p, 0, sizeof(long long) * (size_t)n);
   cudaMemset(bCnt.p, 0, sizeof(int) * ncells);
-  cudaMemset(bFlags.p, 0, sizeof(int) * 4);
+  cudaMemset(bFlags.p, 0, sizeof(int) * 8);
   // [0] placed count, [1] placed-grid overflow, [2] candidate overflow,
-  // [3] a slot used all its draws
+  // [3] a slot used all its draws, [4] unplaced slots listed this round
   int* flags = bFlags.as<int>();
   auto grid_of = [&](int* cnt, int* slot, int* ovf, int capc) {
     RsaGrid G;
@@ -242,15 +268,21 @@ extern "C" int rg_scene_rsa_device(int n, double L, double d, double lo, double 
   int h_flags[4] = {0, 0, 0, 0};
   for (int round = 0; remaining > 0; ++round) {
     // draws per slot this round: about 2e6 candidate draws per round, at
-    // most 64 per slot (one thread runs a slot's draws one after the other)
+    // most 64 per slot, one thread per draw
     int D = (int)std::min<long long>(64, std::max<long long>(1, 2000000LL / std::max(remaining, 1)));
     RsaGrid G = grid_of(bCnt.as<int>(), bSlot.as<int>(), flags + 1, capP);
     RsaGrid Gc = grid_of(bCntC.as<int>(), bSlotC.as<int>(), flags + 2, capC);
     cudaMemsetAsync(bCntC.p, 0, sizeof(int) * ncells);
     cudaMemsetAsync(flags + 2, 0, sizeof(int));
-    RGL k_rsa_try<<<blocks, kRsaBS>>>(n, seed, G, Gc, bX.as<double>(), bU.as<double>(), bCX.as<double>(),
-                                      bCU.as<double>(), bPl.as<unsigned char>(), bDraw.as<long long>(), D,
-                                      (long long)max_attempts, bSurv.as<unsigned char>(), h, d, cut2, flags + 3);
+    cudaMemsetAsync(flags + 4, 0, sizeof(int));
+    RGL k_rsa_list<<<blocks, kRsaBS>>>(n, bPl.as<unsigned char>(), bSurv.as<unsigned char>(), bList.as<int>(),
+                                       flags + 4, bBest.as<int>());
+    RGL k_rsa_draws<<<grid_for((long long)remaining * D, kRsaBS, 148 * 32), kRsaBS>>>(
+        seed, G, bX.as<double>(), bU.as<double>(), bList.as<int>(), flags + 4, bDraw.as<long long>(), D,
+        (long long)max_attempts, bBest.as<int>(), h, d, cut2);
+    RGL k_rsa_pick<<<blocks, kRsaBS>>>(seed, G, Gc, bList.as<int>(), flags + 4, bDraw.as<long long>(), D,
+                                       (long long)max_attempts, bBest.as<int>(), bCX.as<double>(), bCU.as<double>(),
+                                       bSurv.as<unsigned char>(), flags + 3);
     RGL k_rsa_resolve<<<blocks, kRsaBS>>>(n, Gc, bCX.as<double>(), bCU.as<double>(), bSurv.as<unsigned char>(),
                                           bAcc.as<unsigned char>(), h, d, cut2);
     RGL k_rsa_accept<<<blocks, kRsaBS>>>(n, G, bCX.as<double>(), bCU.as<double>(), bAcc.as<unsigned char>(),
