@@ -392,16 +392,22 @@ __global__ void k_cell_count_dyn(const Seg* seg, int n, const GridDev* gd, int p
 #endif
 __global__ void __launch_bounds__(256, RG_NARROW_MIN_BLOCKS) k_narrow_count(const Seg* seg, State st, Box box, double delta, const int* nbr_cnt,
                                const int* nbr, int maxnb, int words, unsigned long long* mask,
-                               int* hit_cnt, const Ctl* ctl) {
+                               int* hit_cnt, BodyCSR csr, const Ctl* ctl) {
   griddep_wait();
   if (ctl->err) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x)
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < st.n; i += gridDim.x * blockDim.x) {
     hit_cnt[i] = narrow_count_rod(i, seg, st.inv_mass, box, delta, nbr_cnt, nbr, maxnb, words, mask);
+    if (csr.cnt) {  // body CSR counts start from zero (counted by k_narrow_write)
+      csr.cnt[i] = 0;
+      csr.fill[i] = 0;
+      if (i == 0) csr.cnt[st.n] = 0;
+    }
+  }
 }
 
 __global__ void k_narrow_write(const Seg* seg, int n, Box box, const int* nbr_cnt, const int* nbr,
                                int maxnb, int words, const unsigned long long* mask, const int* hit_off,
-                               Contacts con, Ctl* ctl) {
+                               Contacts con, BodyCSR csr, Ctl* ctl) {
   griddep_wait();
   if (ctl->err) return;
   int total = hit_off[n];
@@ -411,8 +417,13 @@ __global__ void k_narrow_write(const Seg* seg, int n, Box box, const int* nbr_cn
   }
   if (total > con.cap) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (hit_off[i + 1] == hit_off[i]) continue;
-    narrow_write_rod(i, hit_off[i], seg, box, nbr_cnt, nbr, maxnb, words, mask, con);
+    const int o0 = hit_off[i], o1 = hit_off[i + 1];
+    if (o1 == o0) continue;
+    narrow_write_rod(i, o0, seg, box, nbr_cnt, nbr, maxnb, words, mask, con);
+    if (csr.cnt) {  // contacts per body for the body CSR (both sides)
+      atomicAdd(&csr.cnt[i], o1 - o0);
+      for (int o = o0; o < o1; ++o) atomicAdd(&csr.cnt[con.b[o]], 1);
+    }
   }
 }
 
@@ -559,7 +570,7 @@ void force_rebuild(rg_system* s) {
 // Full detection at the current state with activation margin `delta`:
 // segment records, (optional) displacement check and list rebuild, narrow
 // phase.  Result: s->con sorted by (a,b) and ctl->contacts.
-void detect_launch(rg_system* s, double delta, bool check_rebuild, bool seg_ready) {
+void detect_launch(rg_system* s, double delta, bool check_rebuild, bool seg_ready, bool body_csr) {
   Detector& d = s->det;
   const int n = s->n;
   cudaStream_t st = s->stream;
@@ -604,11 +615,12 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild, bool seg_read
     lnbr = d.near_nbr;
   }
   // --- narrow phase ---
+  const BodyCSR csr = body_csr ? s->csr : BodyCSR{};
   RGL launch_dep(k_narrow_count, g, bs, st, d.seg, s->st, s->box, delta, lcnt, lnbr, d.maxnb,
-                                   d.mask_words, d.hit_mask, d.hit_cnt, ctl);
+                                   d.mask_words, d.hit_mask, d.hit_cnt, csr, ctl);
   s->scan.run(d.hit_cnt, d.hit_off, &dd->n, &ctl->err, st);
   RGL launch_dep(k_narrow_write, g, bs, st, d.seg, n, s->box, lcnt, lnbr, d.maxnb, d.mask_words,
-                                   d.hit_mask, d.hit_off, s->con, ctl);
+                                   d.hit_mask, d.hit_off, s->con, csr, ctl);
 }
 
 }  // namespace rg

@@ -70,11 +70,13 @@ __global__ void k_csr_sort(int n, const int* off, int* ent, const Ctl* ctl) {
   }
 }
 
-void csr_launch(rg_system* s) {
+void csr_launch(rg_system* s, bool counted) {
   const int bs = 256;
   cudaStream_t st = s->stream;
-  RGL launch_dep(k_csr_zero, grid_for(s->n + 1, bs), bs, st, s->csr.cnt, s->csr.fill, s->n, s->d_ctl);
-  RGL launch_dep(k_csr_count, grid_for(s->ccap, bs), bs, st, s->con.a, s->con.b, s->csr.cnt, s->d_ctl);
+  if (!counted) {  // else the narrow phase zeroed and counted (detect_launch, body_csr)
+    RGL launch_dep(k_csr_zero, grid_for(s->n + 1, bs), bs, st, s->csr.cnt, s->csr.fill, s->n, s->d_ctl);
+    RGL launch_dep(k_csr_count, grid_for(s->ccap, bs), bs, st, s->con.a, s->con.b, s->csr.cnt, s->d_ctl);
+  }
   s->scan.run(s->csr.cnt, s->csr.off, detector_n_dev(s), &s->d_ctl->err, st);
   RGL launch_dep(k_csr_fill, grid_for(s->ccap, bs), bs, st, s->con.a, s->con.b, s->csr.off, s->csr.fill,
                                                    s->csr.ent, s->d_ctl);
@@ -157,9 +159,7 @@ __global__ void k_hist_merge(const int* ca, const int* cb, const int* touched, c
 __global__ void k_hist_finish(const int* toff, const int* koff, Ctl* ctl) {
   griddep_wait();
   if (ctl->err) return;
-  int T = toff[ctl->contacts], K = koff[ctl->hist_n];
-  ctl->hist_n = T + K;
-  ctl->contact_steps += ctl->contacts;  // contact-evaluations of the call
+  hist_finish(HistFinish{toff, koff}, ctl);
 }
 
 // ---------------------------------------------------------------------------
@@ -421,32 +421,23 @@ __global__ void k_soft_wall(State st, rg_config cfg, const Ctl* ctl) {
 }
 
 // Deterministic potential-energy sum: fixed-shape two-level reduction.
-constexpr int kPeBlocks = 64;
-__global__ void k_pe_partial(const double* pe, double* part, const Ctl* ctl) {
+// Potential energy Σ pe[c] by one block in a fixed order (deterministic).
+constexpr int kPeThreads = 1024;
+__global__ void __launch_bounds__(kPeThreads) k_pe_sum(const double* pe, Ctl* ctl) {
   griddep_wait();
   if (ctl->err) return;
   __shared__ double sm[32];
   const int C = ctl->contacts;
   double v = 0;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < C; c += gridDim.x * blockDim.x) v += pe[c];
+  for (int c = threadIdx.x; c < C; c += blockDim.x) v += pe[c];
   v = warp_sum(v);
   if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
   __syncthreads();
   if (threadIdx.x < 32) {
-    double u = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+    double u = sm[threadIdx.x];
     u = warp_sum(u);
-    if (threadIdx.x == 0) part[blockIdx.x] = u;
+    if (threadIdx.x == 0) ctl->pe = u;
   }
-}
-__global__ void k_pe_final(const double* part, Ctl* ctl) {
-  griddep_wait();
-  if (ctl->err) return;
-  double v = threadIdx.x < kPeBlocks ? part[threadIdx.x] : 0.0;
-  v = warp_sum(v);
-  __shared__ double sm[2];
-  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) ctl->pe = sm[0] + sm[1];
 }
 
 // One force evaluation: detect unless the contacts are fresh (seg_ready: the
@@ -464,8 +455,8 @@ void force_eval_launch(rg_system* s, EvalTail tail, bool seg_ready) {
   const int bs = 256;
   if (!s->contacts_fresh) {
     ProfScope p(s, ST_DETECT);
-    detect_launch(s, hm ? 0.0 : c.soft_delta, true, seg_ready);
-    csr_launch(s);
+    detect_launch(s, hm ? 0.0 : c.soft_delta, true, seg_ready, true);
+    csr_launch(s, true);
   }
   ProfScope prof(s, ST_FORCES);
   History& H = s->hist;
@@ -488,25 +479,25 @@ void force_eval_launch(rg_system* s, EvalTail tail, bool seg_ready) {
   RGL launch_dep(k_hist_merge, gc, bs, st, s->con.a, s->con.b, H.touched, H.touched_off, H.newval, H.key[cur],
                                   H.val[cur], H.frame[cur], H.kept, H.kept_off, H.key[nxt], H.val[nxt],
                                   H.frame[nxt], H.cap, s->ccap, s->d_ctl);
-  RGL launch_dep(k_hist_finish, 1, 1, st, H.touched_off, H.kept_off, s->d_ctl);
   H.cur = nxt;
   const bool wall = !hm && c.cylinder_enabled;
+  // the kick kernels also close the history merge (hist_finish)
+  const HistFinish hf{H.touched_off, H.kept_off};
   if (tail == EvalTail::kHalfPos) {
-    reduce_drift_launch(s, wall);
+    reduce_drift_launch(s, wall, hf);
     return;
   }
   if (tail == EvalTail::kSecondHalf) {
-    reduce_kick_launch(s, wall);
+    reduce_kick_launch(s, wall, hf);
   } else {
+    RGL launch_dep(k_hist_finish, 1, 1, st, H.touched_off, H.kept_off, s->d_ctl);
     RGL launch_dep(k_body_reduce, grid_for(s->n, bs), bs, st, s->st, s->csr.off, s->csr.ent, s->d_cf, s->ccap,
                                                      s->d_ctl);
     if (wall) {
       RGL launch_dep(k_soft_wall, grid_for(s->n, bs), bs, st, s->st, c, s->d_ctl);
     }
   }
-  double* part = s->d_cf + 13 * (size_t)s->ccap;
-  RGL launch_dep(k_pe_partial, kPeBlocks, 256, st, io.pe, part, s->d_ctl);
-  RGL launch_dep(k_pe_final, 1, 64, st, part, s->d_ctl);
+  RGL launch_dep(k_pe_sum, 1, kPeThreads, st, static_cast<const double*>(io.pe), s->d_ctl);
 }
 
 }  // namespace rg

@@ -50,9 +50,10 @@ struct DriftOut {
 };
 __global__ void __launch_bounds__(256, RG_BODY_MIN_BLOCKS)
     k_reduce_drift(State st, Box box, rg_config cfg, const int* off, const int* ent, const double* cf,
-                   int ccap, int wall, DriftOut o, Ctl* ctl) {
+                   int ccap, int wall, DriftOut o, HistFinish hf, Ctl* ctl) {
   griddep_wait();
   if (ctl->err) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) hist_finish(hf, ctl);
   __shared__ double sm[32], sm2[32];
   const d3 g{cfg.gravity[0], cfg.gravity[1], cfg.gravity[2]};
   const double dt = cfg.dt, hdt = 0.5 * cfg.dt;
@@ -112,9 +113,10 @@ __global__ void __launch_bounds__(256, RG_BODY_MIN_BLOCKS)
 // kept in f, tau; then the half kick, damping and the angular-speed clamp.
 __global__ void __launch_bounds__(256, RG_BODY_MIN_BLOCKS)
     k_reduce_kick(State st, rg_config cfg, const int* off, const int* ent, const double* cf, int ccap,
-                  int wall, Ctl* ctl) {
+                  int wall, HistFinish hf, Ctl* ctl) {
   griddep_wait();
   if (ctl->err) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) hist_finish(hf, ctl);
   const d3 g{cfg.gravity[0], cfg.gravity[1], cfg.gravity[2]};
   const double hdt = 0.5 * cfg.dt;
   const double el = exp(-cfg.lin_damp * cfg.dt), ea = exp(-cfg.ang_damp * cfg.dt);
@@ -180,7 +182,7 @@ __global__ void k_wrap_clear(State st, Box box, const Ctl* ctl) {
 
 static inline int body_grid(rg_system* s) { return grid_for(s->n, 256, s->sm_count * 8); }
 
-void reduce_drift_launch(rg_system* s, bool wall) {
+void reduce_drift_launch(rg_system* s, bool wall, HistFinish hf) {
   const Detector& d = s->det;
   DriftOut o;
   o.seg = d.seg;
@@ -188,11 +190,11 @@ void reduce_drift_launch(rg_system* s, bool wall) {
   o.ref2 = (d.all_pairs || !d.near_cnt) ? nullptr : d.ref2;
   o.skin = d.skin;
   RGL launch_dep(k_reduce_drift, body_grid(s), 256, s->stream, s->st, s->box, s->cfg, s->csr.off, s->csr.ent,
-                                                          s->d_cf, s->ccap, wall ? 1 : 0, o, s->d_ctl);
+                                                          s->d_cf, s->ccap, wall ? 1 : 0, o, hf, s->d_ctl);
 }
-void reduce_kick_launch(rg_system* s, bool wall) {
+void reduce_kick_launch(rg_system* s, bool wall, HistFinish hf) {
   RGL launch_dep(k_reduce_kick, body_grid(s), 256, s->stream, s->st, s->cfg, s->csr.off, s->csr.ent, s->d_cf,
-                                                         s->ccap, wall ? 1 : 0, s->d_ctl);
+                                                         s->ccap, wall ? 1 : 0, hf, s->d_ctl);
 }
 void clear_forces_launch(rg_system* s) {
   RGL launch_dep(k_clear_forces, body_grid(s), 256, s->stream, s->st, s->d_ctl);

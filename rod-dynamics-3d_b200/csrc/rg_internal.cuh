@@ -101,6 +101,19 @@ struct Detector {
   bool all_pairs = false;         // tiny periodic box: scan every cell
 };
 
+// Closes a history merge: the new table size from the two offset scans
+// (touched contacts + retained entries), and the call's contact-evaluation
+// count (k_hist_finish, or the first thread of the kick kernel after it).
+struct HistFinish {
+  const int* toff;
+  const int* koff;
+};
+__device__ inline void hist_finish(const HistFinish& h, Ctl* ctl) {
+  const int T = h.toff[ctl->contacts], K = h.koff[ctl->hist_n];
+  ctl->hist_n = T + K;
+  ctl->contact_steps += ctl->contacts;  // contact-evaluations of the call
+}
+
 struct BodyCSR {  // contacts incident to each body, in contact order
   int* cnt = nullptr;   // n+1
   int* off = nullptr;   // n+1
@@ -315,7 +328,10 @@ cudaError_t detector_alloc(rg_system* s);
 void detector_free(rg_system* s);
 // seg_ready: the segment records and the displacement check of the current
 // positions were written by the drift kernel (reduce_drift_launch)
-void detect_launch(rg_system* s, double delta, bool check_rebuild, bool seg_ready = false);
+// body_csr: the narrow phase also zeroes and counts the body CSR (csr_launch
+// then starts at its scan)
+void detect_launch(rg_system* s, double delta, bool check_rebuild, bool seg_ready = false,
+                   bool body_csr = false);
 void force_rebuild(rg_system* s);
 // rg_forces.cu
 enum class EvalTail { kForces, kHalfPos, kSecondHalf };
@@ -323,10 +339,10 @@ enum class EvalTail { kForces, kHalfPos, kSecondHalf };
 void force_eval_launch(rg_system* s, EvalTail tail = EvalTail::kForces, bool seg_ready = false);
 // forces at t reduced per body, first half kick and drift, segment records
 // and displacement check of the drifted positions (velocity Verlet)
-void reduce_drift_launch(rg_system* s, bool wall);
+void reduce_drift_launch(rg_system* s, bool wall, rg::HistFinish hf);
 // forces at t + dt reduced per body (kept in f, tau) and the second half kick
-void reduce_kick_launch(rg_system* s, bool wall);
-void csr_launch(rg_system* s);         // body CSR of the current contacts
+void reduce_kick_launch(rg_system* s, bool wall, rg::HistFinish hf);
+void csr_launch(rg_system* s, bool counted = false);  // body CSR of the current contacts
 // rg_integrate.cu
 void clear_forces_launch(rg_system* s);
 void nsc_free_flight_launch(rg_system* s);
