@@ -393,6 +393,21 @@ def time_batch(b, n_total, args, clk=None):
             "bytes": nsc_bytes(n_total * args.steps, cs, rs)}
 
 
+def job_totals(ms, rods, dist, device="cuda"):
+    """Whole-job figures of N replicas: the slowest rank's time (max over
+    ranks) and the rods all ranks stepped (sum).  Every rank calls it at the
+    same point (one all-reduce each for the two figures)."""
+    if not dist:
+        return ms, rods
+    import torch
+    import torch.distributed as tdist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    r = torch.tensor([float(rods)], dtype=torch.float64, device=device)
+    tdist.all_reduce(r, op=tdist.ReduceOp.SUM)
+    return float(t.item()), int(round(r.item()))
+
+
 def run_ours(args, rank, world):
     import rodgpu
     from rodgpu import scene
@@ -429,12 +444,10 @@ def run_ours(args, rank, world):
     clk = ClockSampler(dev)
     res = time_batch(learned, n_total, args, clk)
     torch.cuda.synchronize()
-    ms = res["ms"]
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = n_total * args.steps * world / (ms / 1000.0)
+    # replicas step different packings (seed + rank): whole-job rods are the
+    # sum over ranks, the time the slowest rank's
+    ms, job_rods = job_totals(res["ms"], n_total, dist)
+    value = job_rods * args.steps / (ms / 1000.0)
 
     # end to end through the C ABI: every step uploads all members' states
     # from page-locked host arrays (one bulk transfer per array), steps, and
@@ -451,7 +464,8 @@ def run_ours(args, rank, world):
         learned.step(1, stats=False)
         learned.get_state_all(out=host)
     t1 = time.perf_counter()
-    e2e = n_total * k_e2e / (t1 - t0)
+    e2e_s, _ = job_totals(t1 - t0, n_total, dist)
+    e2e = job_rods * k_e2e / e2e_s
     sched = learned.schedule()
     learned.close()
 
@@ -480,8 +494,8 @@ def run_ours(args, rank, world):
                        "speedup_learned_vs_plain_batched": round(res["value"] / res_plain["value"], 3),
                        "autotuned_rods_per_block": {"plain": best_plain, "learned": best},
                        "training": train},
-        "e2e": {"value": round(e2e, 1), "unit": "rod-steps/s", "h2d_bytes_per_step": n_total * 13 * 8,
-                "d2h_bytes_per_step": n_total * 13 * 8, "steps": k_e2e,
+        "e2e": {"value": round(e2e, 1), "unit": "rod-steps/s", "h2d_bytes_per_step": job_rods * 13 * 8,
+                "d2h_bytes_per_step": job_rods * 13 * 8, "steps": k_e2e,
                 "path": "rg_batch_set_state_all + rg_batch_step(1) + rg_batch_get_state_all, pinned host arrays"},
         "gpu_launches": res["kernel_launches"],
         "roofline": roof,
