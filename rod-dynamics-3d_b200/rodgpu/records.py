@@ -17,8 +17,8 @@ fraction, friction, dt, steps, ...).  Several files concatenate with merge().
 
 generate() produces a data set with the library's own plain PSOR: many
 seeded systems of the same generator, stepped together in one batch while
-recording (SURVEY config 3: N = 50,000, aspect ratio 20, mu ~ U[0.1, 0.8],
-200 runs x 200 steps).
+recording (the learned-warm-start configuration: N = 50,000, aspect ratio
+20, mu ~ U[0.1, 0.8], 200 runs x 200 steps).
 """
 import json
 
