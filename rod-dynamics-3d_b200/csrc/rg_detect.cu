@@ -52,14 +52,14 @@ __device__ inline void scan_status_store(unsigned long long* w, unsigned long lo
 }
 
 // Exclusive prefix of tile t (t > 0) from its predecessors' status words
-// (status[p] for tile p), by warp 0; valid in every lane.  Returns false
-// when a wait ran out (ERR_TIMEOUT set).
-__device__ inline bool scan_lookback(unsigned long long* status, int t, int* err, int& prefix) {
+// (status[p] for tile p >= first, the array's first tile), by warp 0;
+// valid in every lane.  Returns false when a wait ran out (ERR_TIMEOUT set).
+__device__ inline bool scan_lookback(unsigned long long* status, int t, int first, int* err, int& prefix) {
   const int lane = threadIdx.x & 31;
   prefix = 0;
   for (int p = t - 1;; p -= 32) {
-    const int idx = p - lane;  // lane k reads tile p - k
-    unsigned long long w = idx >= 0 ? scan_status_load(&status[idx]) : kTileInc;
+    const int idx = p - lane;  // lane k reads tile p - k (tiles before `first` belong to another array)
+    unsigned long long w = idx >= first ? scan_status_load(&status[idx]) : kTileInc;
     long long it = 0;
     while (!__all_sync(0xffffffffu, (w >> 62) != 0)) {
       if (++it > kScanSpin) {
@@ -72,37 +72,52 @@ __device__ inline bool scan_lookback(unsigned long long* status, int t, int* err
     // the nearest inclusive prefix (lowest lane) ends the walk
     const unsigned inc = __ballot_sync(0xffffffffu, (w & kTileInc) != 0);
     const int stop = inc ? __ffs(inc) - 1 : 32;
-    const int v = (lane <= stop && idx >= 0) ? (int)(unsigned)(w & 0xffffffffull) : 0;
+    const int v = (lane <= stop && idx >= first) ? (int)(unsigned)(w & 0xffffffffull) : 0;
     prefix += warp_sum_i(v);
     if (inc) return true;
   }
 }
 
 // words: [0] tile counter, [1] exit counter, [2 + t] status of tile t.
-__global__ void __launch_bounds__(kScanBS) k_scan_lookback(const int* in, int* out, const int* n_dev,
-                                                           unsigned long long* words, int* err) {
+// One or two arrays: tiles [0, nt0) scan array 0, [nt0, nt0 + nt1) array 1.
+struct ScanArrays {
+  const int* in[2];
+  int* out[2];
+  const int* n_dev[2];
+  int count;
+};
+__global__ void __launch_bounds__(kScanBS) k_scan_lookback(ScanArrays A, unsigned long long* words, int* err) {
   griddep_wait();
   __shared__ int shw[32];
   __shared__ int sh_tile, sh_excl, sh_ok, sh_last;
   int* tile_ctr = reinterpret_cast<int*>(&words[0]);
   int* exit_ctr = reinterpret_cast<int*>(&words[1]);
   unsigned long long* status = words + 2;
-  const int n = *n_dev;
-  const int ntile = (n + kScanTile - 1) / kScanTile;
-  if (ntile == 0 && blockIdx.x == 0 && threadIdx.x == 0) out[0] = 0;
-  const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+  int n_arr[2] = {0, 0}, nt[2] = {0, 0};
+  for (int a = 0; a < A.count; ++a) {
+    n_arr[a] = *A.n_dev[a];
+    nt[a] = (n_arr[a] + kScanTile - 1) / kScanTile;
+    if (nt[a] == 0 && blockIdx.x == 0 && threadIdx.x == 0) A.out[a][0] = 0;
+  }
+  const int ntile = nt[0] + nt[1];
   while (ntile > 0) {
     if (threadIdx.x == 0) sh_tile = atomicAdd(tile_ctr, 1);
     __syncthreads();
     const int t = sh_tile;
     if (t >= ntile) break;
-    const int base = t * kScanTile + threadIdx.x * kScanItems;
+    const int a = t < nt[0] ? 0 : 1;
+    const int first = a ? nt[0] : 0, lt = t - first;  // the array's first tile, the tile within it
+    const int n = n_arr[a];
+    const int* in = A.in[a];
+    int* out = A.out[a];
+    const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0;
+    const int base = lt * kScanTile + threadIdx.x * kScanItems;
     int v[kScanItems];
     if (vec && base + kScanItems <= n) {
-      const int4 a = *reinterpret_cast<const int4*>(in + base);
-      const int4 b = *reinterpret_cast<const int4*>(in + base + 4);
-      v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-      v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+      const int4 x = *reinterpret_cast<const int4*>(in + base);
+      const int4 y = *reinterpret_cast<const int4*>(in + base + 4);
+      v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+      v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
     } else {
 #pragma unroll
       for (int k = 0; k < kScanItems; ++k) v[k] = base + k < n ? in[base + k] : 0;
@@ -115,18 +130,18 @@ __global__ void __launch_bounds__(kScanBS) k_scan_lookback(const int* in, int* o
     if (threadIdx.x < 32) {
       int prefix = 0;
       bool ok = true;
-      if (t == 0) {
-        if (threadIdx.x == 0) scan_status_store(&status[0], kTileInc | (unsigned)tot);
+      if (lt == 0) {
+        if (threadIdx.x == 0) scan_status_store(&status[t], kTileInc | (unsigned)tot);
       } else {
         if (threadIdx.x == 0) scan_status_store(&status[t], kTileAgg | (unsigned)tot);
-        ok = scan_lookback(status, t, err, prefix);
+        ok = scan_lookback(status, t, first, err, prefix);
         // gave up: the call fails with ERR_TIMEOUT; later tiles see an aggregate
         if (ok && threadIdx.x == 0) scan_status_store(&status[t], kTileInc | (unsigned)(prefix + tot));
       }
       if (threadIdx.x == 0) {
         sh_excl = prefix;
         sh_ok = ok;
-        if (t == ntile - 1) out[n] = prefix + tot;
+        if (lt == nt[a] - 1) out[n] = prefix + tot;
       }
     }
     __syncthreads();
@@ -168,7 +183,7 @@ __global__ void __launch_bounds__(kScanBS) k_scan_lookback(const int* in, int* o
 cudaError_t Scan::alloc(int cap_) {
   cap = cap_;
   const int tiles = (cap + kScanTile - 1) / kScanTile + 1;
-  const size_t bytes = sizeof(unsigned long long) * (tiles + 2);
+  const size_t bytes = sizeof(unsigned long long) * (2 * tiles + 2);  // two arrays at most
   cudaError_t e = cudaMalloc(&d_blocks, bytes);
   if (e == cudaSuccess) e = cudaMemset(d_blocks, 0, bytes);
   return e;
@@ -181,7 +196,15 @@ void Scan::run(const int* in, int* out, const int* n_dev, int* err, cudaStream_t
   const int tiles = (cap + kScanTile - 1) / kScanTile + 1;
   int g = tiles < 148 * 4 ? tiles : 148 * 4;
   if (g < 1) g = 1;
-  RGL launch_dep(k_scan_lookback, g, kScanBS, s, in, out, n_dev, static_cast<unsigned long long*>(d_blocks), err);
+  ScanArrays A = {{in, nullptr}, {out, nullptr}, {n_dev, nullptr}, 1};
+  RGL launch_dep(k_scan_lookback, g, kScanBS, s, A, static_cast<unsigned long long*>(d_blocks), err);
+}
+void Scan::run2(const int* in0, int* out0, const int* n0_dev, const int* in1, int* out1, const int* n1_dev,
+                int* err, cudaStream_t s) const {
+  const int tiles = 2 * ((cap + kScanTile - 1) / kScanTile + 1);
+  int g = tiles < 148 * 4 ? tiles : 148 * 4;
+  ScanArrays A = {{in0, in1}, {out0, out1}, {n0_dev, n1_dev}, 2};
+  RGL launch_dep(k_scan_lookback, g, kScanBS, s, A, static_cast<unsigned long long*>(d_blocks), err);
 }
 
 // ---------------------------------------------------------------------------
@@ -248,7 +271,9 @@ __global__ void k_near_build(const Seg* seg, int n, const double* inv_mass, Box 
                              double near_skin, const int* nbr_cnt, const int* nbr, int maxnb, int* near_cnt,
                              int* near_nbr, double* ref2, const Ctl* ctl) {
   griddep_wait();
-  if (ctl->err || !near_rebuild_due(ctl, near_skin)) return;
+  // a list rebuild of this detection (its flag still set: k_lists_done
+  // clears it) makes the near lists due as well
+  if (ctl->err || !(ctl->rebuild || near_rebuild_due(ctl, near_skin))) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const Seg A = seg[i];
     const bool a_static = !(inv_mass[i] > 0.0);
@@ -270,12 +295,22 @@ __global__ void k_near_build(const Seg* seg, int n, const double* inv_mass, Box 
   }
 }
 
-__global__ void k_near_done(double near_skin, Ctl* ctl) {
+// Closes a detection with near lists (k_build_done and the near-list
+// close-out in one): counts a list rebuild, and marks the near lists built.
+__global__ void k_lists_done(double near_skin, Ctl* ctl) {
   griddep_wait();
-  if (ctl->err || !near_rebuild_due(ctl, near_skin)) return;
-  ctl->near_valid = 1;
-  ctl->near_disp = 0.0;
-  ctl->near_rebuilds += 1;
+  if (ctl->err) return;
+  const bool near_due = ctl->rebuild || near_rebuild_due(ctl, near_skin);
+  if (ctl->rebuild) {
+    ctl->rebuilds += 1;
+    ctl->rebuild = 0;
+  }
+  ctl->maxdisp = 0.0;
+  if (near_due) {
+    ctl->near_valid = 1;
+    ctl->near_disp = 0.0;
+    ctl->near_rebuilds += 1;
+  }
 }
 
 __global__ void k_cell_fill(int n, const int* cell_of, const int* cell_start, int* cell_fill,
@@ -603,16 +638,17 @@ void detect_launch(rg_system* s, double delta, bool check_rebuild, bool seg_read
                                        d.margin, d.skin, d.cut_center, d.all_pairs ? 1 : 0,
                                        d.nbr_cnt, d.nbr, d.maxnb, ctl);
   RGL launch_dep(k_save_ref, g, bs, st, d.seg, n, d.ref, d.nbr, d.nbr_cnt, d.maxnb, ctl);
-  RGL launch_dep(k_build_done, 1, 1, st, ctl);
   // --- near lists (every kernel below returns at once unless they are due) ---
   const int* lcnt = d.nbr_cnt;
   const int* lnbr = d.nbr;
   if (near) {
     RGL launch_dep(k_near_build, g, bs, st, d.seg, n, s->st.inv_mass, s->box, d.margin + d.near_skin, d.near_skin,
                                        d.nbr_cnt, d.nbr, d.maxnb, d.near_cnt, d.near_nbr, d.ref2, ctl);
-    RGL launch_dep(k_near_done, 1, 1, st, d.near_skin, ctl);
+    RGL launch_dep(k_lists_done, 1, 1, st, d.near_skin, ctl);
     lcnt = d.near_cnt;
     lnbr = d.near_nbr;
+  } else {
+    RGL launch_dep(k_build_done, 1, 1, st, ctl);
   }
   // --- narrow phase ---
   const BodyCSR csr = body_csr ? s->csr : BodyCSR{};

@@ -474,8 +474,8 @@ void force_eval_launch(rg_system* s, EvalTail tail, bool seg_ready) {
     RGL launch_dep(k_soft_forces, gc, bs, st, s->st, c, io, s->d_ctl);
   }
   // history merge
-  s->scan.run(H.touched, H.touched_off, &s->d_ctl->contacts, &s->d_ctl->err, st);
-  s->scan.run(H.kept, H.kept_off, &s->d_ctl->hist_n, &s->d_ctl->err, st);
+  s->scan.run2(H.touched, H.touched_off, &s->d_ctl->contacts, H.kept, H.kept_off, &s->d_ctl->hist_n,
+               &s->d_ctl->err, st);
   RGL launch_dep(k_hist_merge, gc, bs, st, s->con.a, s->con.b, H.touched, H.touched_off, H.newval, H.key[cur],
                                   H.val[cur], H.frame[cur], H.kept, H.kept_off, H.key[nxt], H.val[nxt],
                                   H.frame[nxt], H.cap, s->ccap, s->d_ctl);

@@ -20,6 +20,9 @@ struct Scan {
   cudaError_t alloc(int cap_);
   void free_();
   void run(const int* in, int* out, const int* n_dev, int* err, cudaStream_t s) const;
+  // two independent arrays (each of at most cap elements) in one launch
+  void run2(const int* in0, int* out0, const int* n0_dev, const int* in1, int* out1, const int* n1_dev, int* err,
+            cudaStream_t s) const;
 };
 
 // Device-resident control words of one system (one cudaMalloc).
