@@ -16,8 +16,9 @@ unreachable) and with the plain batched path.
   python bench.py --gpus N --steps K --warmup W           # this framework
   python bench.py --impl reference --steps K --warmup W   # reference CPU path
 
-Under torchrun each rank runs an independent replica (the path does not
-shard: replicas only); timing is max over ranks.  'value' is device time
+Under torchrun each rank runs an independent replica on its own packings
+(the path does not shard: replicas only); 'value' counts the rods of all
+ranks over the slowest rank's time.  'value' is device time
 (CUDA events on the library's stream) with the state resident in HBM; 'e2e'
 runs steps through the C ABI with every member's state uploaded from and
 read back to host memory every step.
