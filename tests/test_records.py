@@ -34,3 +34,4 @@ def test_rejects_bad_shapes_and_foreign_files(tmp_path):
     np.savez(tmp_path / "other.npz", format=np.array("something-else"), features=f)
     with pytest.raises(ValueError):
         records.load(tmp_path / "other.npz")
+
